@@ -1,0 +1,419 @@
+"""Benchmark of the determinant-space Hamiltonian hot path on B200.
+
+Workload (one GPU, N=1): a synthetic 30-orbital, 24-electron (12 alpha /
+12 beta) system with Cholesky-form integrals (K = 60), 1,000,000 unique
+determinants from seeded iterated heat-bath sampling (excitation level <= 4
+from HF), static heat-bath screening eps1 = 1e-6.
+
+One step = the hot path of one outer iteration on that space:
+  1. screened build of H_VV (singles + heat-bath doubles, Slater-Condon
+     elements, V lookup, CSR assembly) on the device;
+  2. H.psi with FP64 values -> local energies E_loc,i = (H psi)_i / psi_i
+     and the Rayleigh quotient;
+  3. the same with FP32 values and compensated FP32 accumulation
+     (|dE| against step 2 reported).
+
+`value` = screened H elements (nnz of H_VV) per second over the whole step,
+inputs resident in HBM; `e2e` = the same through the C ABI with host
+buffers (pinned host -> device copy of the determinants and psi, local
+energies copied back).  Under torchrun each rank builds its own system of
+the same size (seed + rank): weak scaling, no collective on the data path.
+
+`--impl reference` times the reference DetNQS C++ core (compiled from its
+sources into oracle/_ref) on a bounded sample of rows of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ORB, N_ALPHA, N_BETA, N_CHOL = 30, 12, 12, 60
+N_DETS = 1_000_000
+EPS1 = 1e-6
+INT_SEED, DET_SEED, PSI_SEED = 1001, 2002, 3003
+CACHE = os.path.join(tempfile.gettempdir(), "detnqs_b200_bench")
+
+
+def workload(rank: int, n_dets: int):
+    from detnqs_b200 import synthetic as S
+    sysm = S.make_system(N_ORB, N_ALPHA, N_BETA, N_CHOL, INT_SEED + rank)
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"dets_{N_ORB}_{n_dets}_{DET_SEED + rank}_{INT_SEED + rank}.npy")
+    if os.path.exists(path):
+        V = np.load(path)
+    else:
+        V = S.heat_bath_sample(sysm, n_dets, DET_SEED + rank)
+        np.save(path, V)
+    psi = S.normalized_psi(n_dets, PSI_SEED + rank)
+    return sysm, V, psi
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(kernel)
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path
+# ---------------------------------------------------------------------------
+
+def cpu_reference_sample(sysm, V, target_s: float = 15.0, min_rows: int = 64):
+    """Time the reference core's static heat-bath H_VV rows on a bounded
+    sample of rows of the same workload.  Returns (elements/s, rows, nnz,
+    seconds, threads, kind)."""
+    import oracle
+    if not os.path.exists(oracle.PORT_LIB):
+        oracle.build(None)
+    kind = "reference" if oracle.Checker.reference_available() else "port"
+    chk = oracle.Checker.reference() if kind == "reference" else oracle.Checker.port()
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    with tempfile.TemporaryDirectory() as d:
+        from detnqs_b200 import synthetic as S
+        if kind == "reference":
+            fd = os.path.join(d, "sys.fcidump")
+            S.write_fcidump(fd, sysm)
+            ctx = chk.ctx_from_fcidump(fd, N_ORB)
+        else:
+            ctx = chk.ctx_from_arrays(N_ORB, sysm.h1e, sysm.eri, sysm.e_core)
+        ctx.hb_prepare(1e-15)
+        rng = np.random.default_rng(77)
+        rows = np.sort(rng.choice(len(V), min_rows, replace=False))
+        t0 = time.perf_counter()
+        r = ctx.vv_hb_rows(V, rows, EPS1)
+        t_probe = time.perf_counter() - t0
+        # the map of V is built inside each call; time it separately
+        t0 = time.perf_counter()
+        ctx.vv_hb_rows(V, rows[:1], EPS1)
+        t_map = time.perf_counter() - t0
+        per_row = max((t_probe - t_map) / len(rows), 1e-6)
+        n_rows = int(min(len(V), max(min_rows, (target_s - t_map) / per_row)))
+        rows = np.sort(rng.choice(len(V), n_rows, replace=False))
+        t0 = time.perf_counter()
+        r = ctx.vv_hb_rows(V, rows, EPS1)
+        t = time.perf_counter() - t0
+        nnz = len(r["val"])
+    return nnz / t, n_rows, nnz, t, threads, kind
+
+
+def scipy_eloc_rate(H, psi, reps: int = 3):
+    """SciPy CSR matvec, exactly detnqs/operator/kernel.py:75-78 (one core)."""
+    A = H.to_scipy(0)
+    A.dot(psi)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        A.dot(psi)
+    t = (time.perf_counter() - t0) / reps
+    return len(psi) / t, t
+
+
+# ---------------------------------------------------------------------------
+# GPU step
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank: int, world: int):
+    import torch
+    from detnqs_b200 import core, device, native
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_dets = args.n_dets
+    sysm, V, psi = workload(rank, n_dets)
+    ctx = core.IntCtx.from_arrays(N_ORB, sysm.h1e, sysm.eri, sysm.e_core, device=local)
+    ctx.hb_prepare(1e-15)
+    V_dev = torch.from_numpy(V.view(np.int64)).to(dev)
+    psi_dev = torch.from_numpy(psi).to(dev)
+    eloc = torch.empty(n_dets, dtype=torch.float64, device=dev)
+    eloc32 = torch.empty(n_dets, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        H = device.build(ctx, V_dev, n_orb=N_ORB, policy=native.POLICY_STATIC,
+                         use_heatbath=True, eps1=EPS1, want_vp=False)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        e64 = H.local_energy(psi_dev, eloc=eloc, precision=native.F64)
+        ev[1].record()
+        e32 = H.local_energy(psi_dev, eloc=eloc32, precision=native.F32)
+        ev[2].record()
+        return H, e64, e32, ev
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        H, *_ = step()
+        H.close()
+    barrier()
+
+    launches0 = native.lib.dnq_launch_count()
+    clk = ClockSampler(local)
+    clk.start()
+    t_steps, t_build, t_fill, t_count, t_e64, t_e32 = [], [], [], [], [], []
+    nnz = cand = 0
+    dE = 0.0
+    for _ in range(args.steps):
+        flush.zero_()                         # L2 flush between timed steps
+        barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        H, e64, e32, ev = step()
+        s1.record()
+        torch.cuda.synchronize()
+        t_steps.append(s0.elapsed_time(s1))
+        tm = H.timings()
+        t_build.append(tm["total"])
+        t_fill.append(tm["fill"])
+        t_count.append(tm["count"])
+        t_e64.append(ev[0].elapsed_time(ev[1]))
+        t_e32.append(ev[1].elapsed_time(ev[2]))
+        nnz, cand = H.nnz_vv, H.candidates
+        dE = abs(e32[0] / e32[1] - e64[0] / e64[1])
+        if _ == args.steps - 1:
+            last = H
+        else:
+            H.close()
+    clocks = clk.stop()
+    launches = (native.lib.dnq_launch_count() - launches0) // args.steps
+    ms_step = float(np.mean(t_steps))
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+
+    # ---- end to end through the C ABI with host buffers
+    pin_V = torch.from_numpy(V.view(np.int64)).pin_memory()
+    pin_psi = torch.from_numpy(psi).pin_memory()
+    pin_eloc = torch.empty(n_dets, dtype=torch.float64).pin_memory()
+    Vh = pin_V.numpy().view(np.uint64)
+    ph = pin_psi.numpy()
+    eh = pin_eloc.numpy()
+    e2e = []
+    for k in range(max(1, args.steps)):
+        flush.zero_()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        H = device.build(ctx, Vh, n_orb=N_ORB, policy=native.POLICY_STATIC,
+                         use_heatbath=True, eps1=EPS1, want_vp=False)
+        H.local_energy(ph, eloc=eh, precision=native.F64)
+        H.local_energy(ph, eloc=eh, precision=native.F32)
+        b.record()
+        torch.cuda.synchronize()
+        e2e.append(a.elapsed_time(b))
+        H.close()
+    e2e_ms = float(np.mean(e2e))
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    peak, peak_kind = measured_peaks()
+    fill_ms = float(np.mean(t_fill))
+    alg_fill = n_dets * 16 + (n_dets + 1) * 8 + nnz * (4 + 8)      # dets in, CSR out
+    spmv_ms = float(np.mean(t_e64))
+    alg_spmv = nnz * (4 + 8) + n_dets * (8 + 8 + 8 + 8 + 8)         # CSR + rowptr/x/y/diag/eloc
+    result = {
+        "metric": "screened H elements/s (H_VV nnz per second of build + FP64 and FP32 "
+                  "local-energy passes)",
+        "value": world * nnz / (ms_step * 1e-3),
+        "unit": "elements/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 build; f64 and f32-compensated H.psi",
+        "data": "synthetic (seeded integrals, heat-bath sampled determinants)",
+        "config": {"workload": "30 orbitals, 12a/12b, K=60, 1e6 heat-bath-sampled dets, "
+                               "eps1=1e-6 static heat-bath, H_VV build + E_loc",
+                   "n_orb": N_ORB, "n_dets": n_dets, "eps1": EPS1, "nnz_H_VV": nnz,
+                   "candidates_per_step": cand, "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps"},
+        "e_loc_per_s": n_dets / (spmv_ms * 1e-3),
+        "e_loc_per_s_fp32": n_dets / (float(np.mean(t_e32)) * 1e-3),
+        "build_elements_per_s": nnz / (float(np.mean(t_build)) * 1e-3),
+        "candidates_per_s": cand / (float(np.mean(t_build)) * 1e-3),
+        "dE_fp32_vs_fp64_Ha": dE,
+        "build_phase_ms": {k: float(v) for k, v in last.timings().items()},
+        "roofline": {"bound": "hbm", "kernel": "k_build<fill>",
+                     "achieved": alg_fill / (fill_ms * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg_fill / (fill_ms * 1e-3) / 1e9 / peak,
+                     "traffic": ncu_traffic("k_build_fill"),
+                     "peak_kind": peak_kind,
+                     "note": "generation is integer/L2-latency bound; bytes are the CSR "
+                             "written and determinants read"},
+        "roofline_spmv": {"bound": "hbm", "kernel": "k_spmv_f64", "achieved":
+                          alg_spmv / (spmv_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": alg_spmv / (spmv_ms * 1e-3) / 1e9 / peak,
+                          "traffic": ncu_traffic("k_spmv_f64"), "peak_kind": peak_kind},
+        "e2e": {"value": world * nnz / (e2e_ms * 1e-3), "unit": "elements/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": n_dets * 16 + 2 * n_dets * 8,
+                "d2h_bytes_per_step": 2 * n_dets * 8 + 32},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, rows, cnnz, t, threads, kind = cpu_reference_sample(sysm, V, args.cpu_seconds)
+        er, et = scipy_eloc_rate(last, psi)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "elements/s", "cores": threads, "kind": kind,
+            "sample": f"{rows} random rows of the same 1e6-det space, static heat-bath "
+                      f"eps1=1e-6, H_VV rows ({cnnz} elements) in {t:.1f} s",
+            "e_loc_per_s_scipy_1core": er}
+    last.close()
+    return result
+
+
+def run_reference(args, rank: int, world: int):
+    """Reference CPU implementation on the same workload (rank 0 only)."""
+    if rank != 0:
+        return None
+    sysm, V, psi = workload(0, args.n_dets)
+    vals = []
+    info = None
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        pass
+    for _ in range(max(1, args.steps)):
+        rate, rows, nnz, t, threads, kind = cpu_reference_sample(
+            sysm, V, max(2.0, args.cpu_seconds / max(1, args.steps)))
+        vals.append(rate)
+        info = (rows, nnz, t, threads, kind)
+    rows, nnz, t, threads, kind = info
+    v = float(np.mean(vals))
+    return {
+        "impl": "reference",
+        "metric": "screened H elements/s (H_VV nnz per second of build + FP64 and FP32 "
+                  "local-energy passes)",
+        "value": v, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "30 orbitals, 12a/12b, K=60, 1e6 heat-bath-sampled dets, "
+                               "eps1=1e-6 static heat-bath, H_VV build + E_loc",
+                   "n_orb": N_ORB, "n_dets": args.n_dets, "eps1": EPS1},
+        "cpu_baseline": {"value": v, "unit": "elements/s", "cores": threads, "kind": kind,
+                         "sample": f"{rows} random rows per step, H_VV rows of the "
+                                   "static heat-bath policy (reference C++ core, OpenMP)"},
+        "e2e": {"value": v, "unit": "elements/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n-dets", type=int, default=N_DETS)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = run_ours(args, rank, world)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

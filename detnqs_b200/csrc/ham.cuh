@@ -1,0 +1,51 @@
+// ham.cuh -- Hamiltonian blocks resident in HBM.
+//
+// CSR with int64 row pointers, u32 column indices and FP64 values (the
+// reference's CSRMatrix, ham_utils.hpp:132-153).  For the FP32 operator the
+// V block also keeps FP32 off-diagonal values (diagonal zeroed) beside the
+// FP64 diagonal vector.
+#pragma once
+
+#include "common.cuh"
+
+namespace dnq {
+
+struct Csr {
+    DBuf<i64> rowptr;
+    DBuf<u32> col;
+    DBuf<double> val;
+    DBuf<float> val32;   // optional FP32 off-diagonal copy
+    i64 nr = 0, nc = 0, nnz = 0;
+    size_t bytes() const {
+        return rowptr.bytes() + col.bytes() + val.bytes() + val32.bytes();
+    }
+};
+
+}  // namespace dnq
+
+struct dnq_ham_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    dnq::i64 n_v = 0, n_p = 0;
+    dnq::Csr vv, vp;
+    dnq::Csr pv;                      // transpose of vp, built on first use
+    bool pv_ready = false;
+    dnq::DBuf<double> diag;           // H_ii of V (0 when dropped)
+    dnq::DBuf<float> x32;             // FP32 scratch for the FP32 operator
+    dnq::DBuf<unsigned long long> dets_p;   // (alpha, beta) pairs
+    dnq::i64 candidates = 0;
+    // device time of the build phases (CUDA events on the build stream), ms:
+    // [0] maps + diagonal, [1] count pass, [2] scans + allocation,
+    // [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total
+    double t_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    size_t bytes() const {
+        return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + x32.bytes() + dets_p.bytes();
+    }
+};
+
+namespace dnq {
+// Segmented sort of (col, val) pairs inside each CSR row by column.
+void sort_rows(Csr& m, cudaStream_t s);
+// Build the FP32 off-diagonal value copy of a square block.
+void make_f32(Csr& m, cudaStream_t s);
+}  // namespace dnq

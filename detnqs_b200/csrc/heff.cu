@@ -1,0 +1,490 @@
+// heff.cu -- downfolding H_eff = H_VV + H_VP D^-1 H_PV
+// (get_ham_eff, ham_eff.cpp:35-233).
+//
+//   1. H_VP and H_VV canonicalised on the device (sort by (row, col), sum
+//      duplicates, drop exact zeros: coo_to_csr, ham_utils.cpp:246-302);
+//      H_PV = transpose (rows ascending inside each column, as coo_to_csc).
+//   2. D^-1 in FP64 (sigma: d/(d^2+eps^2), linear: 1/(d+sgn(d) eps)) and
+//      column screening |D^-1_k| * ||col_k||^2 < 1e-12 (ham_eff.cpp:93-106).
+//   3. One warp per output row i walks the entries (k, a) of H_VP row i in
+//      ascending k and scatters a*D^-1_k*H_VP[j,k] into a dense accumulator
+//      over j (shared memory when it fits, else a per-warp HBM slab), with a
+//      bitmap of touched columns; the k loop is sequential so every output
+//      element is summed in the reference's order.  FP64 mode uses
+//      unfused multiply/add like the reference build; FP32 mode reads FP32
+//      H_VP values and keeps a TwoSum/TwoProduct-compensated FP32 pair per
+//      element.
+//   4. The H_VV row is added, entries with |v| <= 1e-15 dropped
+//      (csr_add, ham_utils.cpp:330-442), and the row is compacted in column
+//      order from the bitmap.
+#include <cub/cub.cuh>
+
+#include <memory>
+
+#include "ham.cuh"
+
+namespace dnq {
+
+void transpose_csr(const Csr& a, Csr& t, cudaStream_t s);
+
+namespace {
+
+constexpr int kHW = 4;   // warps per block
+
+__global__ void k_coo_keys(const u32* r, const u32* c, i64 n, u64* key, u32* idx,
+                           unsigned long long* bad, i64 nr, i64 nc) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        if ((i64)r[t] >= nr || (i64)c[t] >= nc) atomicAdd(bad, 1ull);
+        key[t] = ((u64)r[t] << 32) | c[t];
+        idx[t] = (u32)t;
+    }
+}
+
+__global__ void k_run_flags(const u64* key, i64 n, u32* flag) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        flag[t] = (t == 0 || key[t] != key[t - 1]) ? 1u : 0u;
+}
+
+// Sum each run of equal keys in input order; mark zero sums.
+__global__ void k_run_sum(const u64* key, const u32* perm, const double* val, const u32* runid,
+                          i64 n, double* rsum, u64* rkey) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        if (!(t == 0 || key[t] != key[t - 1])) continue;
+        double acc = val[perm[t]];
+        i64 u = t + 1;
+        while (u < n && key[u] == key[t]) acc = __dadd_rn(acc, val[perm[u]]), ++u;
+        rsum[runid[t] - 1] = acc;
+        rkey[runid[t] - 1] = key[t];
+    }
+}
+
+__global__ void k_nonzero(const double* v, i64 n, u32* f) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        f[t] = v[t] != 0.0;
+}
+
+__global__ void k_scatter_csr(const u64* rkey, const double* rsum, const u32* keep,
+                              const u32* pos, i64 n, u32* col, double* val, u32* rowcnt) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        if (!keep[t]) continue;
+        const u32 p = pos[t];
+        col[p] = (u32)(rkey[t] & 0xffffffffu);
+        val[p] = rsum[t];
+        atomicAdd(&rowcnt[rkey[t] >> 32], 1u);
+    }
+}
+
+__global__ void k_dinv(const double* hpp, i64 n, double e_ref, double eps, int sigma,
+                       double* dinv) {
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < n;
+         k += (i64)gridDim.x * blockDim.x) {
+        const double d = __dsub_rn(e_ref, hpp[k]);
+        dinv[k] = sigma ? __ddiv_rn(d, __dadd_rn(__dmul_rn(d, d), __dmul_rn(eps, eps)))
+                        : __ddiv_rn(1.0, __dadd_rn(d, copysign(eps, d)));
+    }
+}
+
+// ||col_k||^2 in row order (unfused, as the reference) and the skip flag.
+__global__ void k_screen(const i64* rp, const double* val, i64 n, const double* dinv,
+                         u8* skip) {
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < n;
+         k += (i64)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (i64 q = rp[k]; q < rp[k + 1]; ++q) s = __dadd_rn(s, __dmul_rn(val[q], val[q]));
+        skip[k] = __dmul_rn(fabs(dinv[k]), s) < 1e-12;
+    }
+}
+
+__global__ void k_cap(const i64* vprp, const u32* vpcol, const i64* pvrp, const u8* skip,
+                      const i64* vvrp, i64 nv, i64* cap) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nv;
+         i += (i64)gridDim.x * blockDim.x) {
+        i64 c = vvrp[i + 1] - vvrp[i];
+        for (i64 t = vprp[i]; t < vprp[i + 1]; ++t) {
+            const u32 k = vpcol[t];
+            if (!skip[k]) c += pvrp[k + 1] - pvrp[k];
+        }
+        cap[i] = c < nv ? c : nv;
+    }
+}
+
+__device__ __forceinline__ void f_two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float z = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, z)), __fsub_rn(b, z));
+}
+
+struct HeffParams {
+    i64 nv;
+    const i64* vprp; const u32* vpcol; const double* vpval; const float* vpval32;
+    const i64* pvrp; const u32* pvcol; const double* pvval; const float* pvval32;
+    const i64* vvrp; const u32* vvcol; const double* vvval;
+    const double* dinv; const u8* skip;
+    const i64* capoff;
+    u32* tcol; double* tval; u32* rowcnt;
+    int* next_row;
+    double* gacc;    // per-warp dense accumulators when not in shared memory
+    u32* gbits;
+    int words;       // bitmap words per warp
+};
+
+// F32 = false: acc holds FP64 sums.  F32 = true: during the scatter acc
+// holds (sum, err) float pairs, folded to FP64 before H_VV is added.
+template <bool F32, bool SMEM>
+__global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const i64 gw = (i64)blockIdx.x * kHW + w;
+    u32* bits;
+    double* acc;
+    if (SMEM) {
+        const size_t per = (((size_t)P.words * 4 + 15) & ~(size_t)15) + (size_t)P.nv * 8;
+        unsigned char* base = smem + per * w;
+        bits = (u32*)base;
+        acc = (double*)(base + (((size_t)P.words * 4 + 15) & ~(size_t)15));
+        for (int t = lane; t < P.words; t += 32) bits[t] = 0u;
+        for (i64 t = lane; t < P.nv; t += 32) acc[t] = 0.0;
+        __syncwarp();
+    } else {
+        bits = P.gbits + gw * P.words;
+        acc = P.gacc + gw * P.nv;
+    }
+    float2* acc2 = reinterpret_cast<float2*>(acc);
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(P.next_row, 1);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if (i >= P.nv) break;
+        // ---- scatter H_VP row i, k ascending
+        for (i64 t = P.vprp[i]; t < P.vprp[i + 1]; ++t) {
+            const u32 k = P.vpcol[t];
+            if (P.skip[k]) continue;
+            const double s = P.dinv[k];
+            const double a = P.vpval[t];
+            const bool need = !(a == 0.0 || s == 0.0);
+            const i64 q0 = P.pvrp[k], q1 = P.pvrp[k + 1];
+            if (!F32) {
+                const double as = __dmul_rn(a, s);
+                for (i64 q = q0 + lane; q < q1; q += 32) {
+                    const u32 j = P.pvcol[q];
+                    atomicOr(&bits[j >> 5], 1u << (j & 31));
+                    if (need) acc[j] = __dadd_rn(acc[j], __dmul_rn(as, P.pvval[q]));
+                }
+            } else {
+                const float as = (float)__dmul_rn((double)P.vpval32[t], s);
+                for (i64 q = q0 + lane; q < q1; q += 32) {
+                    const u32 j = P.pvcol[q];
+                    atomicOr(&bits[j >> 5], 1u << (j & 31));
+                    if (need) {
+                        const float b = P.pvval32[q];
+                        const float p = __fmul_rn(as, b);
+                        const float pe = fmaf(as, b, -p);
+                        float2 cur = acc2[j];
+                        float s2, e;
+                        f_two_sum(cur.x, p, s2, e);
+                        cur.x = s2;
+                        cur.y = __fadd_rn(cur.y, __fadd_rn(e, pe));
+                        acc2[j] = cur;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (F32) {   // fold (sum, err) pairs to FP64
+            for (int wd = lane; wd < P.words; wd += 32)
+                for (u32 m = bits[wd]; m; m &= m - 1) {
+                    const u32 j = (u32)wd * 32 + (__ffs(m) - 1);
+                    const float2 pr = acc2[j];
+                    acc[j] = (double)pr.x + (double)pr.y;
+                }
+            __syncwarp();
+        }
+        // ---- H_VV row i: csr_add gives vv + add; untouched columns get vv
+        for (i64 t = P.vvrp[i] + lane; t < P.vvrp[i + 1]; t += 32) {
+            const u32 j = P.vvcol[t];
+            const u32 bit = 1u << (j & 31);
+            const bool was = (bits[j >> 5] & bit) != 0u;
+            acc[j] = was ? __dadd_rn(P.vvval[t], acc[j]) : P.vvval[t];
+            atomicOr(&bits[j >> 5], bit);
+        }
+        __syncwarp();
+        // ---- compact in column order, keep |v| > 1e-15, clear the slab
+        i64 wpos = P.capoff[i];
+        u32 written = 0;
+        for (int w0 = 0; w0 < P.words; w0 += 32) {
+            const int wd = w0 + lane;
+            const u32 word = wd < P.words ? bits[wd] : 0u;
+            u32 keep = 0;
+            for (u32 m = word; m; m &= m - 1) {
+                const u32 j = (u32)wd * 32 + (__ffs(m) - 1);
+                if (fabs(acc[j]) > 1e-15) ++keep;
+            }
+            u32 incl = keep;
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+            i64 at = wpos + (incl - keep);
+            for (u32 m = word; m; m &= m - 1) {
+                const u32 j = (u32)wd * 32 + (__ffs(m) - 1);
+                const double v = acc[j];
+                if (fabs(v) > 1e-15) {
+                    P.tcol[at] = j;
+                    P.tval[at] = v;
+                    ++at;
+                }
+                acc[j] = 0.0;
+            }
+            if (wd < P.words) bits[wd] = 0u;
+            wpos += total;
+            written += total;
+        }
+        if (lane == 0) P.rowcnt[i] = written;
+        __syncwarp();
+    }
+}
+
+__global__ void k_compact(const i64* capoff, const u32* tcol, const double* tval,
+                          const i64* outoff, i64 nv, u32* col, double* val) {
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    for (i64 i = gw; i < nv; i += nw) {
+        const i64 src = capoff[i], dst = outoff[i], n = outoff[i + 1] - outoff[i];
+        for (i64 t = lane; t < n; t += 32) {
+            col[dst + t] = tcol[src + t];
+            val[dst + t] = tval[src + t];
+        }
+    }
+}
+
+__global__ void k_to_f32v(const double* v, i64 n, float* o) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        o[t] = (float)v[t];
+}
+
+int gs(i64 n) {
+    i64 b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
+}
+
+template <class T>
+void scan_excl(const T* in, i64* out, i64 n, cudaStream_t s) {
+    size_t tmp = 0;
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
+    DBuf<u8> tb(tmp, s);
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+}
+
+// COO (device) -> canonical CSR (sorted, duplicates summed in input order,
+// exact zeros dropped).
+void coo_to_csr_dev(const u32* r, const u32* c, const double* v, i64 n, i64 nr, i64 nc,
+                    Csr& out, cudaStream_t s) {
+    out.nr = nr;
+    out.nc = nc;
+    out.rowptr.alloc(nr + 1, s);
+    DBuf<u32> rowcnt(nr + 1, s);
+    DNQ_CUDA(cudaMemsetAsync(rowcnt.p, 0, (nr + 1) * 4, s));
+    if (n == 0) {
+        out.nnz = 0;
+        scan_excl(rowcnt.p, out.rowptr.p, nr + 1, s);
+        return;
+    }
+    require(n < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "COO input has more than 2^32 entries");
+    DBuf<u64> key(n, s), skey(n, s), rkey(n, s);
+    DBuf<u32> idx(n, s), perm(n, s), flag(n, s), runid(n, s);
+    DBuf<unsigned long long> bad(1, s);
+    DNQ_CUDA(cudaMemsetAsync(bad.p, 0, 8, s));
+    k_coo_keys<<<gs(n), 256, 0, s>>>(r, c, n, key.p, idx.p, bad.p, nr, nc);
+    DNQ_CHECK_LAUNCH();
+    unsigned long long hb = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&hb, bad.p, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    require(hb == 0, DNQ_ERR_RANGE, "coo_to_csr: row index out of bounds");
+    size_t tmp = 0;
+    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, skey.p, idx.p, perm.p, n, 0, 64, s));
+    DBuf<u8> tb(tmp, s);
+    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, key.p, skey.p, idx.p, perm.p, n, 0, 64, s));
+    k_run_flags<<<gs(n), 256, 0, s>>>(skey.p, n, flag.p);
+    DNQ_CHECK_LAUNCH();
+    size_t tmp2 = 0;
+    DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp2, flag.p, runid.p, n, s));
+    DBuf<u8> tb2(tmp2, s);
+    DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb2.p, tmp2, flag.p, runid.p, n, s));
+    u32 nruns = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&nruns, runid.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    DBuf<double> rsum(nruns, s);
+    k_run_sum<<<gs(n), 256, 0, s>>>(skey.p, perm.p, v, runid.p, n, rsum.p, rkey.p);
+    DNQ_CHECK_LAUNCH();
+    DBuf<u32> keep(nruns, s);
+    k_nonzero<<<gs(nruns), 256, 0, s>>>(rsum.p, nruns, keep.p);
+    DNQ_CHECK_LAUNCH();
+    DBuf<u32> pos32(nruns, s);
+    {   // positions fit in u32 (n < 2^32)
+        size_t t3 = 0;
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t3, keep.p, pos32.p, (i64)nruns, s));
+        DBuf<u8> tb3(t3, s);
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb3.p, t3, keep.p, pos32.p, (i64)nruns, s));
+    }
+    u32 lastpos = 0, lastkeep = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&lastpos, pos32.p + nruns - 1, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaMemcpyAsync(&lastkeep, keep.p + nruns - 1, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    out.nnz = (i64)lastpos + lastkeep;
+    out.col.alloc(out.nnz, s);
+    out.val.alloc(out.nnz, s);
+    k_scatter_csr<<<gs(nruns), 256, 0, s>>>(rkey.p, rsum.p, keep.p, pos32.p, nruns, out.col.p,
+                                            out.val.p, rowcnt.p);
+    DNQ_CHECK_LAUNCH();
+    scan_excl(rowcnt.p, out.rowptr.p, nr + 1, s);
+}
+
+}  // namespace
+
+void ham_eff(const u32* vvr, const u32* vvc, const double* vvv, i64 vvn, i64 nv,
+             const u32* vpr, const u32* vpc, const double* vpv, i64 vpn, i64 np,
+             const double* hpp, double e_ref, int sigma, double eps, int precision,
+             int device, cudaStream_t s, dnq_ham_s* H) {
+    H->device = device;
+    H->stream = s;
+    H->n_v = nv;
+    Csr VV, VP, PV;
+    coo_to_csr_dev(vvr, vvc, vvv, vvn, nv, nv, VV, s);
+    if (np == 0) {   // ham_eff.cpp:72-77: H_VV canonicalised
+        H->vv = std::move(VV);
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    coo_to_csr_dev(vpr, vpc, vpv, vpn, nv, np, VP, s);
+    transpose_csr(VP, PV, s);
+    DBuf<double> dinv(np, s);
+    DBuf<u8> skip(np, s);
+    k_dinv<<<gs(np), 256, 0, s>>>(hpp, np, e_ref, eps, sigma, dinv.p);
+    DNQ_CHECK_LAUNCH();
+    k_screen<<<gs(np), 256, 0, s>>>(PV.rowptr.p, PV.val.p, np, dinv.p, skip.p);
+    DNQ_CHECK_LAUNCH();
+    DBuf<i64> cap(nv + 1, s), capoff(nv + 1, s);
+    DNQ_CUDA(cudaMemsetAsync(cap.p + nv, 0, 8, s));
+    k_cap<<<gs(nv), 256, 0, s>>>(VP.rowptr.p, VP.col.p, PV.rowptr.p, skip.p, VV.rowptr.p, nv,
+                                 cap.p);
+    DNQ_CHECK_LAUNCH();
+    scan_excl(cap.p, capoff.p, nv + 1, s);
+    i64 captot = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&captot, capoff.p + nv, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+
+    HeffParams P{};
+    P.nv = nv;
+    P.vprp = VP.rowptr.p; P.vpcol = VP.col.p; P.vpval = VP.val.p;
+    P.pvrp = PV.rowptr.p; P.pvcol = PV.col.p; P.pvval = PV.val.p;
+    P.vvrp = VV.rowptr.p; P.vvcol = VV.col.p; P.vvval = VV.val.p;
+    P.dinv = dinv.p;
+    P.skip = skip.p;
+    P.capoff = capoff.p;
+    DBuf<u32> tcol(captot, s), rowcnt(nv + 1, s);
+    DBuf<double> tval(captot, s);
+    DNQ_CUDA(cudaMemsetAsync(rowcnt.p + nv, 0, 4, s));
+    P.tcol = tcol.p;
+    P.tval = tval.p;
+    P.rowcnt = rowcnt.p;
+    DBuf<int> next(1, s);
+    DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
+    P.next_row = next.p;
+    P.words = (int)((nv + 31) / 32);
+    DBuf<float> vp32, pv32;
+    if (precision == DNQ_F32) {
+        vp32.alloc(VP.nnz, s);
+        pv32.alloc(PV.nnz, s);
+        if (VP.nnz) k_to_f32v<<<gs(VP.nnz), 256, 0, s>>>(VP.val.p, VP.nnz, vp32.p);
+        DNQ_CHECK_LAUNCH();
+        if (PV.nnz) k_to_f32v<<<gs(PV.nnz), 256, 0, s>>>(PV.val.p, PV.nnz, pv32.p);
+        DNQ_CHECK_LAUNCH();
+        P.vpval32 = vp32.p;
+        P.pvval32 = pv32.p;
+    }
+    const size_t per_warp = (((size_t)P.words * 4 + 15) & ~(size_t)15) + (size_t)nv * 8;
+    const bool smem = per_warp * kHW <= 200 * 1024;
+    const int sms = sm_count(device);
+    DBuf<double> gacc;
+    DBuf<u32> gbits;
+    int grid;
+    if (smem) {
+        const size_t sm_bytes = per_warp * kHW;
+        auto kern = precision == DNQ_F32 ? k_heff<true, true> : k_heff<false, true>;
+        DNQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sm_bytes));
+        int per_sm = 0;
+        DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kHW * 32, sm_bytes));
+        grid = std::max(1, per_sm) * sms;
+        kern<<<grid, kHW * 32, sm_bytes, s>>>(P);
+        DNQ_CHECK_LAUNCH();
+    } else {
+        grid = sms * 2;
+        const i64 nw = (i64)grid * kHW;
+        gacc.alloc((size_t)nw * nv, s);
+        gbits.alloc((size_t)nw * P.words, s);
+        DNQ_CUDA(cudaMemsetAsync(gacc.p, 0, gacc.bytes(), s));
+        DNQ_CUDA(cudaMemsetAsync(gbits.p, 0, gbits.bytes(), s));
+        P.gacc = gacc.p;
+        P.gbits = gbits.p;
+        auto kern = precision == DNQ_F32 ? k_heff<true, false> : k_heff<false, false>;
+        kern<<<grid, kHW * 32, 0, s>>>(P);
+        DNQ_CHECK_LAUNCH();
+    }
+    DNQ_CHECK_LAUNCH();
+    H->vv.nr = nv;
+    H->vv.nc = nv;
+    H->vv.rowptr.alloc(nv + 1, s);
+    scan_excl(rowcnt.p, H->vv.rowptr.p, nv + 1, s);
+    DNQ_CUDA(cudaMemcpyAsync(&H->vv.nnz, H->vv.rowptr.p + nv, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    H->vv.col.alloc(H->vv.nnz, s);
+    H->vv.val.alloc(H->vv.nnz, s);
+    k_compact<<<sms * 4, 256, 0, s>>>(capoff.p, tcol.p, tval.p, H->vv.rowptr.p, nv, H->vv.col.p,
+                                      H->vv.val.p);
+    DNQ_CHECK_LAUNCH();
+    DNQ_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace dnq
+
+using namespace dnq;
+
+extern "C" {
+
+int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols, const double* vv_vals,
+                int64_t vv_nnz, int64_t n_v, const uint32_t* vp_rows, const uint32_t* vp_cols,
+                const double* vp_vals, int64_t vp_nnz, int64_t n_p, const double* h_pp,
+                double e_ref, int reg_sigma, double epsilon, int precision, int device,
+                void* stream, dnq_ham_t* out) {
+    DNQ_API_BEGIN
+    require(out != nullptr, DNQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    require(vv_nnz >= 0 && vp_nnz >= 0 && n_v >= 0 && n_p >= 0, DNQ_ERR_INVALID, "negative size");
+    require(n_v <= (int64_t)0xffffffffll && n_p <= (int64_t)0xffffffffll, DNQ_ERR_OVERFLOW,
+            "dimension exceeds u32 index capacity");
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    require(vv_nnz == 0 || (vv_rows && vv_cols && vv_vals), DNQ_ERR_INVALID, "null H_VV array");
+    require(vp_nnz == 0 || (vp_rows && vp_cols && vp_vals), DNQ_ERR_INVALID, "null H_VP array");
+    require(n_p == 0 || h_pp, DNQ_ERR_INVALID, "null h_pp_diag");
+    DeviceGuard g(device);
+    cudaStream_t s = (cudaStream_t)stream;
+    DIn<u32> vr(vv_rows, vv_nnz, s), vc(vv_cols, vv_nnz, s), pr(vp_rows, vp_nnz, s),
+        pc(vp_cols, vp_nnz, s);
+    DIn<double> vvv(vv_vals, vv_nnz, s), vpv(vp_vals, vp_nnz, s), hpp(h_pp, n_p, s);
+    std::unique_ptr<dnq_ham_s> H(new dnq_ham_s);
+    ham_eff(vr.p, vc.p, vvv.p, vv_nnz, n_v, pr.p, pc.p, vpv.p, vp_nnz, n_p, hpp.p, e_ref,
+            reg_sigma, epsilon, precision, device, s, H.get());
+    *out = H.release();
+    DNQ_API_END
+}
+
+}  // extern "C"

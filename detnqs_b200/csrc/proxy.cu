@@ -1,0 +1,170 @@
+// proxy.cu -- proxy operator on T = V + P (detnqs/operator/kernel.py:87-145):
+//   yv = H_VV xv + H_VP xp
+//   yp = H_PV xv + diag(H_PP) xp
+// H_PV is the transpose of H_VP, built once per handle on first use.
+#include <cub/cub.cuh>
+
+#include "ham.cuh"
+
+namespace dnq {
+
+void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
+                const double* yadd, int precision, cudaStream_t s, float* x32,
+                const double* diag);
+void to_f32(const double* x, i64 n, float* o, cudaStream_t s);
+
+namespace {
+
+__global__ void k_rows_of(const i64* rowptr, i64 nr, u32* rows) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
+         r += (i64)gridDim.x * blockDim.x)
+        for (i64 k = rowptr[r]; k < rowptr[r + 1]; ++k) rows[k] = (u32)r;
+}
+
+__global__ void k_iota32(u32* p, i64 n) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        p[t] = (u32)t;
+}
+
+__global__ void k_gather_t(const u32* perm, const u32* rows, const double* val, i64 n,
+                           u32* tcol, double* tval) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 k = perm[t];
+        tcol[t] = rows[k];
+        tval[t] = val[k];
+    }
+}
+
+// row pointer of the transposed block from the sorted column keys
+__global__ void k_bounds(const u32* skey, i64 n, i64 ncols, i64* rowptr) {
+    for (i64 c = blockIdx.x * (i64)blockDim.x + threadIdx.x; c <= ncols;
+         c += (i64)gridDim.x * blockDim.x) {
+        i64 lo = 0, hi = n;
+        while (lo < hi) {
+            const i64 mid = (lo + hi) / 2;
+            if ((i64)skey[mid] < c) lo = mid + 1; else hi = mid;
+        }
+        rowptr[c] = lo;
+    }
+}
+
+__global__ void k_diag_mul_add(const double* d, const double* x, i64 n, double* y) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        y[t] = d[t] * x[t];
+}
+
+__global__ void k_f32_all(const double* v, i64 n, float* o) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        o[t] = (float)v[t];
+}
+
+int gsz(i64 n) {
+    i64 b = (n + 255) / 256;
+    return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
+}
+
+}  // namespace
+
+void transpose_csr(const Csr& a, Csr& t, cudaStream_t s) {
+    t.nr = a.nc;
+    t.nc = a.nr;
+    t.nnz = a.nnz;
+    t.rowptr.alloc(t.nr + 1, s);
+    t.col.alloc(a.nnz, s);
+    t.val.alloc(a.nnz, s);
+    if (a.nnz == 0) {
+        DNQ_CUDA(cudaMemsetAsync(t.rowptr.p, 0, (t.nr + 1) * sizeof(i64), s));
+        return;
+    }
+    DBuf<u32> rows(a.nnz, s), perm(a.nnz, s), perm2(a.nnz, s), skey(a.nnz, s);
+    k_rows_of<<<gsz(a.nr), 256, 0, s>>>(a.rowptr.p, a.nr, rows.p);
+    DNQ_CHECK_LAUNCH();
+    k_iota32<<<gsz(a.nnz), 256, 0, s>>>(perm.p, a.nnz);
+    DNQ_CHECK_LAUNCH();
+    size_t tmp = 0;
+    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, a.col.p, skey.p, perm.p, perm2.p,
+                                             a.nnz, 0, 32, s));
+    DBuf<u8> tb(tmp, s);
+    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, a.col.p, skey.p, perm.p, perm2.p,
+                                             a.nnz, 0, 32, s));
+    k_gather_t<<<gsz(a.nnz), 256, 0, s>>>(perm2.p, rows.p, a.val.p, a.nnz, t.col.p, t.val.p);
+    DNQ_CHECK_LAUNCH();
+    k_bounds<<<gsz(t.nr + 1), 256, 0, s>>>(skey.p, a.nnz, t.nr, t.rowptr.p);
+    DNQ_CHECK_LAUNCH();
+}
+
+}  // namespace dnq
+
+using namespace dnq;
+
+namespace {
+Csr& pv_of(dnq_ham_s* h, cudaStream_t s) {
+    if (!h->pv_ready) {
+        transpose_csr(h->vp, h->pv, s);
+        h->pv_ready = true;
+    }
+    return h->pv;
+}
+}  // namespace
+
+extern "C" {
+
+int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp, const double* diag_p,
+                       double* yv, double* yp, int precision, void* stream) {
+    DNQ_API_BEGIN
+    require(h && xv && yv, DNQ_ERR_INVALID, "null argument");
+    require(h->n_p == 0 || (xp && yp && diag_p), DNQ_ERR_INVALID, "null P-space argument");
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const i64 nv = h->n_v, np = h->n_p;
+    DIn<double> xvd(xv, nv, s), xpd(xp, np, s), dpd(diag_p, np, s);
+    DBuf<double> yvd(nv, s), ypd(np, s), tmp(nv, s);
+    if (precision == DNQ_F64) {
+        spmv_block(h, h->vp, xpd.p, tmp.p, nullptr, DNQ_F64, s, nullptr, nullptr);
+        spmv_block(h, h->vv, xvd.p, yvd.p, tmp.p, DNQ_F64, s, nullptr, nullptr);
+        if (np) {
+            Csr& pv = pv_of(h, s);
+            DBuf<double> dterm(np, s);
+            k_diag_mul_add<<<gsz(np), 256, 0, s>>>(dpd.p, xpd.p, np, dterm.p);
+            DNQ_CHECK_LAUNCH();
+            spmv_block(h, pv, xvd.p, ypd.p, dterm.p, DNQ_F64, s, nullptr, nullptr);
+        }
+    } else {
+        // FP32 values for all three blocks; diagonal terms in FP64.
+        DBuf<float> xv32(nv, s), xp32(np, s);
+        to_f32(xvd.p, nv, xv32.p, s);
+        to_f32(xpd.p, np, xp32.p, s);
+        if (h->vv.val32.n != (size_t)h->vv.nnz) make_f32(h->vv, s);
+        if (h->vp.val32.n != (size_t)h->vp.nnz) {
+            h->vp.val32.alloc(h->vp.nnz, s);
+            if (h->vp.nnz) k_f32_all<<<gsz(h->vp.nnz), 256, 0, s>>>(h->vp.val.p, h->vp.nnz, h->vp.val32.p);
+            DNQ_CHECK_LAUNCH();
+        }
+        spmv_block(h, h->vp, xpd.p, tmp.p, nullptr, DNQ_F32, s, xp32.p, nullptr);
+        spmv_block(h, h->vv, xvd.p, yvd.p, tmp.p, DNQ_F32, s, xv32.p, h->diag.p);
+        if (np) {
+            Csr& pv = pv_of(h, s);
+            if (pv.val32.n != (size_t)pv.nnz) {
+                pv.val32.alloc(pv.nnz, s);
+                if (pv.nnz) k_f32_all<<<gsz(pv.nnz), 256, 0, s>>>(pv.val.p, pv.nnz, pv.val32.p);
+                DNQ_CHECK_LAUNCH();
+            }
+            DBuf<double> dterm(np, s);
+            k_diag_mul_add<<<gsz(np), 256, 0, s>>>(dpd.p, xpd.p, np, dterm.p);
+            DNQ_CHECK_LAUNCH();
+            spmv_block(h, pv, xvd.p, ypd.p, dterm.p, DNQ_F32, s, xv32.p, nullptr);
+        }
+    }
+    DNQ_CHECK_LAUNCH();
+    copy_out(yv, yvd.p, nv, s);
+    copy_out(yp, ypd.p, np, s);
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    DNQ_API_END
+}
+
+}  // extern "C"

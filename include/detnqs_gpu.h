@@ -1,0 +1,170 @@
+/*
+ * detnqs_gpu.h -- C ABI of the B200 determinant-space Hamiltonian library
+ * (libdetnqs_b200.so).
+ *
+ * Plain pointers, sizes and status codes only.  Every input pointer may be
+ * host memory or device memory of the context's GPU (the library detects
+ * which and copies host buffers itself); outputs of known size are written
+ * to caller pointers of either kind.  Results of data-dependent size stay in
+ * HBM inside a dnq_ham_t handle and are copied out on request.
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * wsmxcz/DetNQS).  The reference binds those through nanobind
+ * (csrc/bridge/bridge.cpp) and re-exports them from detnqs/core.py.
+ *
+ * Status: 0 on success, otherwise one of DNQ_ERR_*; dnq_last_error() returns
+ * the message of the last failure on the calling thread.  Messages for
+ * conditions the reference reports keep the reference's wording (for
+ * example "Heat-Bath table not initialized", bridge.cpp:303-304).
+ */
+#ifndef DETNQS_GPU_H
+#define DETNQS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dnq_ctx_s* dnq_ctx_t;    /* integrals + tables in HBM (IntCtx) */
+typedef struct dnq_ham_s* dnq_ham_t;    /* H_VV / H_VP / P-space in HBM      */
+
+enum {
+    DNQ_OK = 0,
+    DNQ_ERR_INVALID = 1,      /* std::invalid_argument in the reference      */
+    DNQ_ERR_NO_HEATBATH = 2,  /* heat-bath table required but not prepared  */
+    DNQ_ERR_DUPLICATE = 3,    /* duplicate determinant in an ordered set    */
+    DNQ_ERR_OUT_OF_MEMORY = 4,
+    DNQ_ERR_BUDGET = 5,       /* request exceeds the context's HBM budget   */
+    DNQ_ERR_OVERFLOW = 6,     /* an index would not fit in 32 bits          */
+    DNQ_ERR_TIMEOUT = 7,      /* a bounded device wait gave up              */
+    DNQ_ERR_CUDA = 8,
+    DNQ_ERR_IO = 9,           /* FCIDUMP could not be read                  */
+    DNQ_ERR_RANGE = 10        /* std::out_of_range in the reference         */
+};
+
+/* Screening policies of the row-streamed builder
+ * (csrc/src/hamiltonian/build_ham.cpp:78-196). */
+enum {
+    DNQ_POLICY_KNOWN_SETS = 0,  /* full doubles, route to V or a given set  */
+    DNQ_POLICY_STATIC = 1,      /* heat-bath doubles w >= eps1, P discovered */
+    DNQ_POLICY_DYNAMIC = 2      /* tau_i = eps1/max(|psi_i|,1e-12)          */
+};
+
+/* Value storage of a built block. */
+enum { DNQ_F64 = 0, DNQ_F32 = 1 };
+
+const char* dnq_last_error(void);
+int dnq_version(void);
+/* Number of kernels this library has launched in the process so far
+ * (its own kernels; CUB primitives it calls are not counted).  No
+ * reference counterpart (instrumentation). */
+int64_t dnq_launch_count(void);
+
+/* ---- integral context ------------------------------------------------------
+ * Replaces IntCtx(fcidump_path, num_orb) (bridge.cpp:108-128, :242-248) and
+ * IntegralMO (csrc/detnqs/integral/integral_mo.hpp:58-120).  Arrays are in
+ * the reference's packed layout: h1e[n(n+1)/2], eri[n1e(n1e+1)/2]. */
+int dnq_ctx_create(int n_orb, const double* h1e, const double* eri,
+                   double e_nuc, int device, dnq_ctx_t* out);
+int dnq_ctx_create_fcidump(const char* path, int n_orb, int device,
+                           dnq_ctx_t* out);
+int dnq_ctx_destroy(dnq_ctx_t ctx);
+int dnq_ctx_e_nuc(dnq_ctx_t ctx, double* out);      /* IntCtx.get_e_nuc   */
+int dnq_ctx_device_bytes(dnq_ctx_t ctx, int64_t* out);
+/* IntCtx.hb_prepare(threshold) / hb_clear() (hb_table.cpp:39-168). */
+int dnq_hb_prepare(dnq_ctx_t ctx, double threshold);
+int dnq_hb_clear(dnq_ctx_t ctx);
+/* Row {i,j} of the heat-bath table (HeatBathTable::row_view, hb_table.hpp:
+ * 155-158): writes min(len, cap) entries sorted by weight descending and
+ * returns len in *len.  Weights are |<ij||ab>|. */
+int dnq_hb_row(dnq_ctx_t ctx, int i, int j, int32_t* a, int32_t* b,
+               double* w, int64_t cap, int64_t* len);
+
+/* ---- Slater-Condon elements ---------------------------------------------- */
+/* detnqs.core.get_ham_diag (bridge.cpp:450-457, build_ham.cpp:388-400). */
+int dnq_ham_diag(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, double* out,
+                 void* stream);
+/* HamEval::compute_elem for n (bra, ket) pairs (ham_eval.cpp:33-51). */
+int dnq_ham_elems(dnq_ctx_t ctx, const uint64_t* bra, const uint64_t* ket,
+                  int64_t n, double* out, void* stream);
+/* det_ops::analyze_excitation degree and phase (det_ops.cpp:159-196). */
+int dnq_excitations(const uint64_t* bra, const uint64_t* ket, int64_t n,
+                    int32_t* degree, double* phase, int device, void* stream);
+
+/* ---- screened Hamiltonian build ------------------------------------------
+ * One call covers the four reference builders (build_ham.cpp:402-535):
+ *   get_ham_vv      : policy KNOWN_SETS, ext = NULL, want_vp = 0
+ *   get_ham_block   : policy KNOWN_SETS, ext = ket set
+ *   get_ham_conn    : policy STATIC (use_heatbath 0/1)
+ *   get_ham_conn_amp: policy DYNAMIC, psi = amplitudes on V
+ * want_vp = 0 keeps only the V->V block (the P set is not materialised).
+ * Values are kept in FP64; the FP32 operator copy is made on first use. */
+int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V,
+              const uint64_t* dets_ext, int64_t n_ext, const double* psi,
+              int n_orb, int policy, int use_heatbath, double eps1,
+              int want_vp, void* stream, dnq_ham_t* out);
+int dnq_ham_destroy(dnq_ham_t h);
+/* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
+ *        [4] candidates examined, [5] device bytes held */
+int dnq_ham_info(dnq_ham_t h, int64_t* info6);
+/* Device time of the build phases, from CUDA events recorded on the build
+ * stream (ms): [0] maps + diagonal, [1] count pass, [2] scans/allocation,
+ * [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total,
+ * [7] unused.  No reference counterpart (instrumentation). */
+int dnq_ham_timings(dnq_ham_t h, double* ms8);
+/* block 0 = H_VV, 1 = H_VP; COO sorted by (row, col) as in
+ * from_coo_matrix (bridge.cpp:173-196).  Any pointer may be NULL. */
+int dnq_ham_copy_coo(dnq_ham_t h, int block, uint32_t* rows, uint32_t* cols,
+                     double* vals, void* stream);
+/* CSR view: row_ptr[n_rows+1] (int64), cols, vals (FP64). */
+int dnq_ham_copy_csr(dnq_ham_t h, int block, int64_t* row_ptr, uint32_t* cols,
+                     double* vals, void* stream);
+int dnq_ham_copy_dets_p(dnq_ham_t h, uint64_t* dets, void* stream);
+int dnq_ham_copy_diag(dnq_ham_t h, double* diag, void* stream);
+
+/* ---- H.psi / local energy -------------------------------------------------
+ * Replaces the SciPy CSR matvec of detnqs/operator/kernel.py:75-78
+ * (build_vv_operator) with y = H_VV x on the device.  precision DNQ_F64
+ * computes in FP64; DNQ_F32 reads FP32 off-diagonal values and FP32 x with
+ * two-sum compensated FP32 accumulation, adds the FP64 diagonal term in FP64
+ * and writes FP64 y. */
+int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision,
+                 void* stream);
+/* Proxy operator (kernel.py:127-139):
+ *   yv = H_VV xv + H_VP xp ;  yp = H_PV xv + diag_p * xp */
+int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp,
+                       const double* diag_p, double* yv, double* yp,
+                       int precision, void* stream);
+/* Rayleigh quotient and local energies from one y = H x pass:
+ * out2 = {x.Hx, x.x} (compensated FP64 sums); eloc[i] = y_i / x_i
+ * (NULL to skip). */
+int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc,
+                         double* out2, int precision, void* stream);
+
+/* ---- matrix-free contractions (csrc/src/hamiltonian/local_conn.cpp) ------ */
+/* compute_variational_energy (local_conn.cpp:148-229). */
+int dnq_variational_energy(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
+                           const double* coeffs, int n_orb, int use_heatbath,
+                           double eps1, double* out, void* stream);
+
+/* ---- downfolding -----------------------------------------------------------
+ * get_ham_eff (ham_eff.cpp:64-233): H_eff = H_VV + H_VP D^-1 H_PV with
+ * D_k = e_ref - h_pp[k]; reg_sigma 1 -> d/(d^2+eps^2), 0 -> 1/(d+sgn(d)eps).
+ * Inputs are COO triplets (any order, duplicates summed).  precision
+ * DNQ_F32 stores H_VP values in FP32 and accumulates each output element
+ * with two-sum compensation; D^-1 stays FP64. */
+int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols,
+                const double* vv_vals, int64_t vv_nnz, int64_t n_v,
+                const uint32_t* vp_rows, const uint32_t* vp_cols,
+                const double* vp_vals, int64_t vp_nnz, int64_t n_p,
+                const double* h_pp, double e_ref, int reg_sigma,
+                double epsilon, int precision, int device, void* stream,
+                dnq_ham_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DETNQS_GPU_H */
