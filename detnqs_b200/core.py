@@ -254,6 +254,111 @@ def get_ham_eff(H_VV: dict, H_VP: dict, h_pp_diag, e_ref: float,
         H.close()
 
 
+# ---------------------------------------------------------------------------
+# Determinant generation (bridge.cpp:265-341)
+# ---------------------------------------------------------------------------
+
+_MODES = {"none": 0, "static": 1, "dynamic": 2}
+
+
+def _gen(int_ctx, dets, n_orb, psi, mode: int, eps1: float) -> np.ndarray:
+    d = _dets(dets)
+    p = None if psi is None else _f64(psi)
+    h = C.c_void_p()
+    ctx = None if int_ctx is None else _ctx(int_ctx)
+    N.check(N.lib.dnq_gen_dets(None if ctx is None else ctx.handle, N.ptr(d), d.shape[0],
+                               int(n_orb), N.ptr(p), mode, float(eps1),
+                               0 if ctx is None else ctx.device, N.stream_of(d, p),
+                               C.byref(h)))
+    H = DeviceHamiltonian(h.value)
+    try:
+        return H.dets_p()
+    finally:
+        H.close()
+
+
+def gen_connected_dets(ref_dets, n_orb: int, device: int = 0) -> np.ndarray:
+    """All unique singles and doubles of the references, sorted
+    (det_space.cpp:167-213 + canonicalize)."""
+    d = _dets(ref_dets)
+    h = C.c_void_p()
+    N.check(N.lib.dnq_gen_dets(None, N.ptr(d), d.shape[0], int(n_orb), None, -1, 0.0,
+                               int(device), N.stream_of(d), C.byref(h)))
+    H = DeviceHamiltonian(h.value)
+    try:
+        return H.dets_p()
+    finally:
+        H.close()
+
+
+def gen_perturbative_dets(ref_dets, n_orb: int, int_ctx=None, psi_v=None,
+                          mode: str = "none", eps1: float = 1e-6) -> np.ndarray:
+    """P = C \\ V with optional heat-bath screening (bridge.cpp:278-341)."""
+    if mode not in _MODES:
+        raise ValueError(f"invalid screen mode: {mode}")
+    m = _MODES[mode]
+    if m == 0:
+        d = _dets(ref_dets)
+        h = C.c_void_p()
+        dev = 0 if int_ctx is None else _ctx(int_ctx).device
+        N.check(N.lib.dnq_gen_dets(None, N.ptr(d), d.shape[0], int(n_orb), None, 0, 0.0, dev,
+                                   N.stream_of(d), C.byref(h)))
+        H = DeviceHamiltonian(h.value)
+        try:
+            return H.dets_p()
+        finally:
+            H.close()
+    if int_ctx is None:
+        raise TypeError("screened modes need int_ctx")
+    if m == 2:
+        if psi_v is None:
+            raise TypeError("dynamic mode needs psi_v")
+        p = _f64(psi_v)
+        if (p.shape[0] if isinstance(p, np.ndarray) else p.numel()) != _dets(ref_dets).shape[0]:
+            raise ValueError("psi_v size mismatch")
+        return _gen(int_ctx, ref_dets, n_orb, p, 2, eps1)
+    return _gen(int_ctx, ref_dets, n_orb, None, 1, eps1)
+
+
+def get_local_connections(dets, int_ctx, n_orb: int, use_heatbath: bool = False,
+                          eps1: float = 1e-6) -> dict:
+    """CSR-like local connectivity (local_conn.cpp:96-142): ``offsets``
+    int32[N+1], ``dets`` uint64[M, 2], ``values`` float64[M]."""
+    ctx = _ctx(int_ctx)
+    d = _dets(dets)
+    h = C.c_void_p()
+    N.check(N.lib.dnq_local_connections(ctx.handle, N.ptr(d), d.shape[0], int(n_orb),
+                                        int(bool(use_heatbath)), float(eps1),
+                                        N.stream_of(d), C.byref(h)))
+    H = DeviceHamiltonian(h.value)
+    try:
+        m = H.n_p
+        off = np.empty(d.shape[0] + 1, np.int32)
+        kd = np.empty((m, 2), np.uint64)
+        vals = np.empty(m, np.float64)
+        N.check(N.lib.dnq_conn_copy(H.handle, off.ctypes.data, kd.ctypes.data,
+                                    vals.ctypes.data, None))
+        return {"offsets": off, "dets": kd, "values": vals}
+    finally:
+        H.close()
+
+
+def compute_pt2(dets_V, coeffs_V, int_ctx, n_orb: int, e_ref: float,
+                use_heatbath: bool = False, eps1: float = 1e-6) -> dict:
+    """Decomposed EN-PT2 (local_conn.cpp:247-418)."""
+    ctx = _ctx(int_ctx)
+    d = _dets(dets_V)
+    c = _f64(coeffs_V)
+    if (c.shape[0] if isinstance(c, np.ndarray) else c.numel()) != d.shape[0]:
+        raise ValueError("coefficient size mismatch")
+    out = np.zeros(3)
+    N.check(N.lib.dnq_pt2(ctx.handle, N.ptr(d), d.shape[0], N.ptr(c), int(n_orb),
+                          float(e_ref), int(bool(use_heatbath)), float(eps1),
+                          out.ctypes.data, N.stream_of(d, c)))
+    return {"e_pt2_internal": float(out[0]), "e_pt2_external": float(out[1]),
+            "n_ext": int(out[2])}
+
+
 def compute_variational_energy(dets, coeffs, int_ctx, n_orb: int,
                                use_heatbath: bool = False, eps1: float = 1e-6) -> float:
     """<Psi|H|Psi> on a fixed basis, matrix-free (local_conn.cpp:148-229)."""
@@ -280,5 +385,9 @@ __all__ = [
     "get_ham_conn_amp",
     "get_ham_eff",
     "compute_variational_energy",
+    "gen_connected_dets",
+    "gen_perturbative_dets",
+    "get_local_connections",
+    "compute_pt2",
     "HEATBATH_THRESH",
 ]

@@ -223,12 +223,37 @@ __global__ void k_iota(u32* p, i64 n) {
         p[t] = (u32)t;
 }
 
-__global__ void k_to_f32(const i64* rowptr, const u32* col, const double* val, i64 nr,
-                         float* out) {
+// FP32 copy of every value (streaming, 2 values per thread step).
+__global__ void k_vals_f32(const double2* __restrict__ v, i64 n2, float2* __restrict__ o) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n2;
+         t += (i64)gridDim.x * blockDim.x) {
+        const double2 x = v[t];
+        o[t] = make_float2((float)x.x, (float)x.y);
+    }
+}
+
+__global__ void k_val_f32_tail(const double* v, i64 n, float* o) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) o[n - 1] = (float)v[n - 1];
+}
+
+// Diagonal entry of each (column-sorted) row: moved out of the FP32 copy
+// into the FP64 vector (0 when the row has none).
+__global__ void k_split_diag(const i64* rowptr, const u32* col, const double* val, i64 nr,
+                             float* out, double* dout) {
     for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
-         r += (i64)gridDim.x * blockDim.x)
-        for (i64 k = rowptr[r]; k < rowptr[r + 1]; ++k)
-            out[k] = col[k] == (u32)r ? 0.0f : (float)val[k];
+         r += (i64)gridDim.x * blockDim.x) {
+        i64 lo = rowptr[r], hi = rowptr[r + 1];
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if (col[mid] < (u32)r) lo = mid + 1; else hi = mid;
+        }
+        double d = 0.0;
+        if (lo < rowptr[r + 1] && col[lo] == (u32)r) {
+            d = val[lo];
+            out[lo] = 0.0f;
+        }
+        if (dout) dout[r] = d;
+    }
 }
 
 inline int grid_for(i64 n, int threads = 256) {
@@ -273,10 +298,21 @@ void sort_rows(Csr& m, cudaStream_t s) {
     m.val = std::move(val2);
 }
 
-void make_f32(Csr& m, cudaStream_t s) {
+void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out) {
     m.val32.alloc(m.nnz, s);
-    if (m.nnz == 0) return;
-    k_to_f32<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr, m.val32.p);
+    if (diag_out) diag_out->alloc(m.nr, s);
+    if (m.nr == 0) return;
+    if (m.nnz) {
+        int dev = 0;
+        DNQ_CUDA(cudaGetDevice(&dev));
+        const int grid = sm_count(dev) * 8;
+        k_vals_f32<<<grid, 256, 0, s>>>((const double2*)m.val.p, m.nnz / 2, (float2*)m.val32.p);
+        DNQ_CHECK_LAUNCH();
+        k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, m.nnz, m.val32.p);
+        DNQ_CHECK_LAUNCH();
+    }
+    k_split_diag<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr, m.val32.p,
+                                                diag_out ? diag_out->p : nullptr);
     DNQ_CHECK_LAUNCH();
 }
 
@@ -324,12 +360,20 @@ struct PhaseTimer {
     }
 };
 
+// Testing switch: route V->V-only builds through the candidate walk too
+// (dnq_set_option(DNQ_OPT_FORCE_WALK, 1)); both paths give identical blocks.
+bool g_force_walk = false;
+
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
     if (policy == DNQ_POLICY_STATIC && use_hb) return hb_cutoff(c, eps1);
     if (policy == DNQ_POLICY_DYNAMIC) return c->hb_thr;   // floor under tau_i
     return full_cutoff();
 }
+
+void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
+                      double cut, const double* psi, const double* diag, cudaStream_t s,
+                      dnq_ham_s* H, double* t_ms);
 
 void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
                const double* psi_in, int n_orb, int policy, int use_hb, double eps1,
@@ -350,6 +394,18 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
 
     H->diag.alloc(nV, s);
     launch_diag(ctx, V.p, nV, H->diag.p, s);
+
+    if (!want_vp && !has_ext && n_orb < 64 && !g_force_walk) {
+        // V->V block only: match rows against V's string groups.
+        T.mark();
+        T.fill(H->t_ms);   // [0] maps + diagonal
+        build_vv_strings(ctx, V.p, nV, n_orb, policy, eps1, policy_cut(ctx, policy, use_hb, eps1),
+                         psi.p, H->diag.p, s, H, H->t_ms);
+        H->n_p = 0;
+        H->t_ms[6] = H->t_ms[0] + H->t_ms[1] + H->t_ms[2] + H->t_ms[3];
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
 
     BuildParams P{};
     P.C = ctx->view();
@@ -677,6 +733,13 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
     DNQ_API_END
 }
 
+int dnq_set_option(int option, int64_t value) {
+    DNQ_API_BEGIN
+    require(option == 1, DNQ_ERR_INVALID, "unknown option");
+    g_force_walk = value != 0;
+    DNQ_API_END
+}
+
 int dnq_ham_timings(dnq_ham_t h, double* ms8) {
     DNQ_API_BEGIN
     require(h && ms8, DNQ_ERR_INVALID, "null argument");
@@ -765,6 +828,26 @@ int dnq_ham_copy_dets_p(dnq_ham_t h, uint64_t* dets, void* stream) {
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     copy_out(dets, (const uint64_t*)h->dets_p.p, 2 * h->n_p, s);
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    DNQ_API_END
+}
+
+int dnq_ham_p_diag(dnq_ham_t h, dnq_ctx_t ctx, double* out, void* stream) {
+    DNQ_API_BEGIN
+    require(h && ctx, DNQ_ERR_INVALID, "null argument");
+    if (h->n_p == 0) return DNQ_OK;
+    require(out != nullptr, DNQ_ERR_INVALID, "null argument");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool dev_out = is_device_ptr(out);
+    DBuf<double> tmp;
+    double* o = out;
+    if (!dev_out) {
+        tmp.alloc(h->n_p, s);
+        o = tmp.p;
+    }
+    launch_diag(ctx, (const u64*)h->dets_p.p, h->n_p, o, s);
+    if (!dev_out) copy_out(out, o, h->n_p, s);
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_API_END
 }

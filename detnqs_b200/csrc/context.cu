@@ -231,8 +231,19 @@ void upload_tables(dnq_ctx_s* c) {
     DNQ_CUDA(cudaStreamSynchronize(s));
 }
 
+// Keep memory freed by cudaFreeAsync in the device's default pool instead
+// of returning it to the driver at every synchronisation: repeated builds
+// then reuse the same pages (process-local runtime setting).
+void keep_pool(int device) {
+    cudaMemPool_t pool;
+    DNQ_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = ~0ull;
+    DNQ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+}
+
 void init_ctx(dnq_ctx_s* c) {
     DeviceGuard g(c->device);
+    keep_pool(c->device);
     upload_tables(c);
     // Table holding every entry that can yield a kept element (|v| >= 1e-15
     // covers the strict "> 1e-15" test of unscreened doubles).

@@ -30,7 +30,8 @@ struct dnq_ham_s {
     dnq::Csr vv, vp;
     dnq::Csr pv;                      // transpose of vp, built on first use
     bool pv_ready = false;
-    dnq::DBuf<double> diag;           // H_ii of V (0 when dropped)
+    dnq::DBuf<double> diag;           // H_ii of V as evaluated (Slater-Condon)
+    dnq::DBuf<double> diag_op;        // diagonal entries stored in vv (0 if dropped)
     dnq::DBuf<float> x32;             // FP32 scratch for the FP32 operator
     dnq::DBuf<unsigned long long> dets_p;   // (alpha, beta) pairs
     dnq::i64 candidates = 0;
@@ -39,13 +40,14 @@ struct dnq_ham_s {
     // [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total
     double t_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     size_t bytes() const {
-        return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + x32.bytes() + dets_p.bytes();
+        return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + diag_op.bytes() + x32.bytes() + dets_p.bytes();
     }
 };
 
 namespace dnq {
 // Segmented sort of (col, val) pairs inside each CSR row by column.
 void sort_rows(Csr& m, cudaStream_t s);
-// Build the FP32 off-diagonal value copy of a square block.
-void make_f32(Csr& m, cudaStream_t s);
+// FP32 off-diagonal value copy of a square block (diagonal entries zeroed)
+// and, when diag_out is given, the FP64 diagonal entries (0 where absent).
+void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out = nullptr);
 }  // namespace dnq

@@ -349,21 +349,14 @@ void coo_to_csr_dev(const u32* r, const u32* c, const double* v, i64 n, i64 nr, 
 
 }  // namespace
 
-void ham_eff(const u32* vvr, const u32* vvc, const double* vvv, i64 vvn, i64 nv,
-             const u32* vpr, const u32* vpc, const double* vpv, i64 vpn, i64 np,
-             const double* hpp, double e_ref, int sigma, double eps, int precision,
-             int device, cudaStream_t s, dnq_ham_s* H) {
+// Core of the downfolding on canonical CSR blocks (VV: nv x nv, VP: nv x np).
+void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp, double e_ref,
+                 int sigma, double eps, int precision, int device, cudaStream_t s,
+                 dnq_ham_s* H) {
     H->device = device;
     H->stream = s;
     H->n_v = nv;
-    Csr VV, VP, PV;
-    coo_to_csr_dev(vvr, vvc, vvv, vvn, nv, nv, VV, s);
-    if (np == 0) {   // ham_eff.cpp:72-77: H_VV canonicalised
-        H->vv = std::move(VV);
-        DNQ_CUDA(cudaStreamSynchronize(s));
-        return;
-    }
-    coo_to_csr_dev(vpr, vpc, vpv, vpn, nv, np, VP, s);
+    Csr PV;
     transpose_csr(VP, PV, s);
     DBuf<double> dinv(np, s);
     DBuf<u8> skip(np, s);
@@ -454,11 +447,69 @@ void ham_eff(const u32* vvr, const u32* vvc, const double* vvv, i64 vvn, i64 nv,
     DNQ_CUDA(cudaStreamSynchronize(s));
 }
 
+void ham_eff(const u32* vvr, const u32* vvc, const double* vvv, i64 vvn, i64 nv,
+             const u32* vpr, const u32* vpc, const double* vpv, i64 vpn, i64 np,
+             const double* hpp, double e_ref, int sigma, double eps, int precision,
+             int device, cudaStream_t s, dnq_ham_s* H) {
+    H->device = device;
+    H->stream = s;
+    H->n_v = nv;
+    Csr VV, VP;
+    coo_to_csr_dev(vvr, vvc, vvv, vvn, nv, nv, VV, s);
+    if (np == 0) {   // ham_eff.cpp:72-77: H_VV canonicalised
+        H->vv = std::move(VV);
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    coo_to_csr_dev(vpr, vpc, vpv, vpn, nv, np, VP, s);
+    ham_eff_csr(VV, VP, nv, np, hpp, e_ref, sigma, eps, precision, device, s, H);
+}
+
 }  // namespace dnq
 
 using namespace dnq;
 
 extern "C" {
+
+int dnq_ham_eff_from(dnq_ham_t proxy, const double* h_pp, double e_ref, int reg_sigma,
+                     double epsilon, int precision, void* stream, dnq_ham_t* out) {
+    DNQ_API_BEGIN
+    require(proxy && out, DNQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    require(proxy->n_p == 0 || h_pp, DNQ_ERR_INVALID, "null h_pp_diag");
+    DeviceGuard g(proxy->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    std::unique_ptr<dnq_ham_s> H(new dnq_ham_s);
+    if (proxy->n_p == 0 || proxy->vp.nnz == 0 && proxy->n_p == 0) {
+        // empty P: H_eff is H_VV itself
+        Csr copy;
+        copy.nr = copy.nc = proxy->n_v;
+        copy.nnz = proxy->vv.nnz;
+        copy.rowptr.alloc(proxy->n_v + 1, s);
+        copy.col.alloc(copy.nnz, s);
+        copy.val.alloc(copy.nnz, s);
+        DNQ_CUDA(cudaMemcpyAsync(copy.rowptr.p, proxy->vv.rowptr.p, (proxy->n_v + 1) * 8,
+                                 cudaMemcpyDeviceToDevice, s));
+        if (copy.nnz) {
+            DNQ_CUDA(cudaMemcpyAsync(copy.col.p, proxy->vv.col.p, copy.nnz * 4,
+                                     cudaMemcpyDeviceToDevice, s));
+            DNQ_CUDA(cudaMemcpyAsync(copy.val.p, proxy->vv.val.p, copy.nnz * 8,
+                                     cudaMemcpyDeviceToDevice, s));
+        }
+        H->device = proxy->device;
+        H->stream = s;
+        H->n_v = proxy->n_v;
+        H->vv = std::move(copy);
+        DNQ_CUDA(cudaStreamSynchronize(s));
+    } else {
+        DIn<double> hpp(h_pp, proxy->n_p, s);
+        ham_eff_csr(proxy->vv, proxy->vp, proxy->n_v, proxy->n_p, hpp.p, e_ref, reg_sigma,
+                    epsilon, precision, proxy->device, s, H.get());
+    }
+    *out = H.release();
+    DNQ_API_END
+}
 
 int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols, const double* vv_vals,
                 int64_t vv_nnz, int64_t n_v, const uint32_t* vp_rows, const uint32_t* vp_cols,

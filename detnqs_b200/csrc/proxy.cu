@@ -56,12 +56,6 @@ __global__ void k_diag_mul_add(const double* d, const double* x, i64 n, double* 
         y[t] = d[t] * x[t];
 }
 
-__global__ void k_f32_all(const double* v, i64 n, float* o) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
-         t += (i64)gridDim.x * blockDim.x)
-        o[t] = (float)v[t];
-}
-
 int gsz(i64 n) {
     i64 b = (n + 255) / 256;
     return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
@@ -99,17 +93,12 @@ void transpose_csr(const Csr& a, Csr& t, cudaStream_t s) {
 
 }  // namespace dnq
 
-using namespace dnq;
+namespace dnq {
+Csr& pv_block(dnq_ham_s* h, cudaStream_t s);
+void ensure_f32_all(Csr& m, cudaStream_t s);
+}  // namespace dnq
 
-namespace {
-Csr& pv_of(dnq_ham_s* h, cudaStream_t s) {
-    if (!h->pv_ready) {
-        transpose_csr(h->vp, h->pv, s);
-        h->pv_ready = true;
-    }
-    return h->pv;
-}
-}  // namespace
+using namespace dnq;
 
 extern "C" {
 
@@ -128,7 +117,7 @@ int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp, const do
         spmv_block(h, h->vp, xpd.p, tmp.p, nullptr, DNQ_F64, s, nullptr, nullptr);
         spmv_block(h, h->vv, xvd.p, yvd.p, tmp.p, DNQ_F64, s, nullptr, nullptr);
         if (np) {
-            Csr& pv = pv_of(h, s);
+            Csr& pv = pv_block(h, s);
             DBuf<double> dterm(np, s);
             k_diag_mul_add<<<gsz(np), 256, 0, s>>>(dpd.p, xpd.p, np, dterm.p);
             DNQ_CHECK_LAUNCH();
@@ -139,21 +128,14 @@ int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp, const do
         DBuf<float> xv32(nv, s), xp32(np, s);
         to_f32(xvd.p, nv, xv32.p, s);
         to_f32(xpd.p, np, xp32.p, s);
-        if (h->vv.val32.n != (size_t)h->vv.nnz) make_f32(h->vv, s);
-        if (h->vp.val32.n != (size_t)h->vp.nnz) {
-            h->vp.val32.alloc(h->vp.nnz, s);
-            if (h->vp.nnz) k_f32_all<<<gsz(h->vp.nnz), 256, 0, s>>>(h->vp.val.p, h->vp.nnz, h->vp.val32.p);
-            DNQ_CHECK_LAUNCH();
-        }
+        if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
+            make_f32(h->vv, s, &h->diag_op);
+        ensure_f32_all(h->vp, s);
         spmv_block(h, h->vp, xpd.p, tmp.p, nullptr, DNQ_F32, s, xp32.p, nullptr);
-        spmv_block(h, h->vv, xvd.p, yvd.p, tmp.p, DNQ_F32, s, xv32.p, h->diag.p);
+        spmv_block(h, h->vv, xvd.p, yvd.p, tmp.p, DNQ_F32, s, xv32.p, h->diag_op.p);
         if (np) {
-            Csr& pv = pv_of(h, s);
-            if (pv.val32.n != (size_t)pv.nnz) {
-                pv.val32.alloc(pv.nnz, s);
-                if (pv.nnz) k_f32_all<<<gsz(pv.nnz), 256, 0, s>>>(pv.val.p, pv.nnz, pv.val32.p);
-                DNQ_CHECK_LAUNCH();
-            }
+            Csr& pv = pv_block(h, s);
+            ensure_f32_all(pv, s);
             DBuf<double> dterm(np, s);
             k_diag_mul_add<<<gsz(np), 256, 0, s>>>(dpd.p, xpd.p, np, dterm.p);
             DNQ_CHECK_LAUNCH();

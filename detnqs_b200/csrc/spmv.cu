@@ -201,7 +201,6 @@ void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
             case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
             case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
             default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
-            DNQ_CHECK_LAUNCH();
         }
     } else {
         switch (G) {
@@ -209,7 +208,6 @@ void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
             case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
             case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
             default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
-            DNQ_CHECK_LAUNCH();
         }
     }
     DNQ_CHECK_LAUNCH();
@@ -235,9 +233,37 @@ void energy_reduce(const double* x, const double* y, i64 n, double* eloc, double
 // each column.
 void transpose_csr(const Csr& a, Csr& t, cudaStream_t s);
 
+// H_PV (transpose of H_VP), built once per handle.
+Csr& pv_block(dnq_ham_s* h, cudaStream_t s) {
+    if (!h->pv_ready) {
+        transpose_csr(h->vp, h->pv, s);
+        h->pv_ready = true;
+    }
+    return h->pv;
+}
+
+namespace {
+__global__ void k_all_f32(const double* v, i64 n, float* o) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        o[t] = (float)v[t];
+}
+}  // namespace
+
+// FP32 copy of every value of a rectangular block (no diagonal split).
+void ensure_f32_all(Csr& m, cudaStream_t s) {
+    if (m.val32.n == (size_t)m.nnz && m.nnz) return;
+    m.val32.alloc(m.nnz, s);
+    if (m.nnz) {
+        k_all_f32<<<1184, 256, 0, s>>>(m.val.p, m.nnz, m.val32.p);
+        DNQ_CHECK_LAUNCH();
+    }
+}
+
 // Prepare the FP32 operator buffers of the V block.
 void ensure_f32(dnq_ham_s* h, cudaStream_t s) {
-    if (h->vv.val32.n != (size_t)h->vv.nnz || h->vv.nnz == 0) make_f32(h->vv, s);
+    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
+        make_f32(h->vv, s, &h->diag_op);
     if ((i64)h->x32.n < h->n_v) h->x32.alloc(h->n_v, s);
 }
 
@@ -263,7 +289,7 @@ int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision, void* s
     if (precision == DNQ_F32) {
         ensure_f32(h, s);
         to_f32(xd.p, n, h->x32.p, s);
-        spmv_block(h, h->vv, xd.p, yd, nullptr, DNQ_F32, s, h->x32.p, h->diag.p);
+        spmv_block(h, h->vv, xd.p, yd, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
     } else {
         spmv_block(h, h->vv, xd.p, yd, nullptr, DNQ_F64, s, nullptr, nullptr);
     }
@@ -271,6 +297,40 @@ int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision, void* s
         copy_out(y, yd, n, s);
         DNQ_CUDA(cudaStreamSynchronize(s));
     }
+    DNQ_API_END
+}
+
+int dnq_ham_block_spmv(dnq_ham_t h, int block, const double* x, double* y, int precision,
+                       void* stream) {
+    DNQ_API_BEGIN
+    require(h && x && y, DNQ_ERR_INVALID, "null argument");
+    require(block >= 0 && block <= 2, DNQ_ERR_INVALID, "invalid block");
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    if (block == 0) return dnq_ham_spmv(h, x, y, precision, stream);
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const Csr& m = block == 1 ? h->vp : pv_block(h, s);
+    const i64 nin = block == 1 ? h->n_p : h->n_v;
+    const i64 nout = block == 1 ? h->n_v : h->n_p;
+    if (nout == 0) return DNQ_OK;
+    DIn<double> xd(x, nin, s);
+    const bool dev_out = is_device_ptr(y);
+    DBuf<double> ybuf;
+    double* yd = y;
+    if (!dev_out) { ybuf.alloc(nout, s); yd = ybuf.p; }
+    if (m.nnz == 0) {
+        DNQ_CUDA(cudaMemsetAsync(yd, 0, nout * 8, s));
+    } else if (precision == DNQ_F32) {
+        Csr& mm = const_cast<Csr&>(m);
+        ensure_f32_all(mm, s);
+        DBuf<float> x32(nin, s);
+        to_f32(xd.p, nin, x32.p, s);
+        spmv_block(h, mm, xd.p, yd, nullptr, DNQ_F32, s, x32.p, nullptr);
+    } else {
+        spmv_block(h, m, xd.p, yd, nullptr, DNQ_F64, s, nullptr, nullptr);
+    }
+    if (!dev_out) copy_out(y, yd, nout, s);
+    DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_API_END
 }
 
@@ -293,7 +353,7 @@ int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc, double* out
     if (precision == DNQ_F32) {
         ensure_f32(h, s);
         to_f32(xd.p, n, h->x32.p, s);
-        spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F32, s, h->x32.p, h->diag.p);
+        spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
     } else {
         spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F64, s, nullptr, nullptr);
     }

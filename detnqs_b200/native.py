@@ -39,10 +39,12 @@ EXPORTS = (
     "dnq_ctx_create", "dnq_ctx_create_fcidump", "dnq_ctx_destroy", "dnq_ctx_e_nuc",
     "dnq_ctx_device_bytes", "dnq_hb_prepare", "dnq_hb_clear", "dnq_hb_row",
     "dnq_ham_diag", "dnq_ham_elems", "dnq_excitations",
-    "dnq_build", "dnq_ham_destroy", "dnq_ham_info", "dnq_ham_timings", "dnq_ham_copy_coo",
+    "dnq_build", "dnq_set_option", "dnq_ham_destroy", "dnq_ham_info", "dnq_ham_timings", "dnq_ham_copy_coo",
     "dnq_ham_copy_csr", "dnq_ham_copy_dets_p", "dnq_ham_copy_diag",
     "dnq_ham_spmv", "dnq_ham_proxy_spmv", "dnq_ham_local_energy",
-    "dnq_variational_energy", "dnq_ham_eff",
+    "dnq_variational_energy", "dnq_ham_eff", "dnq_ham_eff_from", "dnq_ham_p_diag",
+    "dnq_ham_block_spmv", "dnq_gen_dets", "dnq_local_connections", "dnq_conn_copy",
+    "dnq_pt2",
 )
 
 
@@ -94,6 +96,7 @@ _sig("dnq_ham_elems", _P, _P, _P, _I64, _P, _P)
 _sig("dnq_excitations", _P, _P, _I64, _P, _P, _I, _P)
 _sig("dnq_build", _P, _P, _I64, _P, _I64, _P, _I, _I, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_ham_destroy", _P)
+_sig("dnq_set_option", _I, _I64)
 _sig("dnq_ham_info", _P, _P)
 _sig("dnq_ham_timings", _P, _P)
 _sig("dnq_ham_copy_coo", _P, _I, _P, _P, _P, _P)
@@ -103,6 +106,13 @@ _sig("dnq_ham_copy_diag", _P, _P, _P)
 _sig("dnq_ham_spmv", _P, _P, _P, _I, _P)
 _sig("dnq_ham_proxy_spmv", _P, _P, _P, _P, _P, _P, _I, _P)
 _sig("dnq_ham_local_energy", _P, _P, _P, _P, _I, _P)
+_sig("dnq_ham_block_spmv", _P, _I, _P, _P, _I, _P)
+_sig("dnq_ham_p_diag", _P, _P, _P, _P)
+_sig("dnq_gen_dets", _P, _P, _I64, _I, _P, _I, _D, _I, _P, C.POINTER(_P))
+_sig("dnq_local_connections", _P, _P, _I64, _I, _I, _D, _P, C.POINTER(_P))
+_sig("dnq_conn_copy", _P, _P, _P, _P, _P)
+_sig("dnq_pt2", _P, _P, _I64, _P, _I, _D, _I, _D, _P, _P)
+_sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_variational_energy", _P, _P, _I64, _P, _I, _I, _D, C.POINTER(_D), _P)
 _sig("dnq_ham_eff", _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _D, _I, _D, _I, _I,
      _P, C.POINTER(_P))

@@ -107,6 +107,12 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V,
               int n_orb, int policy, int use_heatbath, double eps1,
               int want_vp, void* stream, dnq_ham_t* out);
 int dnq_ham_destroy(dnq_ham_t h);
+/* Library options (no reference counterpart).  DNQ_OPT_FORCE_WALK = 1:
+ * value 1 routes V->V-only builds through the per-row candidate walk
+ * instead of the string-group matcher (both give identical blocks; used by
+ * tests to cross-check the two). */
+enum { DNQ_OPT_FORCE_WALK = 1 };
+int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */
 int dnq_ham_info(dnq_ham_t h, int64_t* info6);
@@ -124,6 +130,9 @@ int dnq_ham_copy_csr(dnq_ham_t h, int block, int64_t* row_ptr, uint32_t* cols,
                      double* vals, void* stream);
 int dnq_ham_copy_dets_p(dnq_ham_t h, uint64_t* dets, void* stream);
 int dnq_ham_copy_diag(dnq_ham_t h, double* diag, void* stream);
+/* <x|H|x> of the P determinants held by h, computed on the device
+ * (get_ham_diag(det_P), hamiltonian.py:202-206). */
+int dnq_ham_p_diag(dnq_ham_t h, dnq_ctx_t ctx, double* out, void* stream);
 
 /* ---- H.psi / local energy -------------------------------------------------
  * Replaces the SciPy CSR matvec of detnqs/operator/kernel.py:75-78
@@ -138,6 +147,10 @@ int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision,
 int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp,
                        const double* diag_p, double* yv, double* yp,
                        int precision, void* stream);
+/* One block: 0 -> y = H_VV x, 1 -> y = H_VP x, 2 -> y = H_PV x
+ * (the H_VP.dot / H_PV.dot calls of kernel.py:132-133). */
+int dnq_ham_block_spmv(dnq_ham_t h, int block, const double* x, double* y,
+                       int precision, void* stream);
 /* Rayleigh quotient and local energies from one y = H x pass:
  * out2 = {x.Hx, x.x} (compensated FP64 sums); eloc[i] = y_i / x_i
  * (NULL to skip). */
@@ -150,12 +163,47 @@ int dnq_variational_energy(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
                            const double* coeffs, int n_orb, int use_heatbath,
                            double eps1, double* out, void* stream);
 
+/* ---- determinant-space generators ----------------------------------------
+ * mode -1: gen_connected_dets (det_space.cpp:167-213 + canonicalize): all
+ *          singles and doubles of dets, sorted and unique; ctx may be NULL.
+ * mode  0: gen_perturbative_dets(mode="none") (det_space.cpp:233-255):
+ *          the same minus dets.
+ * mode  1: "static"  (ham_utils.cpp:546-701): singles with |h| > 1e-15,
+ *          heat-bath doubles with w >= eps1, minus dets.
+ * mode  2: "dynamic": singles also need |h psi_i| >= eps1, doubles
+ *          w >= eps1 / max(|psi_i|, 1e-12).
+ * The sorted result is held by *out: read its size with dnq_ham_info
+ * (info[2]) and copy it with dnq_ham_copy_dets_p. */
+int dnq_gen_dets(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, int n_orb,
+                 const double* psi, int mode, double eps1, int device,
+                 void* stream, dnq_ham_t* out);
+/* get_local_connections (local_conn.cpp:96-142; bridge.cpp:635-677): per
+ * row the diagonal, singles above max(eps1,1e-15) (heat-bath) or 1e-15,
+ * doubles above 1e-15.  Sizes via dnq_ham_info (info[2] = total entries),
+ * copy with dnq_conn_copy (offsets int32[n+1], dets, values). */
+int dnq_local_connections(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
+                          int n_orb, int use_heatbath, double eps1,
+                          void* stream, dnq_ham_t* out);
+int dnq_conn_copy(dnq_ham_t h, int32_t* offsets, uint64_t* dets,
+                  double* values, void* stream);
+/* compute_pt2 (local_conn.cpp:247-418): out3 = {e_pt2_internal,
+ * e_pt2_external, n_ext}. */
+int dnq_pt2(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
+            const double* coeffs, int n_orb, double e_ref, int use_heatbath,
+            double eps1, double* out3, void* stream);
+
 /* ---- downfolding -----------------------------------------------------------
  * get_ham_eff (ham_eff.cpp:64-233): H_eff = H_VV + H_VP D^-1 H_PV with
  * D_k = e_ref - h_pp[k]; reg_sigma 1 -> d/(d^2+eps^2), 0 -> 1/(d+sgn(d)eps).
  * Inputs are COO triplets (any order, duplicates summed).  precision
  * DNQ_F32 stores H_VP values in FP32 and accumulates each output element
  * with two-sum compensation; D^-1 stays FP64. */
+/* Same downfolding from the V and P blocks of a device-resident proxy
+ * build (build_effective_hamiltonian, hamiltonian.py:215-281), without
+ * copying them to the host.  Returns a new handle holding H_eff. */
+int dnq_ham_eff_from(dnq_ham_t proxy, const double* h_pp, double e_ref,
+                     int reg_sigma, double epsilon, int precision,
+                     void* stream, dnq_ham_t* out);
 int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols,
                 const double* vv_vals, int64_t vv_nnz, int64_t n_v,
                 const uint32_t* vp_rows, const uint32_t* vp_cols,
