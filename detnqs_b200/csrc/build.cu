@@ -402,7 +402,7 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
         build_vv_strings(ctx, V.p, nV, n_orb, policy, eps1, policy_cut(ctx, policy, use_hb, eps1),
                          psi.p, H->diag.p, s, H, H->t_ms);
         H->n_p = 0;
-        H->t_ms[6] = H->t_ms[0] + H->t_ms[1] + H->t_ms[2] + H->t_ms[3];
+        H->t_ms[6] = H->t_ms[0] + H->t_ms[1] + H->t_ms[2] + H->t_ms[3] + H->t_ms[4];
         DNQ_CUDA(cudaStreamSynchronize(s));
         return;
     }

@@ -77,19 +77,51 @@ __device__ __forceinline__ Dot2<T> shfl_xor(const Dot2<T>& d, int o, unsigned ma
     return r;
 }
 
-// One group of G lanes per row; G in {4, 8, 16, 32}.
+// One group of G lanes per row (G in {4, 8, 16, 32}); each lane reads 4
+// consecutive entries per step with 128-bit loads (cols: one uint4; values:
+// two double2 / one float4), starting from the row start rounded down to a
+// multiple of 4 and masking entries outside the row, so a warp streams 128
+// entries per step.  The tail of the arrays is read with scalar loads.
 template <int G>
-__global__ void k_spmv_f64(const i64* __restrict__ rp, const u32* __restrict__ col,
-                           const double* __restrict__ val, const double* __restrict__ x,
-                           i64 nr, double* __restrict__ y, const double* __restrict__ yadd) {
+__global__ void __launch_bounds__(256)
+k_spmv_f64(const i64* __restrict__ rp, const u32* __restrict__ col,
+           const double* __restrict__ val, const double* __restrict__ x, i64 nr, i64 nnz,
+           double* __restrict__ y, const double* __restrict__ yadd) {
     const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
     const int sub = threadIdx.x & (G - 1);
     const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
-    for (i64 r = gid; r < nr + (ngroups - nr % ngroups) % ngroups; r += ngroups) {
+    const i64 rounds = (nr + ngroups - 1) / ngroups;
+    for (i64 it = 0; it < rounds; ++it) {
+        const i64 r = gid + it * ngroups;
         double acc = 0.0;
         if (r < nr) {
             const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-            for (i64 k = b + sub; k < e; k += G) acc += __ldg(&val[k]) * __ldg(&x[__ldg(&col[k])]);
+            for (i64 k = (b & ~3ll) + 4 * sub; k < e; k += 4 * G) {
+                u32 c[4];
+                double v[4];
+                if (k + 3 < nnz) {
+                    const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + k));
+                    const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + k));
+                    const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + k + 2));
+                    c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
+                    v[0] = v01.x; v[1] = v01.y; v[2] = v23.x; v[3] = v23.y;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        c[q] = k + q < nnz ? __ldg(&col[k + q]) : 0u;
+                        v[q] = k + q < nnz ? __ldg(&val[k + q]) : 0.0;
+                    }
+                }
+                double xv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const bool in = k + q >= b && k + q < e;
+                    xv[q] = in ? __ldg(&x[c[q]]) : 0.0;
+                    if (!in) v[q] = 0.0;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc = fma(v[q], xv[q], acc);
+            }
         }
 #pragma unroll
         for (int o = G / 2; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -98,18 +130,45 @@ __global__ void k_spmv_f64(const i64* __restrict__ rp, const u32* __restrict__ c
 }
 
 template <int G>
-__global__ void k_spmv_f32c(const i64* __restrict__ rp, const u32* __restrict__ col,
-                            const float* __restrict__ val, const float* __restrict__ x32,
-                            const double* __restrict__ diag, const double* __restrict__ x,
-                            i64 nr, double* __restrict__ y, const double* __restrict__ yadd) {
+__global__ void __launch_bounds__(256)
+k_spmv_f32c(const i64* __restrict__ rp, const u32* __restrict__ col,
+            const float* __restrict__ val, const float* __restrict__ x32,
+            const double* __restrict__ diag, const double* __restrict__ x, i64 nr, i64 nnz,
+            double* __restrict__ y, const double* __restrict__ yadd) {
     const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
     const int sub = threadIdx.x & (G - 1);
     const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
-    for (i64 r = gid; r < nr + (ngroups - nr % ngroups) % ngroups; r += ngroups) {
+    const i64 rounds = (nr + ngroups - 1) / ngroups;
+    for (i64 it = 0; it < rounds; ++it) {
+        const i64 r = gid + it * ngroups;
         Dot2<float> acc;
         if (r < nr) {
             const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-            for (i64 k = b + sub; k < e; k += G) acc.add_prod(__ldg(&val[k]), __ldg(&x32[__ldg(&col[k])]));
+            for (i64 k = (b & ~3ll) + 4 * sub; k < e; k += 4 * G) {
+                u32 c[4];
+                float v[4];
+                if (k + 3 < nnz) {
+                    const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + k));
+                    const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + k));
+                    c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
+                    v[0] = v4.x; v[1] = v4.y; v[2] = v4.z; v[3] = v4.w;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        c[q] = k + q < nnz ? __ldg(&col[k + q]) : 0u;
+                        v[q] = k + q < nnz ? __ldg(&val[k + q]) : 0.0f;
+                    }
+                }
+                float xv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const bool in = k + q >= b && k + q < e;
+                    xv[q] = in ? __ldg(&x32[c[q]]) : 0.0f;
+                    if (!in) v[q] = 0.0f;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc.add_prod(v[q], xv[q]);
+            }
         }
 #pragma unroll
         for (int o = G / 2; o; o >>= 1) acc.merge(shfl_xor(acc, o, 0xffffffffu));
@@ -178,9 +237,9 @@ __global__ void k_energy_final(const double* part, int nb, double* out2) {
 
 int group_for(const Csr& m) {
     const double avg = m.nr ? (double)m.nnz / (double)m.nr : 0.0;
-    if (avg >= 48) return 32;
-    if (avg >= 20) return 16;
-    if (avg >= 8) return 8;
+    if (avg >= 96) return 32;
+    if (avg >= 48) return 16;
+    if (avg >= 24) return 8;
     return 4;
 }
 
@@ -197,17 +256,17 @@ void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
     const int grid = spmv_grid(h->device), bs = 256;
     if (precision == DNQ_F64 || m.nnz == 0) {
         switch (G) {
-            case 32: k_spmv_f64<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
-            case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
-            case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
-            default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, y, yadd); break;
+            case 32: k_spmv_f64<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
+            case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
+            case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
+            default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
         }
     } else {
         switch (G) {
-            case 32: k_spmv_f32c<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
-            case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
-            case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
-            default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, y, yadd); break;
+            case 32: k_spmv_f32c<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
+            case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
+            case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
+            default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
         }
     }
     DNQ_CHECK_LAUNCH();

@@ -439,7 +439,7 @@ void launch_diag(const dnq_ctx_s* c, const u64* d, i64 n, double* out, cudaStrea
 void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                       double cut, const double* psi, const double* diag, cudaStream_t s,
                       dnq_ham_s* H, double* t_ms) {
-    cudaEvent_t ev[5];
+    cudaEvent_t ev[6];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
     StrIndex A, B;
@@ -502,7 +502,8 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     DNQ_CHECK_LAUNCH();
     DNQ_CUDA(cudaEventRecord(ev[4], s));
     sort_rows(H->vv, s);
-    DNQ_CUDA(cudaEventSynchronize(ev[4]));
+    DNQ_CUDA(cudaEventRecord(ev[5], s));
+    DNQ_CUDA(cudaEventSynchronize(ev[5]));
     float ms;
     DNQ_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
     t_ms[0] += ms;
@@ -512,6 +513,8 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     t_ms[2] = ms;
     DNQ_CUDA(cudaEventElapsedTime(&ms, ev[3], ev[4]));
     t_ms[3] = ms;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[4], ev[5]));
+    t_ms[4] = ms;
     for (auto& e : ev) cudaEventDestroy(e);
 }
 
