@@ -48,15 +48,16 @@ CACHE = os.path.join(tempfile.gettempdir(), "detnqs_b200_bench")
 
 def workload(rank: int, n_dets: int):
     from detnqs_b200 import synthetic as S
-    sysm = S.make_system(N_ORB, N_ALPHA, N_BETA, N_CHOL, INT_SEED + rank)
+    si, sd, sp = rank_seeds(rank)
+    sysm = S.make_system(N_ORB, N_ALPHA, N_BETA, N_CHOL, si)
     os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, f"dets_{N_ORB}_{n_dets}_{DET_SEED + rank}_{INT_SEED + rank}.npy")
+    path = os.path.join(CACHE, f"dets_{N_ORB}_{n_dets}_{sd}_{si}.npy")
     if os.path.exists(path):
         V = np.load(path)
     else:
-        V = S.heat_bath_sample(sysm, n_dets, DET_SEED + rank)
+        V = S.heat_bath_sample(sysm, n_dets, sd)
         np.save(path, V)
-    psi = S.normalized_psi(n_dets, PSI_SEED + rank)
+    psi = S.normalized_psi(n_dets, sp)
     return sysm, V, psi
 
 
@@ -111,6 +112,24 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank timing over all ranks (all_reduce MAX); identity
+    when running alone.  `device` is the tensor device of the process
+    group's backend (cuda for NCCL, cpu for gloo)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seeds(rank: int):
+    """(integral, determinant, psi) seeds of a rank: every rank gets its own
+    system of the same size (weak scaling)."""
+    return INT_SEED + rank, DET_SEED + rank, PSI_SEED + rank
 
 
 def measured_peaks():
@@ -257,11 +276,7 @@ def run_ours(args, rank: int, world: int):
             H.close()
     clocks = clk.stop()
     launches = (native.lib.dnq_launch_count() - launches0) // args.steps
-    ms_step = float(np.mean(t_steps))
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = max_over_ranks(float(np.mean(t_steps)), world, dev)
 
     # ---- steady state of the inner loop: repeated H.psi on the resident H
     ss = {}
@@ -300,11 +315,7 @@ def run_ours(args, rank: int, world: int):
         torch.cuda.synchronize()
         e2e.append(a.elapsed_time(b))
         H.close()
-    e2e_ms = float(np.mean(e2e))
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), world, dev)
 
     peak, peak_kind = measured_peaks()
     fill_ms = float(np.mean(t_fill))
