@@ -288,6 +288,16 @@ void energy_reduce(const double* x, const double* y, i64 n, double* eloc, double
     DNQ_CHECK_LAUNCH();
 }
 
+// Same reduction with caller-provided partials (4 * nb doubles) and result
+// slot: launches only, allocates nothing.
+void energy_reduce_into(const double* x, const double* y, i64 n, double* eloc, double* part,
+                        int nb, double* out2_dev, cudaStream_t s) {
+    k_energy_partials<<<nb, 256, 0, s>>>(x, y, n, eloc, part);
+    DNQ_CHECK_LAUNCH();
+    k_energy_final<<<1, 32, 0, s>>>(part, nb, out2_dev);
+    DNQ_CHECK_LAUNCH();
+}
+
 // Transposed copy of a CSR block (H_PV from H_VP), rows ascending inside
 // each column.
 void transpose_csr(const Csr& a, Csr& t, cudaStream_t s);

@@ -157,6 +157,21 @@ int dnq_ham_block_spmv(dnq_ham_t h, int block, const double* x, double* y,
 int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc,
                          double* out2, int precision, void* stream);
 
+/* Same result as dnq_ham_local_energy without allocating device memory.
+ * No counterpart in the reference: it serves callers that may not allocate
+ * on their own -- an XLA custom call (JAX FFI) that runs inside XLA's memory
+ * plan, or an application that gives the library a fixed budget.  Its
+ * scratch (FP32 copy of x, reduction partials) is a file-scope device array
+ * of 4 MiB + 74 KiB that every GPU loading the library holds until exit, so
+ * n_V is limited to 1048576 (larger handles are rejected).  x and eloc must
+ * be device memory; eloc first receives H x and then y_i / x_i.  DNQ_F32
+ * needs the handle's FP32 values to exist (one earlier FP32 call).  The
+ * first call on a device sets up the scratch address with that device
+ * current: make it before any stream capture.  All calls share the scratch:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+int dnq_ham_local_energy_noalloc(dnq_ham_t h, const double* x, double* eloc,
+                                 double* out2, int precision, void* stream);
+
 /* ---- matrix-free contractions (csrc/src/hamiltonian/local_conn.cpp) ------ */
 /* compute_variational_energy (local_conn.cpp:148-229). */
 int dnq_variational_energy(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
