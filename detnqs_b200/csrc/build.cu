@@ -236,23 +236,30 @@ __global__ void k_val_f32_tail(const double* v, i64 n, float* o) {
     if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) o[n - 1] = (float)v[n - 1];
 }
 
-// Diagonal entry of each (column-sorted) row: moved out of the FP32 copy
-// into the FP64 vector (0 when the row has none).
+// Diagonal entry of each row (column order not assumed): moved out of the
+// FP32 copy into the FP64 vector (0 when the row has none).  Warp per row.
 __global__ void k_split_diag(const i64* rowptr, const u32* col, const double* val, i64 nr,
                              float* out, double* dout) {
-    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
-         r += (i64)gridDim.x * blockDim.x) {
-        i64 lo = rowptr[r], hi = rowptr[r + 1];
-        while (lo < hi) {
-            const i64 mid = (lo + hi) >> 1;
-            if (col[mid] < (u32)r) lo = mid + 1; else hi = mid;
-        }
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    for (i64 r = gw; r < nr; r += nw) {
+        const i64 b = rowptr[r], e = rowptr[r + 1];
         double d = 0.0;
-        if (lo < rowptr[r + 1] && col[lo] == (u32)r) {
-            d = val[lo];
-            out[lo] = 0.0f;
+        for (i64 k0 = b; k0 < e; k0 += 32) {
+            const i64 k = k0 + lane;
+            const bool on = k < e && col[k] == (u32)r;
+            if (on) {
+                d = val[k];
+                out[k] = 0.0f;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (m) {
+                d = __shfl_sync(0xffffffffu, d, __ffs(m) - 1);
+                break;
+            }
         }
-        if (dout) dout[r] = d;
+        if (dout && lane == 0) dout[r] = d;
     }
 }
 
@@ -280,7 +287,13 @@ i64 read_i64(const i64* d, cudaStream_t s) {
 
 }  // namespace
 
+void ensure_sorted(Csr& m, cudaStream_t s) {
+    if (!m.sorted) sort_rows(m, s);
+}
+
 void sort_rows(Csr& m, cudaStream_t s) {
+    m.sorted = true;
+    m.val32.release();   // an FP32 copy follows the old order: rebuilt on next use
     if (m.nnz == 0 || m.nr == 0) return;
     require(m.nnz < (i64)0x7fffffff, DNQ_ERR_OVERFLOW,
             "block has more than 2^31-1 entries for the segmented sort");
@@ -311,8 +324,12 @@ void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out) {
         k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, m.nnz, m.val32.p);
         DNQ_CHECK_LAUNCH();
     }
-    k_split_diag<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr, m.val32.p,
-                                                diag_out ? diag_out->p : nullptr);
+    {
+        int dev = 0;
+        DNQ_CUDA(cudaGetDevice(&dev));
+        k_split_diag<<<sm_count(dev) * 8, 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr,
+                                                       m.val32.p, diag_out ? diag_out->p : nullptr);
+    }
     DNQ_CHECK_LAUNCH();
 }
 
@@ -363,6 +380,8 @@ struct PhaseTimer {
 // Testing switch: route V->V-only builds through the candidate walk too
 // (dnq_set_option(DNQ_OPT_FORCE_WALK, 1)); both paths give identical blocks.
 bool g_force_walk = false;
+extern i64 g_arena_chunk;
+extern i64 g_arena_cap;
 
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
@@ -735,8 +754,11 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
 
 int dnq_set_option(int option, int64_t value) {
     DNQ_API_BEGIN
-    require(option == 1, DNQ_ERR_INVALID, "unknown option");
-    g_force_walk = value != 0;
+    require(option >= 1 && option <= 3, DNQ_ERR_INVALID, "unknown option");
+    require(value >= 0, DNQ_ERR_INVALID, "option value must be >= 0");
+    if (option == 1) g_force_walk = value != 0;
+    if (option == 2) g_arena_chunk = value;
+    if (option == 3) g_arena_cap = value;
     DNQ_API_END
 }
 
@@ -789,8 +811,9 @@ int dnq_ham_copy_coo(dnq_ham_t h, int block, uint32_t* rows, uint32_t* cols, dou
     require(h != nullptr && (block == 0 || block == 1), DNQ_ERR_INVALID, "invalid block");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
-    const Csr& m = block == 0 ? h->vv : h->vp;
+    Csr& m = block == 0 ? h->vv : h->vp;
     if (m.nnz == 0) return DNQ_OK;
+    ensure_sorted(m, s);
     if (rows) {
         DBuf<u32> r(m.nnz, s);
         k_expand_rows<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.nr, r.p);
@@ -810,7 +833,8 @@ int dnq_ham_copy_csr(dnq_ham_t h, int block, int64_t* row_ptr, uint32_t* cols, d
     require(h != nullptr && (block == 0 || block == 1), DNQ_ERR_INVALID, "invalid block");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
-    const Csr& m = block == 0 ? h->vv : h->vp;
+    Csr& m = block == 0 ? h->vv : h->vp;
+    ensure_sorted(m, s);
     if (m.nr > 0) copy_out(row_ptr, m.rowptr.p, m.nr + 1, s);
     else if (row_ptr) {
         const int64_t z = 0;

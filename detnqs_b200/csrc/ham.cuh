@@ -16,6 +16,7 @@ struct Csr {
     DBuf<double> val;
     DBuf<float> val32;   // optional FP32 off-diagonal copy
     i64 nr = 0, nc = 0, nnz = 0;
+    bool sorted = true;   // columns ascending inside each row
     size_t bytes() const {
         return rowptr.bytes() + col.bytes() + val.bytes() + val32.bytes();
     }
@@ -47,6 +48,8 @@ struct dnq_ham_s {
 namespace dnq {
 // Segmented sort of (col, val) pairs inside each CSR row by column.
 void sort_rows(Csr& m, cudaStream_t s);
+// sort_rows unless the block is already sorted.
+void ensure_sorted(Csr& m, cudaStream_t s);
 // FP32 off-diagonal value copy of a square block (diagonal entries zeroed)
 // and, when diag_out is given, the FP64 diagonal entries (0 where absent).
 void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out = nullptr);

@@ -107,11 +107,17 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V,
               int n_orb, int policy, int use_heatbath, double eps1,
               int want_vp, void* stream, dnq_ham_t* out);
 int dnq_ham_destroy(dnq_ham_t h);
-/* Library options (no reference counterpart).  DNQ_OPT_FORCE_WALK = 1:
- * value 1 routes V->V-only builds through the per-row candidate walk
- * instead of the string-group matcher (both give identical blocks; used by
- * tests to cross-check the two). */
-enum { DNQ_OPT_FORCE_WALK = 1 };
+/* Library options (no reference counterpart; used by tests to reach every
+ * code path with small inputs):
+ *   DNQ_OPT_FORCE_WALK  1: route V->V-only builds through the per-row
+ *                          candidate walk instead of the string-group
+ *                          matcher (both give identical blocks);
+ *   DNQ_OPT_ARENA_CHUNK n: entries per warp chunk of the single-pass V->V
+ *                          build (0 = default 8192);
+ *   DNQ_OPT_ARENA_CAP   n: arena capacity in entries (0 = automatic); a
+ *                          too-small arena falls back to an exact two-pass
+ *                          build. */
+enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */

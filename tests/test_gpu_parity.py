@@ -359,3 +359,33 @@ def test_string_groups_match_candidate_walk(core, policy, use_hb, eps):
     assert_coo_equal(A.to_coo(0), B.to_coo(0))
     A.close()
     B.close()
+
+
+@pytest.mark.parametrize("chunk,cap", [(64, 0), (512, 0), (0, 5000)])
+def test_arena_paths_match(core, chunk, cap):
+    """Small warp chunks force row restarts and the long-row pass; a tiny
+    arena forces the exact two-pass fallback.  All give the same block."""
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(18, 6, 6, 36, 23)
+    V = S.heat_bath_sample(sysm, 12000, 3)
+    ctx = core.IntCtx.from_arrays(18, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    kw = dict(n_orb=18, policy=1, use_heatbath=True, eps1=1e-7, want_vp=False)
+    A = D.build(ctx, V, **kw)
+    N.check(N.lib.dnq_set_option(2, chunk))
+    N.check(N.lib.dnq_set_option(3, cap))
+    try:
+        ctx2 = core.IntCtx.from_arrays(18, sysm.h1e, sysm.eri, sysm.e_core)
+        ctx2.hb_prepare(1e-15)
+        B = D.build(ctx2, V, **kw)
+    finally:
+        N.check(N.lib.dnq_set_option(2, 0))
+        N.check(N.lib.dnq_set_option(3, 0))
+    assert_coo_equal(A.to_coo(0), B.to_coo(0))
+    # H.psi agrees with the sorted copy
+    x = S.normalized_psi(len(V), 1)
+    ref = A.to_scipy(0).dot(x)
+    np.testing.assert_allclose(B.spmv(x), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    A.close()
+    B.close()
