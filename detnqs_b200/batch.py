@@ -1,0 +1,215 @@
+"""Batched engine: many systems of uneven size in one launch per phase.
+
+A :class:`Batch` holds, for every system, its integral context and its
+determinant space; one :meth:`Batch.step` rebuilds every screened H_VV
+(same rules and bit-identical results as the single-system build), applies
+H to the concatenated amplitudes and returns per-system Rayleigh quotients
+and local energies.  With ``graph=True`` the whole step is replayed from a
+captured CUDA graph.  :func:`autotune` picks the kernel tunables for a
+workload and caches the choice by workload signature.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native as N
+from . import synthetic as S
+
+
+class Batch:
+    def __init__(self, ctxs, dets_list, n_orbs, *, policy: int = N.POLICY_STATIC,
+                 use_heatbath: bool = True, eps1: float = 1e-7, device: int = 0, stream=None):
+        self.n_sys = len(ctxs)
+        if not (len(dets_list) == len(n_orbs) == self.n_sys):
+            raise ValueError("one determinant array and n_orb per context")
+        self._dets = [np.ascontiguousarray(d, dtype=np.uint64) for d in dets_list]
+        ptrs = (C.c_void_p * self.n_sys)(*[d.ctypes.data for d in self._dets])
+        hs = (C.c_void_p * self.n_sys)(*[c.handle.value for c in ctxs])
+        nd = np.array([len(d) for d in self._dets], np.int64)
+        no = np.array(n_orbs, np.int32)
+        h = C.c_void_p()
+        N.check(N.lib.dnq_batch_create(self.n_sys, hs, ptrs, nd.ctypes.data, no.ctypes.data,
+                                       int(policy), int(bool(use_heatbath)), float(eps1),
+                                       int(device), stream, C.byref(h)))
+        self._h = h
+        self._ctxs = list(ctxs)            # keep contexts alive
+        self.offsets = np.concatenate([[0], np.cumsum(nd)])
+        info = np.zeros(4, np.int64)
+        N.check(N.lib.dnq_batch_info(self._h, info.ctypes.data))
+        self.total, self.nnz, self.device_bytes = int(info[1]), int(info[2]), int(info[3])
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            N.check(N.lib.dnq_batch_destroy(self._h))
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def config(self):
+        c = np.zeros(3, np.int64)
+        N.check(N.lib.dnq_batch_get_config(self._h, c.ctypes.data))
+        return tuple(int(x) for x in c)
+
+    @config.setter
+    def config(self, cfg):
+        c = np.asarray(cfg, np.int64)
+        N.check(N.lib.dnq_batch_set_config(self._h, c.ctypes.data))
+
+    def step(self, psi, *, precision: int = N.F32, graph: bool = False, stream=None,
+             eloc=None):
+        """One batched step.  Returns (energies[n_sys, 2], device ms)."""
+        p = psi if hasattr(psi, "data_ptr") else np.ascontiguousarray(psi, np.float64)
+        e2 = np.zeros((self.n_sys, 2))
+        ms = C.c_double()
+        if graph and stream is None:
+            stream = _side_stream()
+        N.check(N.lib.dnq_batch_step(self._h, N.ptr(p), N.ptr(eloc), e2.ctypes.data,
+                                     int(precision), int(bool(graph)), stream, C.byref(ms)))
+        return e2, ms.value
+
+    def coo(self, k: int) -> dict:
+        nnz = C.c_int64()
+        N.check(N.lib.dnq_batch_copy_coo(self._h, k, None, None, None, C.byref(nnz)))
+        r = np.empty(nnz.value, np.uint32)
+        c = np.empty(nnz.value, np.uint32)
+        v = np.empty(nnz.value, np.float64)
+        N.check(N.lib.dnq_batch_copy_coo(self._h, k, r.ctypes.data, c.ctypes.data, v.ctypes.data,
+                                         C.byref(nnz)))
+        n = len(self._dets[k])
+        return {"row": r, "col": c, "val": v, "shape": (n, n)}
+
+
+_STREAM = None
+
+
+def _side_stream():
+    """A non-default stream for graph capture (the legacy stream cannot be
+    captured)."""
+    global _STREAM
+    if _STREAM is None:
+        import torch
+        _STREAM = torch.cuda.Stream()
+    return _STREAM.cuda_stream
+
+
+# ---------------------------------------------------------------------------
+# Autotuner
+# ---------------------------------------------------------------------------
+
+CHUNKS = (2048, 8192, 32768)
+GROUPS = (512, 2048, 8192)
+LANES = (0, 8, 16, 32)
+
+
+def signature(batch: Batch) -> str:
+    """Workload key: size class of the batch (rows, nnz per row)."""
+    rows = batch.total
+    per_row = batch.nnz / max(rows, 1)
+    return f"sys{batch.n_sys}-rows{int(np.log2(max(rows, 1)))}-nnz{int(np.log2(max(per_row, 1)))}"
+
+
+def _time(batch: Batch, psi, reps: int, precision: int) -> float:
+    ts = []
+    for _ in range(reps):
+        _, ms = batch.step(psi, precision=precision)
+        ts.append(ms)
+    return float(np.median(ts))
+
+
+def autotune(batch: Batch, psi, *, reps: int = 3, precision: int = N.F32,
+             cache: str | None = None) -> dict:
+    """Coordinate search: (chunk, group threshold) with automatic lanes,
+    then the lanes per row of H.psi.  The winner is set on the batch and
+    stored under the workload signature in ``cache`` (JSON) if given."""
+    key = signature(batch)
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            table = json.load(f)
+        if key in table:
+            batch.config = table[key]["config"]
+            return table[key]
+    t0 = time.perf_counter()
+    results = []
+    best = None
+    for ch in CHUNKS:
+        for g in GROUPS:
+            batch.config = (ch, g, 0)
+            t = _time(batch, psi, reps, precision)
+            results.append(((ch, g, 0), t))
+            if best is None or t < best[1]:
+                best = ((ch, g, 0), t)
+    ch, g, _ = best[0]
+    for lanes in LANES[1:]:
+        batch.config = (ch, g, lanes)
+        t = _time(batch, psi, reps, precision)
+        results.append(((ch, g, lanes), t))
+        if t < best[1]:
+            best = ((ch, g, lanes), t)
+    batch.config = best[0]
+    entry = {"config": list(best[0]), "ms": best[1], "signature": key,
+             "tried": [[list(c), t] for c, t in results],
+             "tune_seconds": time.perf_counter() - t0}
+    if cache:
+        table = {}
+        if os.path.exists(cache):
+            with open(cache) as f:
+                table = json.load(f)
+        table[key] = entry
+        os.makedirs(os.path.dirname(os.path.abspath(cache)), exist_ok=True)
+        with open(cache, "w") as f:
+            json.dump(table, f, indent=1)
+    return entry
+
+
+# ---------------------------------------------------------------------------
+# Workload: many synthetic systems of uneven size
+# ---------------------------------------------------------------------------
+
+@dataclass
+class BatchSystem:
+    sysm: S.SyntheticSystem
+    dets: np.ndarray
+
+
+def make_batch_workload(n_sys: int = 64, seed: int = 77, n_min: int = 10, n_max: int = 40,
+                        dets_min: float = 1e3, dets_max: float = 2e5,
+                        cache_dir: str | None = None) -> list[BatchSystem]:
+    """n_orb uniform in [n_min, n_max]; n_elec an even number in
+    [0.4, 0.6] * 2 n_orb with n_alpha = n_beta; K = 2 n_orb Cholesky vectors;
+    determinant counts log-uniform in [dets_min, dets_max], HF plus sampled
+    excitations up to triples."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_sys):
+        n = int(rng.integers(n_min, n_max + 1))
+        lo, hi = int(np.ceil(0.4 * n)), int(np.floor(0.6 * n))
+        na = int(rng.integers(lo, hi + 1))               # n_elec = 2 na, even
+        nd = int(np.exp(rng.uniform(np.log(dets_min), np.log(dets_max))))
+        sysm = S.make_system(n, na, na, 2 * n, seed * 1000 + k)
+        path = None
+        if cache_dir:
+            os.makedirs(cache_dir, exist_ok=True)
+            path = os.path.join(cache_dir, f"batch_{seed}_{k}_{n}_{na}_{nd}.npy")
+        if path and os.path.exists(path):
+            V = np.load(path)
+        else:
+            V = S.heat_bath_sample(sysm, nd, seed * 7919 + k, max_level=3)
+            if path:
+                np.save(path, V)
+        out.append(BatchSystem(sysm, V))
+    return out
+
+
+__all__ = ["Batch", "autotune", "signature", "make_batch_workload", "BatchSystem"]

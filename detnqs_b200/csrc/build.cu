@@ -311,6 +311,23 @@ void sort_rows(Csr& m, cudaStream_t s) {
     m.val = std::move(val2);
 }
 
+// FP32 copy + diagonal split into caller buffers (no allocation; graph-safe).
+void launch_f32_split(const Csr& m, float* val32, double* diag_out, cudaStream_t s) {
+    int dev = 0;
+    DNQ_CUDA(cudaGetDevice(&dev));
+    const int sms = sm_count(dev);
+    if (m.nnz) {
+        k_vals_f32<<<sms * 8, 256, 0, s>>>((const double2*)m.val.p, m.nnz / 2, (float2*)val32);
+        DNQ_CHECK_LAUNCH();
+        k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, m.nnz, val32);
+        DNQ_CHECK_LAUNCH();
+    }
+    if (m.nr) {
+        k_split_diag<<<sms * 8, 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr, val32, diag_out);
+        DNQ_CHECK_LAUNCH();
+    }
+}
+
 void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out) {
     m.val32.alloc(m.nnz, s);
     if (diag_out) diag_out->alloc(m.nr, s);

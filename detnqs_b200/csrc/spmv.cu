@@ -247,6 +247,32 @@ int spmv_grid(int device) { return sm_count(device) * 8; }
 
 }  // namespace
 
+// Same as spmv_block with the lanes-per-row group given (0 = automatic).
+void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
+                  cudaStream_t s, const float* x32, const float* val32, const double* diag,
+                  int G, int device) {
+    if (m.nr == 0) return;
+    if (G == 0) G = group_for(m);
+    const int grid = spmv_grid(device), bs = 256;
+    (void)h;
+    if (precision == DNQ_F64 || m.nnz == 0) {
+        switch (G) {
+            case 32: k_spmv_f64<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
+            case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
+            case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
+            default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
+        }
+    } else {
+        switch (G) {
+            case 32: k_spmv_f32c<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
+            case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
+            case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
+            default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
+        }
+    }
+    DNQ_CHECK_LAUNCH();
+}
+
 // y (+)= M x for one block; x FP64 device, y FP64 device.
 void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
                 const double* yadd, int precision, cudaStream_t s, float* x32,

@@ -20,6 +20,10 @@
 #include <cub/cub.cuh>
 #include <cuda/std/tuple>
 
+#include <algorithm>
+#include <memory>
+#include <vector>
+
 #include "gen.cuh"
 #include "ham.cuh"
 
@@ -28,7 +32,7 @@ namespace dnq {
 namespace {
 
 constexpr int kWS = 8;               // warps per block
-constexpr u32 kBigGroup = 2048;      // part C: search instead of scan above this
+constexpr u32 kBigGroup = 2048;      // part C default: search instead of scan above this
 
 struct StrMapView {
     const ulonglong2* slots = nullptr;   // x = string (~0 empty), y = start<<32 | len
@@ -178,9 +182,13 @@ struct VVParams {
     double eps1;
     double cut;             // doubles: keep w >= cut (and > 1e-15)
     const double* psi;
-    int* next_row;
-    unsigned long long* n_test;
-    // single pass: rows appended to warp-private chunks of an arena
+    u32 big_group;          // part C: binary search for groups longer than this
+};
+
+// Where rows are written.  Single pass: rows appended to warp-private
+// chunks of an arena; long rows get exact space in a second walk; the
+// two-pass fallback counts, then fills at known offsets.
+struct Arena {
     u32* acol;
     double* aval;
     i64 cap;                          // arena capacity (entries)
@@ -191,18 +199,52 @@ struct VVParams {
     u32* row_len;
     u32* big;                         // rows longer than one chunk
     int* n_big;
-    // two-pass fallback
-    u32* cnt;
+    int* next_row;
+    unsigned long long* n_test;
+    u32* cnt;                         // two-pass fallback
     const i64* off;
     u32* col;
     double* val;
 };
 
+// Row sources: one system, or many systems laid end to end (block-diagonal
+// global matrix; row g of system s has local row g - row_off[s] and its
+// columns are offset by row_off[s]).
+struct OneSys {
+    VVParams P;
+    __device__ __forceinline__ i64 rows() const { return P.n; }
+    __device__ __forceinline__ const VVParams& at(i64 g, int& r, u32& base) const {
+        r = (int)g;
+        base = 0;
+        return P;
+    }
+};
+
+struct ManySys {
+    const VVParams* sys;
+    const i64* row_off;    // [n_sys + 1]
+    int n_sys;
+    i64 total;
+    __device__ __forceinline__ i64 rows() const { return total; }
+    __device__ __forceinline__ const VVParams& at(i64 g, int& r, u32& base) const {
+        int lo = 0, hi = n_sys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(&row_off[mid]) <= g) lo = mid; else hi = mid - 1;
+        }
+        const i64 o = __ldg(&row_off[lo]);
+        r = (int)(g - o);
+        base = (u32)o;
+        return sys[lo];
+    }
+};
+
 constexpr i64 kChunk = 8192;   // default arena entries per warp chunk
 
-// Warp-collective sinks of one row's entries.
+// Warp-collective sinks of one row's entries (columns offset by `base`).
 struct CountOut {
     u32 c = 0;
+    u32 base = 0;
     __device__ __forceinline__ void put(bool keep, u32, double) {
         c += __popc(__ballot_sync(0xffffffffu, keep));
     }
@@ -212,12 +254,13 @@ struct ExactOut {
     u32* col;
     double* val;
     i64 w;
+    u32 base;
     u32 c = 0;
     __device__ __forceinline__ void put(bool keep, u32 j, double h) {
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) {
             const i64 at = w + __popc(m & lanemask_lt());
-            col[at] = j;
+            col[at] = j + base;
             val[at] = h;
         }
         w += __popc(m);
@@ -230,6 +273,7 @@ struct ChunkOut {
     u32* col;
     double* val;
     i64 w, end;
+    u32 base;
     u32 c = 0;
     bool over = false;
     __device__ __forceinline__ void put(bool keep, u32 j, double h) {
@@ -241,7 +285,7 @@ struct ChunkOut {
             } else {
                 if (keep) {
                     const i64 at = w + __popc(m & lanemask_lt());
-                    col[at] = j;
+                    col[at] = j + base;
                     val[at] = h;
                 }
                 w += k;
@@ -380,7 +424,7 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
             pp = S.vira[sidx % nva];
             if (!P.amap.find(a ^ (1ull << hh) ^ (1ull << pp), gs, gl)) gl = 0;
         }
-        const bool big = gl > kBigGroup;
+        const bool big = gl > P.big_group;
         const u32 sl = big ? 0u : gl;
         S.start[lane] = gs;
         S.len[lane] = sl;
@@ -471,106 +515,117 @@ __device__ __forceinline__ int next_row(int* ctr) {
     return __shfl_sync(0xffffffffu, r, 0);
 }
 
-__device__ __forceinline__ void add_tests(const VVParams& P, unsigned long long t) {
-    if ((threadIdx.x & 31) == 0) atomicAdd(P.n_test, t);
-}
-
 // Single pass: each warp appends its rows to private chunks of the arena.
-__global__ void __launch_bounds__(kWS * 32) k_vv_arena(VVParams P) {
+template <class Loc>
+__global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const u64 all = low_mask(P.n_orb);
+    const i64 nrows = L.rows();
     i64 cpos = 0, cend = 0;
     {   // first chunk of this warp
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(P.cursor, (unsigned long long)P.chunk);
+        if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)A.chunk);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if ((i64)base + P.chunk <= P.cap) {
+        if ((i64)base + A.chunk <= A.cap) {
             cpos = (i64)base;
-            cend = cpos + P.chunk;
+            cend = cpos + A.chunk;
         }
     }
     unsigned long long tests = 0;
     for (;;) {
-        const int r = next_row(P.next_row);
-        if (r >= P.n) break;
-        if (*(volatile int*)P.overflow) continue;
+        const int g = next_row(A.next_row);
+        if (g >= nrows) break;
+        if (*(volatile int*)A.overflow) continue;
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, all);
+        load_lists(S, a, b, low_mask(P.n_orb));
         for (int attempt = 0; attempt < 2; ++attempt) {
-            ChunkOut out{P.acol, P.aval, cpos, cend};
+            ChunkOut out{A.acol, A.aval, cpos, cend, cb};
             unsigned long long tt = 0;
             vv_row(P, r, a, b, psr, cut, S, out, tt);
             if (attempt == 0) tests += tt;
             if (!out.over) {
                 if (lane == 0) {
-                    P.row_pos[r] = cpos;
-                    P.row_len[r] = out.c;
+                    A.row_pos[g] = cpos;
+                    A.row_len[g] = out.c;
                 }
                 cpos = out.w;
                 break;
             }
-            if ((i64)out.c > P.chunk || attempt == 1) {   // longer than any chunk
+            if ((i64)out.c > A.chunk || attempt == 1) {   // longer than any chunk
                 if (lane == 0) {
-                    P.row_len[r] = out.c;
-                    P.big[atomicAdd(P.n_big, 1)] = (u32)r;
+                    A.row_len[g] = out.c;
+                    A.big[atomicAdd(A.n_big, 1)] = (u32)g;
                 }
                 break;
             }
             unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(P.cursor, (unsigned long long)P.chunk);
+            if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)A.chunk);
             base = __shfl_sync(0xffffffffu, base, 0);
-            if ((i64)base + P.chunk > P.cap) {
-                if (lane == 0) atomicExch(P.overflow, 1);
+            if ((i64)base + A.chunk > A.cap) {
+                if (lane == 0) atomicExch(A.overflow, 1);
                 break;
             }
             cpos = (i64)base;
-            cend = cpos + P.chunk;
+            cend = cpos + A.chunk;
         }
         __syncwarp();
     }
-    add_tests(P, tests);
+    if (lane == 0) atomicAdd(A.n_test, tests);
 }
 
-// Rows longer than a chunk: exact contiguous space, second walk.
-__global__ void __launch_bounds__(kWS * 32) k_vv_big(VVParams P, int nbig) {
+// Rows longer than a chunk: exact contiguous space, second walk.  The count
+// of such rows is read on the device so the launch can sit in a graph.
+template <class Loc>
+__global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const u64 all = low_mask(P.n_orb);
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int nbig = *A.n_big;
+    if (*(volatile int*)A.overflow) return;
     for (int i = gw; i < nbig; i += nw) {
-        const int r = (int)P.big[i];
-        const u32 len = P.row_len[r];
+        const int g = (int)A.big[i];
+        const u32 len = A.row_len[g];
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(P.cursor, (unsigned long long)len);
+        if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)len);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if ((i64)base + len > P.cap) {
-            if (lane == 0) atomicExch(P.overflow, 1);
+        if ((i64)base + len > A.cap) {
+            if (lane == 0) atomicExch(A.overflow, 1);
             continue;
         }
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, all);
-        ExactOut out{P.acol, P.aval, (i64)base};
+        load_lists(S, a, b, low_mask(P.n_orb));
+        ExactOut out{A.acol, A.aval, (i64)base, cb};
         unsigned long long tt = 0;
         vv_row(P, r, a, b, psr, cut, S, out, tt);
-        if (lane == 0) P.row_pos[r] = (i64)base;
+        if (lane == 0) A.row_pos[g] = (i64)base;
         __syncwarp();
     }
 }
 
-// Gather the rows from the arena into a standard CSR.
+// Gather the rows from the arena into a standard CSR; rows past `cap`
+// entries (a stale plan) are not written and raise `*bad`.
 __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const u32* acol,
-                             const double* aval, u32* col, double* val) {
+                             const double* aval, u32* col, double* val, i64 cap, int* bad) {
     const int lane = threadIdx.x & 31;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    if (rowptr[n] > cap) {
+        if (gw == 0 && lane == 0) atomicExch(bad, 1);
+        return;
+    }
     for (i64 r = gw; r < n; r += nw) {
         const i64 src = row_pos[r], dst = rowptr[r], len = rowptr[r + 1] - dst;
         for (i64 t = lane; t < len; t += 32) {
@@ -581,26 +636,29 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
 }
 
 // Two-pass fallback (arena too small): count, then exact fill.
-template <bool FILL>
-__global__ void __launch_bounds__(kWS * 32) k_vv_twopass(VVParams P) {
+template <class Loc, bool FILL>
+__global__ void __launch_bounds__(kWS * 32) k_vv_twopass(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const u64 all = low_mask(P.n_orb);
+    const i64 nrows = L.rows();
     for (;;) {
-        const int r = next_row(P.next_row);
-        if (r >= P.n) break;
+        const int g = next_row(A.next_row);
+        if (g >= nrows) break;
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, all);
+        load_lists(S, a, b, low_mask(P.n_orb));
         unsigned long long tt = 0;
         if (!FILL) {
             CountOut out;
             vv_row(P, r, a, b, psr, cut, S, out, tt);
-            if (lane == 0) P.cnt[r] = out.c;
+            if (lane == 0) A.cnt[g] = out.c;
         } else {
-            ExactOut out{P.col, P.val, P.off[r]};
+            ExactOut out{A.col, A.val, A.off[g], cb};
             vv_row(P, r, a, b, psr, cut, S, out, tt);
         }
         __syncwarp();
@@ -621,22 +679,126 @@ void excl_scan(const T* in, i64* out, i64 n, cudaStream_t s) {
 }
 }  // namespace
 
+void check_orbitals(const u64* d, i64 n, int n_orb, cudaStream_t s);
+
 // Test options: warp chunk size and arena capacity (0 = automatic).
 i64 g_arena_chunk = 0;
 i64 g_arena_cap = 0;
 
-// H_VV only, from string groups.  V on the device, diag already computed.
-// Rows are left in generation order (H->vv.sorted = false); copy-out
-// functions sort them on demand.
-void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
-                      double cut, const double* psi, const double* diag, cudaStream_t s,
-                      dnq_ham_s* H, double* t_ms) {
-    cudaEvent_t ev[5];
+namespace {
+
+template <class Loc>
+int vv_grid(int device) {
+    int per_sm = 0;
+    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vv_arena<Loc>, kWS * 32, 0));
+    return std::max(1, per_sm) * sm_count(device);
+}
+
+// Single-pass build of nrows rows of L into M (allocated here).  cap_hint:
+// expected nnz (0 = unknown).  Falls back to the exact two-pass walk when
+// the arena is too small.  Returns the number of member tests.
+template <class Loc>
+i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
+           double* t_gen, double* t_scan, double* t_compact) {
+    cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
+    const int grid = vv_grid<Loc>(device);
+    const i64 warps = (i64)grid * kWS;
+    size_t freeb = 0, totb = 0;
+    DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
+    const i64 chunk = g_arena_chunk > 0 ? g_arena_chunk : kChunk;
+    i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 256 * nrows;
+    want += warps * chunk;
+    const i64 maxfit = (i64)(freeb / 2 / 12);
+    i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
+    if (g_arena_cap > 0) cap = g_arena_cap;
+    DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
+    DBuf<unsigned long long> nt(1, s), cursor(1, s);
+    DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s);
+    DBuf<double> aval(cap, s);
+    DBuf<i64> rpos(nrows, s);
+    Arena A{};
+    A.acol = acol.p;
+    A.aval = aval.p;
+    A.cap = cap;
+    A.chunk = chunk;
+    A.cursor = cursor.p;
+    A.overflow = ovf.p;
+    A.row_pos = rpos.p;
+    A.row_len = rlen.p;
+    A.big = big.p;
+    A.n_big = nbig.p;
+    A.next_row = next.p;
+    A.n_test = nt.p;
+    DNQ_CUDA(cudaMemsetAsync(nt.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(ovf.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(nbig.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(bad.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(cursor.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(rlen.p + nrows, 0, 4, s));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
-    StrIndex A, B;
-    build_str_index(A, V, n, 0, s);
-    build_str_index(B, V, n, 1, s);
+    k_vv_arena<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_big<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    int hov = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&hov, ovf.p, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    DNQ_CUDA(cudaEventRecord(ev[1], s));
+    M.nr = nrows;
+    M.rowptr.alloc(nrows + 1, s);
+    if (!hov) {
+        excl_scan(rlen.p, M.rowptr.p, nrows + 1, s);
+        DNQ_CUDA(cudaMemcpyAsync(&M.nnz, M.rowptr.p + nrows, 8, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        M.col.alloc(M.nnz, s);
+        M.val.alloc(M.nnz, s);
+        DNQ_CUDA(cudaEventRecord(ev[2], s));
+        k_vv_compact<<<grid, kWS * 32, 0, s>>>(rpos.p, M.rowptr.p, nrows, acol.p, aval.p, M.col.p,
+                                               M.val.p, M.nnz, bad.p);
+        DNQ_CHECK_LAUNCH();
+    } else {
+        acol.release();
+        aval.release();
+        DBuf<u32> cnt(nrows + 1, s);
+        DNQ_CUDA(cudaMemsetAsync(cnt.p + nrows, 0, 4, s));
+        A.cnt = cnt.p;
+        DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
+        k_vv_twopass<Loc, false><<<grid, kWS * 32, 0, s>>>(L, A);
+        DNQ_CHECK_LAUNCH();
+        excl_scan(cnt.p, M.rowptr.p, nrows + 1, s);
+        DNQ_CUDA(cudaMemcpyAsync(&M.nnz, M.rowptr.p + nrows, 8, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        M.col.alloc(M.nnz, s);
+        M.val.alloc(M.nnz, s);
+        A.off = M.rowptr.p;
+        A.col = M.col.p;
+        A.val = M.val.p;
+        DNQ_CUDA(cudaEventRecord(ev[2], s));
+        DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
+        k_vv_twopass<Loc, true><<<grid, kWS * 32, 0, s>>>(L, A);
+        DNQ_CHECK_LAUNCH();
+    }
+    DNQ_CUDA(cudaEventRecord(ev[3], s));
+    unsigned long long tests = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&tests, nt.p, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaEventSynchronize(ev[3]));
+    M.sorted = false;
+    float ms;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    if (t_gen) *t_gen = ms;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+    if (t_scan) *t_scan = ms;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+    if (t_compact) *t_compact = ms;
+    for (auto& e : ev) cudaEventDestroy(e);
+    return (i64)tests;
+}
+
+VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
+                     double cut, const double* psi, const double* diag, const StrIndex& A,
+                     const StrIndex& B) {
     VVParams P{};
     P.C = ctx->view();
     P.E = ctx->erid.p;
@@ -654,110 +816,502 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     P.eps1 = eps1;
     P.cut = cut;
     P.psi = psi;
-    DBuf<int> next(1, s), ovf(1, s), nbig(1, s);
-    DBuf<unsigned long long> nt(1, s), cursor(1, s);
-    DNQ_CUDA(cudaMemsetAsync(nt.p, 0, 8, s));
-    P.next_row = next.p;
-    P.n_test = nt.p;
-    int per_sm = 0;
-    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vv_arena, kWS * 32, 0));
-    const int grid = std::max(1, per_sm) * sm_count(ctx->device);
-    const i64 warps = (i64)grid * kWS;
-    // arena: last build's size for this context if known, else 256 per row,
-    // plus one chunk of slack per warp; capped by free memory
-    size_t freeb = 0, totb = 0;
-    DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
-    const i64 chunk = g_arena_chunk > 0 ? g_arena_chunk : kChunk;
-    i64 want = ctx->vv_nnz_hint > 0 ? (i64)(ctx->vv_nnz_hint * 1.05) : 256 * n;
-    want += warps * chunk;
-    const i64 maxfit = (i64)(freeb / 2 / 12);
-    i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
-    if (g_arena_cap > 0) cap = g_arena_cap;
-    DBuf<u32> acol(cap, s), rlen(n + 1, s), big(n, s);
-    DBuf<double> aval(cap, s);
-    DBuf<i64> rpos(n, s);
-    P.acol = acol.p;
-    P.aval = aval.p;
-    P.cap = cap;
-    P.chunk = chunk;
-    P.cursor = cursor.p;
-    P.overflow = ovf.p;
-    P.row_pos = rpos.p;
-    P.row_len = rlen.p;
-    P.big = big.p;
-    P.n_big = nbig.p;
-    DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
-    DNQ_CUDA(cudaMemsetAsync(ovf.p, 0, 4, s));
-    DNQ_CUDA(cudaMemsetAsync(nbig.p, 0, 4, s));
-    DNQ_CUDA(cudaMemsetAsync(cursor.p, 0, 8, s));
-    DNQ_CUDA(cudaMemsetAsync(rlen.p + n, 0, 4, s));
-    DNQ_CUDA(cudaEventRecord(ev[1], s));
-    k_vv_arena<<<grid, kWS * 32, 0, s>>>(P);
-    DNQ_CHECK_LAUNCH();
-    int hb[2] = {0, 0};
-    DNQ_CUDA(cudaMemcpyAsync(&hb[0], nbig.p, 4, cudaMemcpyDeviceToHost, s));
-    DNQ_CUDA(cudaMemcpyAsync(&hb[1], ovf.p, 4, cudaMemcpyDeviceToHost, s));
-    DNQ_CUDA(cudaStreamSynchronize(s));
-    if (hb[0] > 0 && !hb[1]) {
-        k_vv_big<<<grid, kWS * 32, 0, s>>>(P, hb[0]);
-        DNQ_CHECK_LAUNCH();
-        DNQ_CUDA(cudaMemcpyAsync(&hb[1], ovf.p, 4, cudaMemcpyDeviceToHost, s));
-        DNQ_CUDA(cudaStreamSynchronize(s));
-    }
-    DNQ_CUDA(cudaEventRecord(ev[2], s));
-    H->vv.nr = H->vv.nc = n;
-    H->vv.rowptr.alloc(n + 1, s);
-    if (!hb[1]) {
-        excl_scan(rlen.p, H->vv.rowptr.p, n + 1, s);
-        DNQ_CUDA(cudaMemcpyAsync(&H->vv.nnz, H->vv.rowptr.p + n, 8, cudaMemcpyDeviceToHost, s));
-        DNQ_CUDA(cudaStreamSynchronize(s));
-        H->vv.col.alloc(H->vv.nnz, s);
-        H->vv.val.alloc(H->vv.nnz, s);
-        DNQ_CUDA(cudaEventRecord(ev[3], s));
-        k_vv_compact<<<grid, kWS * 32, 0, s>>>(rpos.p, H->vv.rowptr.p, n, acol.p, aval.p,
-                                               H->vv.col.p, H->vv.val.p);
-        DNQ_CHECK_LAUNCH();
-    } else {
-        // arena too small: exact two-pass walk
-        acol.release();
-        aval.release();
-        DBuf<u32> cnt(n + 1, s);
-        DNQ_CUDA(cudaMemsetAsync(cnt.p + n, 0, 4, s));
-        P.cnt = cnt.p;
-        DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
-        k_vv_twopass<false><<<grid, kWS * 32, 0, s>>>(P);
-        DNQ_CHECK_LAUNCH();
-        excl_scan(cnt.p, H->vv.rowptr.p, n + 1, s);
-        DNQ_CUDA(cudaMemcpyAsync(&H->vv.nnz, H->vv.rowptr.p + n, 8, cudaMemcpyDeviceToHost, s));
-        DNQ_CUDA(cudaStreamSynchronize(s));
-        H->vv.col.alloc(H->vv.nnz, s);
-        H->vv.val.alloc(H->vv.nnz, s);
-        P.off = H->vv.rowptr.p;
-        P.col = H->vv.col.p;
-        P.val = H->vv.val.p;
-        DNQ_CUDA(cudaEventRecord(ev[3], s));
-        DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
-        k_vv_twopass<true><<<grid, kWS * 32, 0, s>>>(P);
-        DNQ_CHECK_LAUNCH();
-    }
-    DNQ_CUDA(cudaEventRecord(ev[4], s));
-    unsigned long long tests = 0;
-    DNQ_CUDA(cudaMemcpyAsync(&tests, nt.p, 8, cudaMemcpyDeviceToHost, s));
-    DNQ_CUDA(cudaEventSynchronize(ev[4]));
-    H->candidates = (i64)tests;
-    H->vv.sorted = false;
-    ctx->vv_nnz_hint = std::max<i64>(ctx->vv_nnz_hint, H->vv.nnz);
-    float ms;
-    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-    t_ms[0] += ms;                  // string indices
-    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
-    t_ms[1] = 0.0;                  // no count pass
-    t_ms[3] = ms;                   // generation pass(es)
-    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
-    t_ms[2] = ms;                   // scan + allocation
-    DNQ_CUDA(cudaEventElapsedTime(&ms, ev[3], ev[4]));
-    t_ms[4] = ms;                   // compaction into CSR (row sort deferred)
-    for (auto& e : ev) cudaEventDestroy(e);
+    P.big_group = kBigGroup;
+    return P;
+}
+
+}  // namespace
+
+// H_VV only, from string groups.  V on the device, diag already computed.
+// Rows are left in generation order (H->vv.sorted = false); copy-out
+// functions sort them on demand.
+void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
+                      double cut, const double* psi, const double* diag, cudaStream_t s,
+                      dnq_ham_s* H, double* t_ms) {
+    cudaEvent_t e0, e1;
+    DNQ_CUDA(cudaEventCreate(&e0));
+    DNQ_CUDA(cudaEventCreate(&e1));
+    DNQ_CUDA(cudaEventRecord(e0, s));
+    StrIndex A, B;
+    build_str_index(A, V, n, 0, s);
+    build_str_index(B, V, n, 1, s);
+    DNQ_CUDA(cudaEventRecord(e1, s));
+    OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
+    double tg = 0, tsc = 0, tc = 0;
+    H->candidates = run_vv(L, n, ctx->vv_nnz_hint, ctx->device, s, H->vv, &tg, &tsc, &tc);
+    H->vv.nc = n;
+    ctx->vv_nnz_hint = std::max<long long>(ctx->vv_nnz_hint, H->vv.nnz);
+    float ms = 0;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t_ms[0] += ms;   // string indices
+    t_ms[1] = 0.0;   // no count pass
+    t_ms[3] = tg;    // generation pass(es)
+    t_ms[2] = tsc;   // scan + allocation
+    t_ms[4] = tc;    // compaction (row sort deferred)
 }
 
 }  // namespace dnq
+
+// ===========================================================================
+// Batched engine: many systems in one launch per phase (block-diagonal).
+// ===========================================================================
+
+namespace dnq {
+
+void launch_f32_split(const Csr& m, float* val32, double* diag_out, cudaStream_t s);
+void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
+                  cudaStream_t s, const float* x32, const float* val32, const double* diag,
+                  int G, int device);
+void to_f32(const double* x, i64 n, float* o, cudaStream_t s);
+
+namespace {
+
+// <x|H|x> of every global row, each with its own system's tables.
+__global__ void k_diag_batch(ManySys L, double* out) {
+    for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < L.total;
+         g += (i64)gridDim.x * blockDim.x) {
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
+        out[g] = diag_elem(P.C, P.V[2 * (i64)r], P.V[2 * (i64)r + 1]);
+    }
+}
+
+__device__ __forceinline__ void tsum_b(double a, double b, double& s, double& e) {
+    s = __dadd_rn(a, b);
+    const double z = __dsub_rn(s, a);
+    e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, z)), __dsub_rn(b, z));
+}
+
+struct DDb {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add_prod(double a, double b) {
+        const double p = __dmul_rn(a, b);
+        const double pe = fma(a, b, -p);
+        double s2, e;
+        tsum_b(s, p, s2, e);
+        s = s2;
+        c = __dadd_rn(c, __dadd_rn(e, pe));
+    }
+    __device__ __forceinline__ void merge(double os, double oc) {
+        double s2, e;
+        tsum_b(s, os, s2, e);
+        s = s2;
+        c = __dadd_rn(__dadd_rn(c, oc), e);
+    }
+};
+
+// One block per system: {x.y, x.x} with Dot2 and eloc = y / x.
+__global__ void k_energy_sys(const i64* row_off, const double* x, const double* y, double* eloc,
+                             double* e2) {
+    const int sy = blockIdx.x;
+    const i64 b = row_off[sy], e = row_off[sy + 1];
+    DDb num, den;
+    for (i64 t = b + threadIdx.x; t < e; t += blockDim.x) {
+        const double xv = x[t], yv = y[t];
+        num.add_prod(xv, yv);
+        den.add_prod(xv, xv);
+        eloc[t] = yv / xv;
+    }
+    for (int o = 16; o; o >>= 1) {
+        num.merge(__shfl_xor_sync(0xffffffffu, num.s, o), __shfl_xor_sync(0xffffffffu, num.c, o));
+        den.merge(__shfl_xor_sync(0xffffffffu, den.s, o), __shfl_xor_sync(0xffffffffu, den.c, o));
+    }
+    __shared__ double sh[4][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sh[0][w] = num.s; sh[1][w] = num.c; sh[2][w] = den.s; sh[3][w] = den.c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DDb a, c;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            a.merge(sh[0][k], sh[1][k]);
+            c.merge(sh[2][k], sh[3][k]);
+        }
+        e2[2 * sy] = a.s + a.c;
+        e2[2 * sy + 1] = c.s + c.c;
+    }
+}
+
+template <class T>
+void scan_plan(const T* in, i64* out, i64 n, cudaStream_t s, DBuf<u8>& tmp) {
+    size_t bytes = 0;
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
+    if (tmp.n < bytes) tmp.alloc(bytes, s);
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, bytes, in, out, n, s));
+}
+
+}  // namespace
+}  // namespace dnq
+
+struct dnq_batch_s {
+    int device = 0;
+    int n_sys = 0;
+    dnq::i64 total = 0;
+    std::vector<dnq_ctx_s*> ctx;
+    std::vector<dnq::DBuf<dnq::u64>> V;
+    std::vector<dnq::StrIndex> A, B;
+    std::vector<dnq::i64> row_off_h;
+    dnq::DBuf<dnq::i64> row_off;
+    dnq::DBuf<dnq::VVParams> sys;
+    dnq::DBuf<double> diag, x, y, eloc, e2;
+    dnq::DBuf<float> x32, val32;
+    dnq::DBuf<double> diag_op;
+    dnq::Csr M;
+    // planned arena (fixed sizes for graph replays)
+    dnq::DBuf<dnq::u32> acol, rlen, big;
+    dnq::DBuf<double> aval;
+    dnq::DBuf<dnq::i64> rpos;
+    dnq::DBuf<int> next, ovf, nbig, bad;
+    dnq::DBuf<unsigned long long> nt, cursor;
+    dnq::DBuf<dnq::u8> scan_tmp;
+    dnq::i64 cap = 0;
+    bool planned = false;
+    // tunables
+    dnq::i64 chunk = dnq::kChunk;
+    dnq::u32 big_group = dnq::kBigGroup;
+    int spmv_group = 0;
+    // graph
+    cudaGraphExec_t gexec = nullptr;
+    int graph_prec = -1;
+    ~dnq_batch_s() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+    }
+};
+
+namespace dnq {
+namespace {
+
+ManySys many(dnq_batch_s* b) {
+    ManySys L;
+    L.sys = b->sys.p;
+    L.row_off = b->row_off.p;
+    L.n_sys = b->n_sys;
+    L.total = b->total;
+    return L;
+}
+
+void upload_params(dnq_batch_s* b, cudaStream_t s) {
+    std::vector<VVParams> hp(b->n_sys);
+    DNQ_CUDA(cudaMemcpyAsync(hp.data(), b->sys.p, b->n_sys * sizeof(VVParams),
+                             cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    for (auto& p : hp) p.big_group = b->big_group;
+    DNQ_CUDA(cudaMemcpyAsync(b->sys.p, hp.data(), b->n_sys * sizeof(VVParams),
+                             cudaMemcpyHostToDevice, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+}
+
+// Plan: one exact build sizes the arena and the CSR; buffers then stay
+// fixed so the step can be replayed from a graph.
+void plan(dnq_batch_s* b, cudaStream_t s) {
+    const ManySys L = many(b);
+    const i64 n = b->total;
+    k_diag_batch<<<sm_count(b->device) * 4, 256, 0, s>>>(L, b->diag.p);
+    DNQ_CHECK_LAUNCH();
+    Csr probe;
+    run_vv(L, n, 0, b->device, s, probe, nullptr, nullptr, nullptr);
+    const int grid = vv_grid<ManySys>(b->device);
+    b->cap = probe.nnz + probe.nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
+    b->M.nr = b->M.nc = n;
+    b->M.nnz = probe.nnz;
+    b->M.rowptr.alloc(n + 1, s);
+    b->M.col.alloc(probe.nnz, s);
+    b->M.val.alloc(probe.nnz, s);
+    b->M.sorted = false;
+    b->acol.alloc(b->cap, s);
+    b->aval.alloc(b->cap, s);
+    b->rlen.alloc(n + 1, s);
+    b->big.alloc(n, s);
+    b->rpos.alloc(n, s);
+    b->next.alloc(1, s);
+    b->ovf.alloc(1, s);
+    b->nbig.alloc(1, s);
+    b->bad.alloc(1, s);
+    b->nt.alloc(1, s);
+    b->cursor.alloc(1, s);
+    b->val32.alloc(probe.nnz, s);
+    b->diag_op.alloc(n, s);
+    b->x.alloc(n, s);
+    b->y.alloc(n, s);
+    b->eloc.alloc(n, s);
+    b->x32.alloc(n, s);
+    b->e2.alloc(2 * b->n_sys, s);
+    {   // scan temporary sized once
+        size_t bytes = 0;
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, b->rlen.p, b->M.rowptr.p, n + 1, s));
+        b->scan_tmp.alloc(bytes, s);
+    }
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    b->planned = true;
+}
+
+// The step on planned buffers: diag, single-pass build, long rows, scan,
+// compaction, FP32 split, H.x, energies.  No allocation, no host sync.
+void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
+    const ManySys L = many(b);
+    const i64 n = b->total;
+    const int grid = vv_grid<ManySys>(b->device);
+    Arena A{};
+    A.acol = b->acol.p;
+    A.aval = b->aval.p;
+    A.cap = b->cap;
+    A.chunk = b->chunk;
+    A.cursor = b->cursor.p;
+    A.overflow = b->ovf.p;
+    A.row_pos = b->rpos.p;
+    A.row_len = b->rlen.p;
+    A.big = b->big.p;
+    A.n_big = b->nbig.p;
+    A.next_row = b->next.p;
+    A.n_test = b->nt.p;
+    k_diag_batch<<<sm_count(b->device) * 4, 256, 0, s>>>(L, b->diag.p);
+    DNQ_CHECK_LAUNCH();
+    DNQ_CUDA(cudaMemsetAsync(b->next.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(b->ovf.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(b->nbig.p, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(b->nt.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(b->cursor.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
+    k_vv_arena<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_big<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    size_t bytes = b->scan_tmp.n;
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(b->scan_tmp.p, bytes, b->rlen.p, b->M.rowptr.p,
+                                           n + 1, s));
+    k_vv_compact<<<grid, kWS * 32, 0, s>>>(b->rpos.p, b->M.rowptr.p, n, b->acol.p, b->aval.p,
+                                           b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p);
+    DNQ_CHECK_LAUNCH();
+    if (precision == DNQ_F32) {
+        launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
+        to_f32(b->x.p, n, b->x32.p, s);
+        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F32, s, b->x32.p, b->val32.p,
+                     b->diag_op.p, b->spmv_group, b->device);
+    } else {
+        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F64, s, nullptr, nullptr, nullptr,
+                     b->spmv_group, b->device);
+    }
+    k_energy_sys<<<b->n_sys, 256, 0, s>>>(b->row_off.p, b->x.p, b->y.p, b->eloc.p, b->e2.p);
+    DNQ_CHECK_LAUNCH();
+}
+
+void check_step(dnq_batch_s* b, cudaStream_t s) {
+    int h[2] = {0, 0};
+    DNQ_CUDA(cudaMemcpyAsync(&h[0], b->ovf.p, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaMemcpyAsync(&h[1], b->bad.p, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    require(!h[0] && !h[1], DNQ_ERR_OVERFLOW,
+            "batched step outgrew its plan (inputs changed); destroy and recreate the batch");
+}
+
+float run_step(dnq_batch_s* b, int precision, bool graph, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    DNQ_CUDA(cudaEventCreate(&e0));
+    DNQ_CUDA(cudaEventCreate(&e1));
+    if (graph && (b->gexec == nullptr || b->graph_prec != precision)) {
+        if (b->gexec) {
+            cudaGraphExecDestroy(b->gexec);
+            b->gexec = nullptr;
+        }
+        cudaGraph_t gr;
+        DNQ_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(b, precision, s);
+        DNQ_CUDA(cudaStreamEndCapture(s, &gr));
+        DNQ_CUDA(cudaGraphInstantiate(&b->gexec, gr, 0));
+        cudaGraphDestroy(gr);
+        b->graph_prec = precision;
+    }
+    DNQ_CUDA(cudaEventRecord(e0, s));
+    if (graph) {
+        DNQ_CUDA(cudaGraphLaunch(b->gexec, s));
+    } else {
+        enqueue_step(b, precision, s);
+    }
+    DNQ_CUDA(cudaEventRecord(e1, s));
+    DNQ_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_step(b, s);
+    return ms;
+}
+
+}  // namespace
+}  // namespace dnq
+
+using namespace dnq;
+
+extern "C" {
+
+int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* dets,
+                     const int64_t* n_dets, const int* n_orb, int policy, int use_heatbath,
+                     double eps1, int device, void* stream, dnq_batch_t* out) {
+    DNQ_API_BEGIN
+    require(out && ctxs && dets && n_dets && n_orb, DNQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    require(n_sys >= 1, DNQ_ERR_INVALID, "a batch needs at least one system");
+    require(policy == DNQ_POLICY_KNOWN_SETS || policy == DNQ_POLICY_STATIC, DNQ_ERR_INVALID,
+            "batched builds support the known-sets and static policies");
+    DeviceGuard g(device);
+    cudaStream_t s = (cudaStream_t)stream;
+    std::unique_ptr<dnq_batch_s> b(new dnq_batch_s);
+    b->device = device;
+    b->n_sys = n_sys;
+    b->ctx.assign(ctxs, ctxs + n_sys);
+    b->row_off_h.assign(n_sys + 1, 0);
+    for (int k = 0; k < n_sys; ++k) {
+        require(ctxs[k] && ctxs[k]->device == device, DNQ_ERR_INVALID,
+                "every context must live on the batch's device");
+        require(n_orb[k] >= 1 && n_orb[k] < 64 && n_orb[k] <= ctxs[k]->n, DNQ_ERR_INVALID,
+                "n_orb must be in [1, min(63, orbitals of the context)]");
+        require(n_dets[k] >= 1 && dets[k], DNQ_ERR_INVALID, "every system needs determinants");
+        if (policy == DNQ_POLICY_STATIC && use_heatbath)
+            require(ctxs[k]->has_hb, DNQ_ERR_NO_HEATBATH, "Heat-Bath table not initialized");
+        b->row_off_h[k + 1] = b->row_off_h[k] + n_dets[k];
+    }
+    b->total = b->row_off_h[n_sys];
+    require(b->total < (i64)0x7fffffff, DNQ_ERR_OVERFLOW, "batch has more than 2^31 rows");
+    b->diag.alloc(b->total, s);
+    std::vector<VVParams> hp(n_sys);
+    b->V.resize(n_sys);
+    b->A.resize(n_sys);
+    b->B.resize(n_sys);
+    for (int k = 0; k < n_sys; ++k) {
+        const i64 n = n_dets[k];
+        b->V[k].alloc(2 * n, s);
+        DNQ_CUDA(cudaMemcpyAsync(b->V[k].p, dets[k], 16 * n, cudaMemcpyDefault, s));
+        check_orbitals(b->V[k].p, n, n_orb[k], s);
+        DetMap dup;
+        build_detmap(dup, b->V[k].p, n, true, s);   // duplicates are an error
+        build_str_index(b->A[k], b->V[k].p, n, 0, s);
+        build_str_index(b->B[k], b->V[k].p, n, 1, s);
+        const double cut = (policy == DNQ_POLICY_STATIC && use_heatbath)
+                               ? hb_cutoff(ctxs[k], eps1) : full_cutoff();
+        hp[k] = make_params(ctxs[k], b->V[k].p, n, n_orb[k], policy, eps1, cut, nullptr,
+                            b->diag.p + b->row_off_h[k], b->A[k], b->B[k]);
+    }
+    b->sys.alloc(n_sys, s);
+    DNQ_CUDA(cudaMemcpyAsync(b->sys.p, hp.data(), n_sys * sizeof(VVParams),
+                             cudaMemcpyHostToDevice, s));
+    b->row_off.alloc(n_sys + 1, s);
+    DNQ_CUDA(cudaMemcpyAsync(b->row_off.p, b->row_off_h.data(), (n_sys + 1) * sizeof(i64),
+                             cudaMemcpyHostToDevice, s));
+    plan(b.get(), s);
+    *out = b.release();
+    DNQ_API_END
+}
+
+int dnq_batch_destroy(dnq_batch_t b) {
+    DNQ_API_BEGIN
+    if (!b) return DNQ_OK;
+    DeviceGuard g(b->device);
+    delete b;
+    DNQ_CUDA(cudaDeviceSynchronize());
+    DNQ_API_END
+}
+
+int dnq_batch_info(dnq_batch_t b, int64_t* info4) {
+    DNQ_API_BEGIN
+    require(b && info4, DNQ_ERR_INVALID, "null argument");
+    info4[0] = b->n_sys;
+    info4[1] = b->total;
+    info4[2] = b->M.nnz;
+    info4[3] = (int64_t)(b->acol.bytes() + b->aval.bytes() + b->M.bytes() + b->val32.bytes());
+    DNQ_API_END
+}
+
+int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3) {
+    DNQ_API_BEGIN
+    require(b && cfg3, DNQ_ERR_INVALID, "null argument");
+    require(cfg3[0] >= 64 && cfg3[0] <= (1 << 20), DNQ_ERR_INVALID, "chunk out of range");
+    require(cfg3[1] >= 32, DNQ_ERR_INVALID, "group threshold out of range");
+    require(cfg3[2] == 0 || cfg3[2] == 4 || cfg3[2] == 8 || cfg3[2] == 16 || cfg3[2] == 32,
+            DNQ_ERR_INVALID, "lanes per row must be 0, 4, 8, 16 or 32");
+    DeviceGuard g(b->device);
+    const bool resize = cfg3[0] > b->chunk;
+    b->chunk = cfg3[0];
+    b->big_group = (u32)cfg3[1];
+    b->spmv_group = (int)cfg3[2];
+    upload_params(b, nullptr);
+    if (resize) {   // larger chunks need a larger arena
+        const int grid = vv_grid<ManySys>(b->device);
+        b->cap = b->M.nnz + b->M.nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
+        b->acol.alloc(b->cap, nullptr);
+        b->aval.alloc(b->cap, nullptr);
+        DNQ_CUDA(cudaStreamSynchronize(nullptr));
+    }
+    if (b->gexec) {
+        cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+    }
+    DNQ_API_END
+}
+
+int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3) {
+    DNQ_API_BEGIN
+    require(b && cfg3, DNQ_ERR_INVALID, "null argument");
+    cfg3[0] = b->chunk;
+    cfg3[1] = b->big_group;
+    cfg3[2] = b->spmv_group;
+    DNQ_API_END
+}
+
+int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc, double* energies,
+                   int precision, int use_graph, void* stream, double* step_ms) {
+    DNQ_API_BEGIN
+    require(b && psi, DNQ_ERR_INVALID, "null argument");
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    DeviceGuard g(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    require(s != nullptr || !use_graph, DNQ_ERR_INVALID,
+            "graph replay needs an explicit (non-default) stream");
+    DNQ_CUDA(cudaMemcpyAsync(b->x.p, psi, b->total * 8, cudaMemcpyDefault, s));
+    const float ms = run_step(b, precision, use_graph != 0, s);
+    if (step_ms) *step_ms = ms;
+    copy_out(eloc, b->eloc.p, b->total, s);
+    copy_out(energies, b->e2.p, 2 * b->n_sys, s);
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    DNQ_API_END
+}
+
+// Sorted COO of one system's block, local indices (reference format).
+int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols, double* vals,
+                       int64_t* nnz) {
+    DNQ_API_BEGIN
+    require(b && nnz && sys >= 0 && sys < b->n_sys, DNQ_ERR_INVALID, "invalid system");
+    DeviceGuard g(b->device);
+    std::vector<i64> rp(b->total + 1);
+    DNQ_CUDA(cudaMemcpy(rp.data(), b->M.rowptr.p, (b->total + 1) * 8, cudaMemcpyDeviceToHost));
+    const i64 r0 = b->row_off_h[sys], r1 = b->row_off_h[sys + 1];
+    const i64 k0 = rp[r0], k1 = rp[r1];
+    *nnz = k1 - k0;
+    if (!rows && !cols && !vals) return DNQ_OK;
+    std::vector<u32> c(k1 - k0);
+    std::vector<double> v(k1 - k0);
+    if (k1 > k0) {
+        DNQ_CUDA(cudaMemcpy(c.data(), b->M.col.p + k0, (k1 - k0) * 4, cudaMemcpyDeviceToHost));
+        DNQ_CUDA(cudaMemcpy(v.data(), b->M.val.p + k0, (k1 - k0) * 8, cudaMemcpyDeviceToHost));
+    }
+    i64 w = 0;
+    for (i64 r = r0; r < r1; ++r) {   // rows are in generation order: sort each
+        std::vector<std::pair<u32, double>> row;
+        for (i64 k = rp[r]; k < rp[r + 1]; ++k)
+            row.push_back({c[k - k0] - (u32)r0, v[k - k0]});
+        std::sort(row.begin(), row.end(),
+                  [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (auto& e : row) {
+            if (rows) rows[w] = (u32)(r - r0);
+            if (cols) cols[w] = e.first;
+            if (vals) vals[w] = e.second;
+            ++w;
+        }
+    }
+    DNQ_API_END
+}
+
+}  // extern "C"

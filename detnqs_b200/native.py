@@ -45,6 +45,8 @@ EXPORTS = (
     "dnq_variational_energy", "dnq_ham_eff", "dnq_ham_eff_from", "dnq_ham_p_diag",
     "dnq_ham_block_spmv", "dnq_gen_dets", "dnq_local_connections", "dnq_conn_copy",
     "dnq_pt2", "dnq_ham_local_energy_noalloc",
+    "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
+    "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_copy_coo",
 )
 
 
@@ -113,6 +115,13 @@ _sig("dnq_gen_dets", _P, _P, _I64, _I, _P, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_local_connections", _P, _P, _I64, _I, _I, _D, _P, C.POINTER(_P))
 _sig("dnq_conn_copy", _P, _P, _P, _P, _P)
 _sig("dnq_pt2", _P, _P, _I64, _P, _I, _D, _I, _D, _P, _P)
+_sig("dnq_batch_create", _I, _P, _P, _P, _P, _I, _I, _D, _I, _P, C.POINTER(_P))
+_sig("dnq_batch_destroy", _P)
+_sig("dnq_batch_info", _P, _P)
+_sig("dnq_batch_set_config", _P, _P)
+_sig("dnq_batch_get_config", _P, _P)
+_sig("dnq_batch_step", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
+_sig("dnq_batch_copy_coo", _P, _I, _P, _P, _P, C.POINTER(_I64))
 _sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_variational_energy", _P, _P, _I64, _P, _I, _I, _D, C.POINTER(_D), _P)
 _sig("dnq_ham_eff", _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _D, _I, _D, _I, _I,

@@ -229,7 +229,8 @@ def heat_bath_sample(sysm: SyntheticSystem, n_dets: int, seed: int,
 
     Children whose excitation level from HF exceeds ``max_level`` are
     dropped; new unique determinants are appended in draw order until
-    ``n_dets`` are collected.  Deterministic for a given ``seed``.
+    ``n_dets`` are collected (or no new determinant appears for 8 rounds,
+    when the space is smaller).  Deterministic for a given ``seed``.
     """
     n = sysm.n_orb
     na, nb = sysm.n_alpha, sysm.n_beta
@@ -260,7 +261,9 @@ def heat_bath_sample(sysm: SyntheticSystem, n_dets: int, seed: int,
     out[0] = hf
     count = 1
     seen = {(int(hf[0]), int(hf[1]))}
-    while count < n_dets:
+    stalled = 0
+    while count < n_dets and stalled < 8:
+        before = count
         m = batch
         par = out[rng.integers(0, count, size=m)]
         occ_a = _occ_table(par[:, 0], n, na)
@@ -324,7 +327,9 @@ def heat_bath_sample(sysm: SyntheticSystem, n_dets: int, seed: int,
                 count += 1
                 if count >= n_dets:
                     break
-    return np.ascontiguousarray(out)
+        stalled = stalled + 1 if count == before else 0
+    # a space smaller than n_dets (few orbitals / low level) ends the draw
+    return np.ascontiguousarray(out[:count])
 
 
 def unpack_eri(eri: np.ndarray, n: int) -> np.ndarray:

@@ -30,6 +30,7 @@ extern "C" {
 
 typedef struct dnq_ctx_s* dnq_ctx_t;    /* integrals + tables in HBM (IntCtx) */
 typedef struct dnq_ham_s* dnq_ham_t;    /* H_VV / H_VP / P-space in HBM      */
+typedef struct dnq_batch_s* dnq_batch_t;  /* many systems, one launch/phase  */
 
 enum {
     DNQ_OK = 0,
@@ -232,6 +233,38 @@ int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols,
                 const double* h_pp, double e_ref, int reg_sigma,
                 double epsilon, int precision, int device, void* stream,
                 dnq_ham_t* out);
+
+/* ---- batched engine (no reference counterpart) ------------------------------
+ * Many independent systems (each with its own integral context and V, any
+ * n_orb < 64) built and contracted together: the rows of all systems form
+ * one block-diagonal problem and every phase is one launch over all of
+ * them.  One step = diagonal, screened V->V build (the same rules and
+ * results as dnq_build with want_vp = 0), H.psi on the concatenated psi,
+ * and per-system {psi.H psi, psi.psi} plus local energies.  Creation runs
+ * one build to size every buffer; afterwards a step allocates nothing and
+ * can be captured into a CUDA graph (use_graph = 1, explicit stream; the
+ * first such call captures, later calls replay).  A step whose sizes no
+ * longer match the plan fails with DNQ_ERR_OVERFLOW.
+ * policy: DNQ_POLICY_KNOWN_SETS or DNQ_POLICY_STATIC. */
+int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* dets,
+                     const int64_t* n_dets, const int* n_orb, int policy,
+                     int use_heatbath, double eps1, int device, void* stream,
+                     dnq_batch_t* out);
+int dnq_batch_destroy(dnq_batch_t b);
+/* info4 = {n_sys, total rows, nnz, device bytes of the planned buffers} */
+int dnq_batch_info(dnq_batch_t b, int64_t* info4);
+/* cfg3 = {arena chunk entries, part-C search threshold, lanes per row of
+ * H.psi (0 = by row length)}: the tunables the autotuner chooses. */
+int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3);
+int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3);
+/* psi: concatenated amplitudes (host or device); eloc (total rows) and
+ * energies (2 per system) may be NULL; *step_ms = device time of the step. */
+int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc,
+                   double* energies, int precision, int use_graph, void* stream,
+                   double* step_ms);
+/* Sorted COO (local indices) of one system's block; *nnz always set. */
+int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols,
+                       double* vals, int64_t* nnz);
 
 #ifdef __cplusplus
 }
