@@ -936,6 +936,20 @@ __global__ void k_energy_sys(const i64* row_off, const double* x, const double* 
     }
 }
 
+// After an overflow (or a total past the plan) the row pointers cannot be
+// trusted: make the block empty so later kernels stay in bounds, and flag.
+// Launched as ONE block, so the decision is read before any entry is zeroed;
+// on the good path it returns at once.
+__global__ void k_sanitize(i64* rowptr, i64 n, i64 cap, const int* overflow, int* bad) {
+    __shared__ int broken;
+    if (threadIdx.x == 0) broken = (*overflow != 0) || rowptr[n] > cap || rowptr[n] < 0;
+    __syncthreads();
+    if (!broken) return;
+    if (threadIdx.x == 0) atomicExch(bad, 1);
+    __syncthreads();
+    for (i64 t = threadIdx.x; t <= n; t += blockDim.x) rowptr[t] = 0;
+}
+
 template <class T>
 void scan_plan(const T* in, i64* out, i64 n, cudaStream_t s, DBuf<u8>& tmp) {
     size_t bytes = 0;
@@ -1012,16 +1026,13 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     const i64 n = b->total;
     k_diag_batch<<<sm_count(b->device) * 4, 256, 0, s>>>(L, b->diag.p);
     DNQ_CHECK_LAUNCH();
-    Csr probe;
-    run_vv(L, n, 0, b->device, s, probe, nullptr, nullptr, nullptr);
+    // the sizing build fills the batch's CSR itself, so the blocks are
+    // valid right after creation
+    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr);
+    b->M.nc = n;
+    const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
-    b->cap = probe.nnz + probe.nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
-    b->M.nr = b->M.nc = n;
-    b->M.nnz = probe.nnz;
-    b->M.rowptr.alloc(n + 1, s);
-    b->M.col.alloc(probe.nnz, s);
-    b->M.val.alloc(probe.nnz, s);
-    b->M.sorted = false;
+    b->cap = nnz + nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
     b->acol.alloc(b->cap, s);
     b->aval.alloc(b->cap, s);
     b->rlen.alloc(n + 1, s);
@@ -1033,7 +1044,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->bad.alloc(1, s);
     b->nt.alloc(1, s);
     b->cursor.alloc(1, s);
-    b->val32.alloc(probe.nnz, s);
+    b->val32.alloc(nnz, s);
     b->diag_op.alloc(n, s);
     b->x.alloc(n, s);
     b->y.alloc(n, s);
@@ -1075,6 +1086,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
     DNQ_CUDA(cudaMemsetAsync(b->nbig.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->nt.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(b->cursor.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(b->bad.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
     k_vv_arena<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1083,6 +1095,8 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
     size_t bytes = b->scan_tmp.n;
     DNQ_CUDA(cub::DeviceScan::ExclusiveSum(b->scan_tmp.p, bytes, b->rlen.p, b->M.rowptr.p,
                                            n + 1, s));
+    k_sanitize<<<1, 1024, 0, s>>>(b->M.rowptr.p, n, b->M.nnz, b->ovf.p, b->bad.p);
+    DNQ_CHECK_LAUNCH();
     k_vv_compact<<<grid, kWS * 32, 0, s>>>(b->rpos.p, b->M.rowptr.p, n, b->acol.p, b->aval.p,
                                            b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p);
     DNQ_CHECK_LAUNCH();
@@ -1288,6 +1302,9 @@ int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols, d
     std::vector<i64> rp(b->total + 1);
     DNQ_CUDA(cudaMemcpy(rp.data(), b->M.rowptr.p, (b->total + 1) * 8, cudaMemcpyDeviceToHost));
     const i64 r0 = b->row_off_h[sys], r1 = b->row_off_h[sys + 1];
+    for (i64 r = r0; r < r1; ++r)
+        require(rp[r] >= 0 && rp[r] <= rp[r + 1] && rp[r + 1] <= b->M.nnz, DNQ_ERR_INVALID,
+                "batch CSR row pointers are not valid");
     const i64 k0 = rp[r0], k1 = rp[r1];
     *nnz = k1 - k0;
     if (!rows && !cols && !vals) return DNQ_OK;
