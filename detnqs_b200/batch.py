@@ -69,15 +69,30 @@ class Batch:
 
     def step(self, psi, *, precision: int = N.F32, graph: bool = False, stream=None,
              eloc=None):
-        """One batched step.  Returns (energies[n_sys, 2], device ms)."""
+        """One batched step (rebuild every H_VV, then H.psi).  Returns
+        (energies[n_sys, 2] = {psi.H psi, psi.psi}, device ms)."""
+        return self._run(N.lib.dnq_batch_step, psi, precision, graph, stream, eloc)
+
+    def apply(self, psi, *, precision: int = N.F32, graph: bool = False, stream=None,
+              eloc=None):
+        """H.psi and energies on the resident H_VV blocks (no rebuild)."""
+        return self._run(N.lib.dnq_batch_apply, psi, precision, graph, stream, eloc)
+
+    def _run(self, fn, psi, precision, graph, stream, eloc):
         p = psi if hasattr(psi, "data_ptr") else np.ascontiguousarray(psi, np.float64)
         e2 = np.zeros((self.n_sys, 2))
         ms = C.c_double()
         if graph and stream is None:
             stream = _side_stream()
-        N.check(N.lib.dnq_batch_step(self._h, N.ptr(p), N.ptr(eloc), e2.ctypes.data,
-                                     int(precision), int(bool(graph)), stream, C.byref(ms)))
+        N.check(fn(self._h, N.ptr(p), N.ptr(eloc), e2.ctypes.data, int(precision),
+                   int(bool(graph)), stream, C.byref(ms)))
         return e2, ms.value
+
+    def timings(self) -> dict:
+        """Device ms of the phases of the last eager step."""
+        t = np.zeros(4)
+        N.check(N.lib.dnq_batch_timings(self._h, t.ctypes.data))
+        return dict(zip(("diag", "build", "compact", "hpsi"), (float(x) for x in t)))
 
     def coo(self, k: int) -> dict:
         nnz = C.c_int64()
@@ -183,33 +198,54 @@ class BatchSystem:
     dets: np.ndarray
 
 
+def _sample(job):
+    n, na, nd, sys_seed, det_seed, path = job
+    if path and os.path.exists(path):
+        return np.load(path)
+    sysm = S.make_system(n, na, na, 2 * n, sys_seed)
+    V = S.heat_bath_sample(sysm, nd, det_seed, max_level=3)
+    if path:
+        np.save(path, V)
+    return V
+
+
 def make_batch_workload(n_sys: int = 64, seed: int = 77, n_min: int = 10, n_max: int = 40,
                         dets_min: float = 1e3, dets_max: float = 2e5,
-                        cache_dir: str | None = None) -> list[BatchSystem]:
+                        cache_dir: str | None = None, workers: int | None = None
+                        ) -> list[BatchSystem]:
     """n_orb uniform in [n_min, n_max]; n_elec an even number in
     [0.4, 0.6] * 2 n_orb with n_alpha = n_beta; K = 2 n_orb Cholesky vectors;
     determinant counts log-uniform in [dets_min, dets_max], HF plus sampled
-    excitations up to triples."""
+    excitations up to triples.
+
+    The systems are sampled in ``workers`` spawned processes (default: one
+    per core, at most ``n_sys``); every system has its own seeds, so the
+    result does not depend on the worker count."""
     rng = np.random.default_rng(seed)
-    out = []
+    jobs = []
     for k in range(n_sys):
         n = int(rng.integers(n_min, n_max + 1))
         lo, hi = int(np.ceil(0.4 * n)), int(np.floor(0.6 * n))
         na = int(rng.integers(lo, hi + 1))               # n_elec = 2 na, even
         nd = int(np.exp(rng.uniform(np.log(dets_min), np.log(dets_max))))
-        sysm = S.make_system(n, na, na, 2 * n, seed * 1000 + k)
         path = None
         if cache_dir:
             os.makedirs(cache_dir, exist_ok=True)
             path = os.path.join(cache_dir, f"batch_{seed}_{k}_{n}_{na}_{nd}.npy")
-        if path and os.path.exists(path):
-            V = np.load(path)
-        else:
-            V = S.heat_bath_sample(sysm, nd, seed * 7919 + k, max_level=3)
-            if path:
-                np.save(path, V)
-        out.append(BatchSystem(sysm, V))
-    return out
+        jobs.append((n, na, nd, seed * 1000 + k, seed * 7919 + k, path))
+    workers = min(n_sys, workers or os.cpu_count() or 1)
+    if workers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        # largest first, spawned (safe whatever the parent has initialised)
+        order = sorted(range(n_sys), key=lambda k: -jobs[k][2])
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            got = dict(zip(order, ex.map(_sample, [jobs[k] for k in order])))
+        dets = [got[k] for k in range(n_sys)]
+    else:
+        dets = [_sample(j) for j in jobs]
+    return [BatchSystem(S.make_system(n, na, na, 2 * n, ss), V)
+            for (n, na, _, ss, _, _), V in zip(jobs, dets)]
 
 
 __all__ = ["Batch", "autotune", "signature", "make_batch_workload", "BatchSystem"]

@@ -988,12 +988,21 @@ struct dnq_batch_s {
     dnq::i64 chunk = dnq::kChunk;
     dnq::u32 big_group = dnq::kBigGroup;
     int spmv_group = 0;
-    // graph
-    cudaGraphExec_t gexec = nullptr;
-    int graph_prec = -1;
-    ~dnq_batch_s() {
-        if (gexec) cudaGraphExecDestroy(gexec);
+    // graphs: [0] full step (build + H.psi), [1] H.psi on the resident CSR
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    int graph_prec[2] = {-1, -1};
+    bool f32_ready = false;   // val32 / diag_op match the resident CSR
+    // phases of the last eager step: diag, build (arena + long rows),
+    // scan + compaction (+ FP32 split), H.psi + energies
+    double phase_ms[4] = {0, 0, 0, 0};
+    void drop_graphs() {
+        for (auto& g : gexec)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
     }
+    ~dnq_batch_s() { drop_graphs(); }
 };
 
 namespace dnq {
@@ -1060,9 +1069,28 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->planned = true;
 }
 
+// H.x and the per-system energies on the resident CSR (FP32: val32 and
+// diag_op must already hold the split of M).
+void enqueue_apply(dnq_batch_s* b, int precision, cudaStream_t s) {
+    if (precision == DNQ_F32) {
+        to_f32(b->x.p, b->total, b->x32.p, s);
+        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F32, s, b->x32.p, b->val32.p,
+                     b->diag_op.p, b->spmv_group, b->device);
+    } else {
+        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F64, s, nullptr, nullptr, nullptr,
+                     b->spmv_group, b->device);
+    }
+    k_energy_sys<<<b->n_sys, 256, 0, s>>>(b->row_off.p, b->x.p, b->y.p, b->eloc.p, b->e2.p);
+    DNQ_CHECK_LAUNCH();
+}
+
 // The step on planned buffers: diag, single-pass build, long rows, scan,
 // compaction, FP32 split, H.x, energies.  No allocation, no host sync.
-void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
+void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+    auto mark = [&](int k) {
+        if (ev) DNQ_CUDA(cudaEventRecord(ev[k], s));
+    };
+    mark(0);
     const ManySys L = many(b);
     const i64 n = b->total;
     const int grid = vv_grid<ManySys>(b->device);
@@ -1081,6 +1109,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
     A.n_test = b->nt.p;
     k_diag_batch<<<sm_count(b->device) * 4, 256, 0, s>>>(L, b->diag.p);
     DNQ_CHECK_LAUNCH();
+    mark(1);
     DNQ_CUDA(cudaMemsetAsync(b->next.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->ovf.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->nbig.p, 0, 4, s));
@@ -1092,6 +1121,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     k_vv_big<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
+    mark(2);
     size_t bytes = b->scan_tmp.n;
     DNQ_CUDA(cub::DeviceScan::ExclusiveSum(b->scan_tmp.p, bytes, b->rlen.p, b->M.rowptr.p,
                                            n + 1, s));
@@ -1100,17 +1130,10 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s) {
     k_vv_compact<<<grid, kWS * 32, 0, s>>>(b->rpos.p, b->M.rowptr.p, n, b->acol.p, b->aval.p,
                                            b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p);
     DNQ_CHECK_LAUNCH();
-    if (precision == DNQ_F32) {
-        launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
-        to_f32(b->x.p, n, b->x32.p, s);
-        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F32, s, b->x32.p, b->val32.p,
-                     b->diag_op.p, b->spmv_group, b->device);
-    } else {
-        spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F64, s, nullptr, nullptr, nullptr,
-                     b->spmv_group, b->device);
-    }
-    k_energy_sys<<<b->n_sys, 256, 0, s>>>(b->row_off.p, b->x.p, b->y.p, b->eloc.p, b->e2.p);
-    DNQ_CHECK_LAUNCH();
+    if (precision == DNQ_F32) launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
+    mark(3);
+    enqueue_apply(b, precision, s);
+    mark(4);
 }
 
 void check_step(dnq_batch_s* b, cudaStream_t s) {
@@ -1122,28 +1145,42 @@ void check_step(dnq_batch_s* b, cudaStream_t s) {
             "batched step outgrew its plan (inputs changed); destroy and recreate the batch");
 }
 
-float run_step(dnq_batch_s* b, int precision, bool graph, cudaStream_t s) {
+// mode 0: full step; mode 1: H.psi only on the resident CSR.
+float run_step(dnq_batch_s* b, int mode, int precision, bool graph, cudaStream_t s) {
+    cudaEvent_t ph[5];
+    const bool phases = mode == 0 && !graph;
+    if (phases)
+        for (auto& e : ph) DNQ_CUDA(cudaEventCreate(&e));
+    auto enqueue = [&](cudaStream_t st) {
+        if (mode == 0) enqueue_step(b, precision, st, phases ? ph : nullptr);
+        else enqueue_apply(b, precision, st);
+    };
+    if (mode == 1 && precision == DNQ_F32 && !b->f32_ready) {
+        launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);   // once, outside any graph
+        b->f32_ready = true;
+    }
     cudaEvent_t e0, e1;
     DNQ_CUDA(cudaEventCreate(&e0));
     DNQ_CUDA(cudaEventCreate(&e1));
-    if (graph && (b->gexec == nullptr || b->graph_prec != precision)) {
-        if (b->gexec) {
-            cudaGraphExecDestroy(b->gexec);
-            b->gexec = nullptr;
+    cudaGraphExec_t& ge = b->gexec[mode];
+    if (graph && (ge == nullptr || b->graph_prec[mode] != precision)) {
+        if (ge) {
+            cudaGraphExecDestroy(ge);
+            ge = nullptr;
         }
         cudaGraph_t gr;
         DNQ_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(b, precision, s);
+        enqueue(s);
         DNQ_CUDA(cudaStreamEndCapture(s, &gr));
-        DNQ_CUDA(cudaGraphInstantiate(&b->gexec, gr, 0));
+        DNQ_CUDA(cudaGraphInstantiate(&ge, gr, 0));
         cudaGraphDestroy(gr);
-        b->graph_prec = precision;
+        b->graph_prec[mode] = precision;
     }
     DNQ_CUDA(cudaEventRecord(e0, s));
     if (graph) {
-        DNQ_CUDA(cudaGraphLaunch(b->gexec, s));
+        DNQ_CUDA(cudaGraphLaunch(ge, s));
     } else {
-        enqueue_step(b, precision, s);
+        enqueue(s);
     }
     DNQ_CUDA(cudaEventRecord(e1, s));
     DNQ_CUDA(cudaEventSynchronize(e1));
@@ -1151,7 +1188,18 @@ float run_step(dnq_batch_s* b, int precision, bool graph, cudaStream_t s) {
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    check_step(b, s);
+    if (phases) {
+        for (int k = 0; k < 4; ++k) {
+            float t = 0.f;
+            DNQ_CUDA(cudaEventElapsedTime(&t, ph[k], ph[k + 1]));
+            b->phase_ms[k] = t;
+        }
+        for (auto& e : ph) cudaEventDestroy(e);
+    }
+    if (mode == 0) {
+        b->f32_ready = precision == DNQ_F32;
+        check_step(b, s);
+    }
     return ms;
 }
 
@@ -1259,10 +1307,14 @@ int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3) {
         b->aval.alloc(b->cap, nullptr);
         DNQ_CUDA(cudaStreamSynchronize(nullptr));
     }
-    if (b->gexec) {
-        cudaGraphExecDestroy(b->gexec);
-        b->gexec = nullptr;
-    }
+    b->drop_graphs();
+    DNQ_API_END
+}
+
+int dnq_batch_timings(dnq_batch_t b, double* ms4) {
+    DNQ_API_BEGIN
+    require(b && ms4, DNQ_ERR_INVALID, "null argument");
+    for (int k = 0; k < 4; ++k) ms4[k] = b->phase_ms[k];
     DNQ_API_END
 }
 
@@ -1275,8 +1327,9 @@ int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3) {
     DNQ_API_END
 }
 
-int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc, double* energies,
-                   int precision, int use_graph, void* stream, double* step_ms) {
+static int batch_run(dnq_batch_t b, int mode, const double* psi, double* eloc,
+                     double* energies, int precision, int use_graph, void* stream,
+                     double* step_ms) {
     DNQ_API_BEGIN
     require(b && psi, DNQ_ERR_INVALID, "null argument");
     require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
@@ -1285,12 +1338,22 @@ int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc, double* energ
     require(s != nullptr || !use_graph, DNQ_ERR_INVALID,
             "graph replay needs an explicit (non-default) stream");
     DNQ_CUDA(cudaMemcpyAsync(b->x.p, psi, b->total * 8, cudaMemcpyDefault, s));
-    const float ms = run_step(b, precision, use_graph != 0, s);
+    const float ms = run_step(b, mode, precision, use_graph != 0, s);
     if (step_ms) *step_ms = ms;
     copy_out(eloc, b->eloc.p, b->total, s);
     copy_out(energies, b->e2.p, 2 * b->n_sys, s);
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_API_END
+}
+
+int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc, double* energies,
+                   int precision, int use_graph, void* stream, double* step_ms) {
+    return batch_run(b, 0, psi, eloc, energies, precision, use_graph, stream, step_ms);
+}
+
+int dnq_batch_apply(dnq_batch_t b, const double* psi, double* eloc, double* energies,
+                    int precision, int use_graph, void* stream, double* step_ms) {
+    return batch_run(b, 1, psi, eloc, energies, precision, use_graph, stream, step_ms);
 }
 
 // Sorted COO of one system's block, local indices (reference format).

@@ -46,7 +46,7 @@ EXPORTS = (
     "dnq_ham_block_spmv", "dnq_gen_dets", "dnq_local_connections", "dnq_conn_copy",
     "dnq_pt2", "dnq_ham_local_energy_noalloc",
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
-    "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_copy_coo",
+    "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
 )
 
 
@@ -121,6 +121,8 @@ _sig("dnq_batch_info", _P, _P)
 _sig("dnq_batch_set_config", _P, _P)
 _sig("dnq_batch_get_config", _P, _P)
 _sig("dnq_batch_step", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
+_sig("dnq_batch_apply", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
+_sig("dnq_batch_timings", _P, _P)
 _sig("dnq_batch_copy_coo", _P, _I, _P, _P, _P, C.POINTER(_I64))
 _sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_variational_energy", _P, _P, _I64, _P, _I, _I, _D, C.POINTER(_D), _P)

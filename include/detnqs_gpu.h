@@ -262,6 +262,16 @@ int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3);
 int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc,
                    double* energies, int precision, int use_graph, void* stream,
                    double* step_ms);
+/* H.psi and energies only, on the CSR resident from creation or the last
+ * step (the inner loop between rebuilds); same arguments as
+ * dnq_batch_step, its own captured graph. */
+int dnq_batch_apply(dnq_batch_t b, const double* psi, double* eloc,
+                    double* energies, int precision, int use_graph, void* stream,
+                    double* step_ms);
+/* Device ms of the phases of the last eager (use_graph = 0) step:
+ * {diagonal, build (arena + long rows), scan + compaction (+ FP32 split),
+ *  H.psi + energies}. */
+int dnq_batch_timings(dnq_batch_t b, double* ms4);
 /* Sorted COO (local indices) of one system's block; *nnz always set. */
 int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols,
                        double* vals, int64_t* nnz);

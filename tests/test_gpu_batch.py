@@ -82,3 +82,42 @@ def test_autotune_keeps_results(workload, tmp_path):
     again = B.autotune(bt, psi, cache=str(tmp_path / "tune.json"))   # cache hit
     assert again["config"] == entry["config"]
     bt.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_apply_on_resident_blocks(workload, prec):
+    """H.psi without a rebuild: right after creation (FP32 split made on
+    first use), equal to the full step on the same psi bit for bit, and a
+    new psi gives the single-system energies."""
+    from detnqs_b200 import batch as B
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    from detnqs_b200 import synthetic as S
+    P = N.F64 if prec == "f64" else N.F32
+    w, ctxs = workload
+    bt = B.Batch(ctxs, [x.dets for x in w], [x.sysm.n_orb for x in w], eps1=1e-7)
+    psi = np.concatenate([S.normalized_psi(len(x.dets), 40 + k) for k, x in enumerate(w)])
+    e_fresh, _ = bt.apply(psi, precision=P)
+    e_step, _ = bt.step(psi, precision=P)
+    e_app, _ = bt.apply(psi, precision=P)
+    e_app_g, _ = bt.apply(psi, precision=P, graph=True)
+    np.testing.assert_array_equal(e_fresh, e_step)
+    np.testing.assert_array_equal(e_app, e_step)
+    np.testing.assert_array_equal(e_app_g, e_step)
+    psi2 = np.concatenate([S.normalized_psi(len(x.dets), 90 + k) for k, x in enumerate(w)])
+    eloc = np.empty(bt.total)
+    e2, _ = bt.apply(psi2, precision=P, graph=True, eloc=eloc)
+    for k, (bs, c) in enumerate(zip(w, ctxs)):
+        H = D.build(c, bs.dets, n_orb=bs.sysm.n_orb, policy=N.POLICY_STATIC,
+                    use_heatbath=True, eps1=1e-7, want_vp=False)
+        x = psi2[bt.offsets[k]:bt.offsets[k + 1]]
+        el = np.empty(len(x))
+        num, den = H.local_energy(x, eloc=el, precision=P)
+        tol = 1e-12 if prec == "f64" else 1e-6
+        assert abs(e2[k, 0] / e2[k, 1] - num / den) < tol
+        np.testing.assert_allclose(eloc[bt.offsets[k]:bt.offsets[k + 1]], el, rtol=1e-12 if
+                                   prec == "f64" else 1e-5, atol=1e-9)
+        H.close()
+    t = bt.timings()
+    assert set(t) == {"diag", "build", "compact", "hpsi"} and t["build"] > 0
+    bt.close()
