@@ -557,7 +557,11 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
                 cpos = out.w;
                 break;
             }
-            if ((i64)out.c > A.chunk || attempt == 1) {   // longer than any chunk
+            // Only rows of at most chunk/4 entries restart in a fresh chunk,
+            // so every retired chunk is at least 3/4 full and the arena
+            // never needs more than 4/3 nnz + (warps + 1) chunks; longer
+            // rows take the exact second pass.
+            if (4 * (i64)out.c > A.chunk || attempt == 1) {
                 if (lane == 0) {
                     A.row_len[g] = out.c;
                     A.big[atomicAdd(A.n_big, 1)] = (u32)g;
@@ -686,6 +690,12 @@ i64 g_arena_chunk = 0;
 i64 g_arena_cap = 0;
 
 namespace {
+
+// Arena entries that always suffice for a matrix of nnz entries built by
+// `grid` blocks (see the restart rule of k_vv_arena).
+i64 arena_bound(i64 nnz, int grid, i64 chunk) {
+    return nnz + nnz / 3 + 1 + ((i64)grid * kWS + 1) * chunk;
+}
 
 template <class Loc>
 int vv_grid(int device) {
@@ -1041,7 +1051,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
-    b->cap = nnz + nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
+    b->cap = arena_bound(nnz, grid, b->chunk);
     b->acol.alloc(b->cap, s);
     b->aval.alloc(b->cap, s);
     b->rlen.alloc(n + 1, s);
@@ -1302,7 +1312,7 @@ int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3) {
     upload_params(b, nullptr);
     if (resize) {   // larger chunks need a larger arena
         const int grid = vv_grid<ManySys>(b->device);
-        b->cap = b->M.nnz + b->M.nnz / 8 + (i64)grid * kWS * b->chunk + b->chunk;
+        b->cap = arena_bound(b->M.nnz, grid, b->chunk);
         b->acol.alloc(b->cap, nullptr);
         b->aval.alloc(b->cap, nullptr);
         DNQ_CUDA(cudaStreamSynchronize(nullptr));
