@@ -58,13 +58,16 @@ class Batch:
 
     @property
     def config(self):
-        c = np.zeros(3, np.int64)
+        """(arena chunk, part-C search threshold, H.psi lanes per row,
+        H.psi slots per lane); 0 = automatic for the last two."""
+        c = np.zeros(4, np.int64)
         N.check(N.lib.dnq_batch_get_config(self._h, c.ctypes.data))
         return tuple(int(x) for x in c)
 
     @config.setter
     def config(self, cfg):
-        c = np.asarray(cfg, np.int64)
+        c = np.zeros(4, np.int64)
+        c[:len(cfg)] = cfg
         N.check(N.lib.dnq_batch_set_config(self._h, c.ctypes.data))
 
     def step(self, psi, *, precision: int = N.F32, graph: bool = False, stream=None,
@@ -125,7 +128,8 @@ def _side_stream():
 
 CHUNKS = (2048, 8192, 32768)
 GROUPS = (512, 2048, 8192)
-LANES = (0, 8, 16, 32)
+LANES = (4, 8, 16, 32)
+SLOTS = (1, 2, 4)
 
 
 def signature(batch: Batch) -> str:
@@ -135,19 +139,21 @@ def signature(batch: Batch) -> str:
     return f"sys{batch.n_sys}-rows{int(np.log2(max(rows, 1)))}-nnz{int(np.log2(max(per_row, 1)))}"
 
 
-def _time(batch: Batch, psi, reps: int, precision: int) -> float:
+def _time(batch: Batch, psi, reps: int, precision: int, apply: bool = False) -> float:
     ts = []
+    run = batch.apply if apply else batch.step
     for _ in range(reps):
-        _, ms = batch.step(psi, precision=precision)
+        _, ms = run(psi, precision=precision)
         ts.append(ms)
     return float(np.median(ts))
 
 
 def autotune(batch: Batch, psi, *, reps: int = 3, precision: int = N.F32,
              cache: str | None = None) -> dict:
-    """Coordinate search: (chunk, group threshold) with automatic lanes,
-    then the lanes per row of H.psi.  The winner is set on the batch and
-    stored under the workload signature in ``cache`` (JSON) if given."""
+    """Coordinate search: (chunk, group threshold) of the build timed on the
+    full step with automatic H.psi shape, then (lanes per row, slots per
+    lane) of H.psi timed on H.psi alone.  The winner is set on the batch
+    and stored under the workload signature in ``cache`` (JSON) if given."""
     key = signature(batch)
     if cache and os.path.exists(cache):
         with open(cache) as f:
@@ -160,20 +166,25 @@ def autotune(batch: Batch, psi, *, reps: int = 3, precision: int = N.F32,
     best = None
     for ch in CHUNKS:
         for g in GROUPS:
-            batch.config = (ch, g, 0)
+            batch.config = (ch, g, 0, 0)
             t = _time(batch, psi, reps, precision)
-            results.append(((ch, g, 0), t))
+            results.append(((ch, g, 0, 0), t))
             if best is None or t < best[1]:
-                best = ((ch, g, 0), t)
-    ch, g, _ = best[0]
-    for lanes in LANES[1:]:
-        batch.config = (ch, g, lanes)
-        t = _time(batch, psi, reps, precision)
-        results.append(((ch, g, lanes), t))
-        if t < best[1]:
-            best = ((ch, g, lanes), t)
-    batch.config = best[0]
-    entry = {"config": list(best[0]), "ms": best[1], "signature": key,
+                best = ((ch, g, 0, 0), t)
+    ch, g = best[0][:2]
+    batch.config = (ch, g, 0, 0)
+    batch.step(psi, precision=precision)
+    hbest = None
+    for lanes in LANES:
+        for slots in SLOTS:
+            batch.config = (ch, g, lanes, slots)
+            t = _time(batch, psi, reps, precision, apply=True)
+            results.append(((ch, g, lanes, slots), t))
+            if hbest is None or t < hbest[1]:
+                hbest = ((ch, g, lanes, slots), t)
+    batch.config = hbest[0]
+    best = (hbest[0], _time(batch, psi, reps, precision))
+    entry = {"config": list(best[0]), "ms": best[1], "hpsi_ms": hbest[1], "signature": key,
              "tried": [[list(c), t] for c, t in results],
              "tune_seconds": time.perf_counter() - t0}
     if cache:

@@ -399,6 +399,7 @@ struct PhaseTimer {
 bool g_force_walk = false;
 extern i64 g_arena_chunk;
 extern i64 g_arena_cap;
+void spmv_set_option(int lanes, int unroll);
 
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
@@ -771,11 +772,19 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
 
 int dnq_set_option(int option, int64_t value) {
     DNQ_API_BEGIN
-    require(option >= 1 && option <= 3, DNQ_ERR_INVALID, "unknown option");
+    require(option >= 1 && option <= 5, DNQ_ERR_INVALID, "unknown option");
     require(value >= 0, DNQ_ERR_INVALID, "option value must be >= 0");
+    if (option == 4)
+        require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
+                DNQ_ERR_INVALID, "lanes per row must be 0, 4, 8, 16 or 32");
+    if (option == 5)
+        require(value == 0 || value == 1 || value == 2 || value == 4, DNQ_ERR_INVALID,
+                "slots per lane must be 0, 1, 2 or 4");
     if (option == 1) g_force_walk = value != 0;
     if (option == 2) g_arena_chunk = value;
     if (option == 3) g_arena_cap = value;
+    if (option == 4) spmv_set_option((int)value, -1);
+    if (option == 5) spmv_set_option(-1, (int)value);
     DNQ_API_END
 }
 

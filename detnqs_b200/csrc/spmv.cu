@@ -77,103 +77,104 @@ __device__ __forceinline__ Dot2<T> shfl_xor(const Dot2<T>& d, int o, unsigned ma
     return r;
 }
 
-// One group of G lanes per row (G in {4, 8, 16, 32}); each lane reads 4
-// consecutive entries per step with 128-bit loads (cols: one uint4; values:
-// two double2 / one float4), starting from the row start rounded down to a
-// multiple of 4 and masking entries outside the row, so a warp streams 128
-// entries per step.  The tail of the arrays is read with scalar loads.
-template <int G>
-__global__ void __launch_bounds__(256)
-k_spmv_f64(const i64* __restrict__ rp, const u32* __restrict__ col,
-           const double* __restrict__ val, const double* __restrict__ x, i64 nr, i64 nnz,
-           double* __restrict__ y, const double* __restrict__ yadd) {
-    const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
-    const int sub = threadIdx.x & (G - 1);
-    const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
-    const i64 rounds = (nr + ngroups - 1) / ngroups;
-    for (i64 it = 0; it < rounds; ++it) {
-        const i64 r = gid + it * ngroups;
-        double acc = 0.0;
-        if (r < nr) {
-            const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-            for (i64 k = (b & ~3ll) + 4 * sub; k < e; k += 4 * G) {
-                u32 c[4];
-                double v[4];
-                if (k + 3 < nnz) {
-                    const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + k));
-                    const double2 v01 = __ldg(reinterpret_cast<const double2*>(val + k));
-                    const double2 v23 = __ldg(reinterpret_cast<const double2*>(val + k + 2));
-                    c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
-                    v[0] = v01.x; v[1] = v01.y; v[2] = v23.x; v[3] = v23.y;
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        c[q] = k + q < nnz ? __ldg(&col[k + q]) : 0u;
-                        v[q] = k + q < nnz ? __ldg(&val[k + q]) : 0.0;
-                    }
-                }
-                double xv[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const bool in = k + q >= b && k + q < e;
-                    xv[q] = in ? __ldg(&x[c[q]]) : 0.0;
-                    if (!in) v[q] = 0.0;
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc = fma(v[q], xv[q], acc);
-            }
-        }
-#pragma unroll
-        for (int o = G / 2; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (sub == 0 && r < nr) y[r] = yadd ? acc + yadd[r] : acc;
+// Row accumulators: FP64 plain fused multiply-add, FP32 Dot2.
+struct AccF64 {
+    double s = 0.0;
+    __device__ __forceinline__ void add_prod(double v, double x) { s = fma(v, x, s); }
+    __device__ __forceinline__ void reduce(int G) {
+        for (int o = G / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     }
+    __device__ __forceinline__ double value() const { return s; }
+};
+
+struct AccF32 {
+    Dot2<float> d;
+    __device__ __forceinline__ void add_prod(float v, float x) { d.add_prod(v, x); }
+    __device__ __forceinline__ void reduce(int G) {
+        for (int o = G / 2; o; o >>= 1) d.merge(shfl_xor(d, o, 0xffffffffu));
+    }
+    __device__ __forceinline__ double value() const { return (double)d.s + (double)d.c; }
+};
+
+// Four consecutive values from a 16-byte aligned position, streamed past L1
+// (the values are used once; L1 and L2 stay with x).
+__device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
+    const float4 a = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
 }
 
-template <int G>
+// One group of G lanes per row (G in {4, 8, 16, 32}).  Lane `sub` owns the
+// 4-entry slots k = (b & ~3) + 4 sub + 4 G t, t = 0, 1, ...: it reads each
+// slot with 128-bit loads (cols: one uint4; values: two double2 or one
+// float4), masks entries outside [b, e), and accumulates its slots in
+// ascending t; the G lane sums are then combined by a butterfly.  U slots
+// are loaded before any is used, so a lane keeps U column/value loads and
+// 4U gathers of x in flight; the order of accumulation does not depend on U
+// (results are identical for every U).  The last entries of the arrays are
+// read with scalar loads.
+//   T = double: y_r = sum H_rk x_k                         (val, x)
+//   T = float : y_r = Dot2 sum of val32 * x32 + diag_r x_r (FP32 off-diagonal
+//               values, FP64 diagonal term)
+template <int G, int U, class T, class Acc>
 __global__ void __launch_bounds__(256)
-k_spmv_f32c(const i64* __restrict__ rp, const u32* __restrict__ col,
-            const float* __restrict__ val, const float* __restrict__ x32,
-            const double* __restrict__ diag, const double* __restrict__ x, i64 nr, i64 nnz,
-            double* __restrict__ y, const double* __restrict__ yadd) {
+k_spmv(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restrict__ val,
+       const T* __restrict__ xg, const double* __restrict__ diag,
+       const double* __restrict__ x, i64 nr, i64 nnz, double* __restrict__ y,
+       const double* __restrict__ yadd) {
     const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
     const int sub = threadIdx.x & (G - 1);
     const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
     const i64 rounds = (nr + ngroups - 1) / ngroups;
     for (i64 it = 0; it < rounds; ++it) {
         const i64 r = gid + it * ngroups;
-        Dot2<float> acc;
+        Acc acc;
         if (r < nr) {
             const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-            for (i64 k = (b & ~3ll) + 4 * sub; k < e; k += 4 * G) {
-                u32 c[4];
-                float v[4];
-                if (k + 3 < nnz) {
-                    const uint4 c4 = __ldg(reinterpret_cast<const uint4*>(col + k));
-                    const float4 v4 = __ldg(reinterpret_cast<const float4*>(val + k));
-                    c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
-                    v[0] = v4.x; v[1] = v4.y; v[2] = v4.z; v[3] = v4.w;
-                } else {
+            for (i64 k0 = (b & ~3ll) + 4 * sub; k0 < e; k0 += 4 * G * U) {
+                u32 c[U][4];
+                T v[U][4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        c[q] = k + q < nnz ? __ldg(&col[k + q]) : 0u;
-                        v[q] = k + q < nnz ? __ldg(&val[k + q]) : 0.0f;
+                for (int u = 0; u < U; ++u) {
+                    const i64 k = k0 + (i64)u * 4 * G;
+                    if (k + 3 < nnz && k < e) {
+                        const uint4 c4 = __ldcs(reinterpret_cast<const uint4*>(col + k));
+                        c[u][0] = c4.x; c[u][1] = c4.y; c[u][2] = c4.z; c[u][3] = c4.w;
+                        load4(val + k, v[u]);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const bool ok = k < e && k + q < nnz;
+                            c[u][q] = ok ? __ldg(&col[k + q]) : 0u;
+                            v[u][q] = ok ? __ldg(&val[k + q]) : T(0);
+                        }
                     }
                 }
-                float xv[4];
+                T xv[U][4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const bool in = k + q >= b && k + q < e;
-                    xv[q] = in ? __ldg(&x32[c[q]]) : 0.0f;
-                    if (!in) v[q] = 0.0f;
-                }
+                for (int u = 0; u < U; ++u)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc.add_prod(v[q], xv[q]);
+                    for (int q = 0; q < 4; ++q) {
+                        const i64 kk = k0 + (i64)u * 4 * G + q;
+                        const bool in = kk >= b && kk < e;
+                        xv[u][q] = in ? __ldg(&xg[c[u][q]]) : T(0);
+                        if (!in) v[u][q] = T(0);
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (k0 + (i64)u * 4 * G < e) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc.add_prod(v[u][q], xv[u][q]);
+                    }
             }
         }
-#pragma unroll
-        for (int o = G / 2; o; o >>= 1) acc.merge(shfl_xor(acc, o, 0xffffffffu));
+        acc.reduce(G);
         if (sub == 0 && r < nr) {
-            double v = (double)acc.s + (double)acc.c;
+            double v = acc.value();
             if (diag) v += diag[r] * x[r];
             y[r] = yadd ? v + yadd[r] : v;
         }
@@ -243,59 +244,88 @@ int group_for(const Csr& m) {
     return 4;
 }
 
-int spmv_grid(int device) { return sm_count(device) * 8; }
+// Slots in flight per lane: as many as the average row fills, at most 4.
+int unroll_for(const Csr& m, int G) {
+    const double avg = m.nr ? (double)m.nnz / (double)m.nr : 0.0;
+    const double slots = avg / (4.0 * G);
+    if (slots >= 4) return 4;
+    if (slots >= 2) return 2;
+    return 1;
+}
+
+template <class K>
+int blocks_for(K kern, int device) {
+    int per_sm = 0;
+    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+    return std::max(1, per_sm) * sm_count(device);
+}
+
+template <int G, int U>
+void launch_gu(const Csr& m, const double* x, double* y, const double* yadd, int precision,
+               const float* x32, const float* val32, const double* diag, int device,
+               cudaStream_t s) {
+    if (precision == DNQ_F64 || m.nnz == 0) {
+        auto kern = k_spmv<G, U, double, AccF64>;
+        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, nullptr,
+                                                      x, m.nr, m.nnz, y, yadd);
+    } else {
+        auto kern = k_spmv<G, U, float, AccF32>;
+        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x,
+                                                      m.nr, m.nnz, y, yadd);
+    }
+}
+
+template <int G>
+void launch_g(int U, const Csr& m, const double* x, double* y, const double* yadd,
+              int precision, const float* x32, const float* val32, const double* diag,
+              int device, cudaStream_t s) {
+    switch (U) {
+        case 4: launch_gu<G, 4>(m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+        case 2: launch_gu<G, 2>(m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+        default: launch_gu<G, 1>(m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+    }
+}
+
+// Lanes per row / slots per lane forced by dnq_set_option (0 = automatic).
+int g_spmv_lanes = 0;
+int g_spmv_unroll = 0;
+
+void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, int precision,
+                 const float* x32, const float* val32, const double* diag, int G, int U,
+                 int device, cudaStream_t s) {
+    if (m.nr == 0) return;
+    if (G == 0) G = g_spmv_lanes ? g_spmv_lanes : group_for(m);
+    if (U == 0) U = g_spmv_unroll ? g_spmv_unroll : unroll_for(m, G);
+    switch (G) {
+        case 32: launch_g<32>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+        case 16: launch_g<16>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+        case 8: launch_g<8>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+        default: launch_g<4>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
+    }
+    DNQ_CHECK_LAUNCH();
+}
 
 }  // namespace
 
-// Same as spmv_block with the lanes-per-row group given (0 = automatic).
+void spmv_set_option(int lanes, int unroll) {
+    if (lanes >= 0) g_spmv_lanes = lanes;
+    if (unroll >= 0) g_spmv_unroll = unroll;
+}
+
+// Same as spmv_block with lanes per row G and slots per lane U given
+// (0 = automatic).
 void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
                   cudaStream_t s, const float* x32, const float* val32, const double* diag,
-                  int G, int device) {
-    if (m.nr == 0) return;
-    if (G == 0) G = group_for(m);
-    const int grid = spmv_grid(device), bs = 256;
+                  int G, int device, int U) {
     (void)h;
-    if (precision == DNQ_F64 || m.nnz == 0) {
-        switch (G) {
-            case 32: k_spmv_f64<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
-            case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
-            case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
-            default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, nullptr); break;
-        }
-    } else {
-        switch (G) {
-            case 32: k_spmv_f32c<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
-            case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
-            case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
-            default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x, m.nr, m.nnz, y, nullptr); break;
-        }
-    }
-    DNQ_CHECK_LAUNCH();
+    launch_spmv(m, x, y, nullptr, precision, x32, val32, diag, G, U, device, s);
 }
 
 // y (+)= M x for one block; x FP64 device, y FP64 device.
 void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
                 const double* yadd, int precision, cudaStream_t s, float* x32,
                 const double* diag) {
-    if (m.nr == 0) return;
-    const int G = group_for(m);
-    const int grid = spmv_grid(h->device), bs = 256;
-    if (precision == DNQ_F64 || m.nnz == 0) {
-        switch (G) {
-            case 32: k_spmv_f64<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
-            case 16: k_spmv_f64<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
-            case 8: k_spmv_f64<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
-            default: k_spmv_f64<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, m.nr, m.nnz, y, yadd); break;
-        }
-    } else {
-        switch (G) {
-            case 32: k_spmv_f32c<32><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
-            case 16: k_spmv_f32c<16><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
-            case 8: k_spmv_f32c<8><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
-            default: k_spmv_f32c<4><<<grid, bs, 0, s>>>(m.rowptr.p, m.col.p, m.val32.p, x32, diag, x, m.nr, m.nnz, y, yadd); break;
-        }
-    }
-    DNQ_CHECK_LAUNCH();
+    launch_spmv(m, x, y, yadd, precision, x32, m.val32.p, diag, 0, 0, h->device, s);
 }
 
 void to_f32(const double* x, i64 n, float* o, cudaStream_t s) {

@@ -873,7 +873,7 @@ namespace dnq {
 void launch_f32_split(const Csr& m, float* val32, double* diag_out, cudaStream_t s);
 void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
                   cudaStream_t s, const float* x32, const float* val32, const double* diag,
-                  int G, int device);
+                  int G, int device, int U);
 void to_f32(const double* x, i64 n, float* o, cudaStream_t s);
 
 namespace {
@@ -998,6 +998,7 @@ struct dnq_batch_s {
     dnq::i64 chunk = dnq::kChunk;
     dnq::u32 big_group = dnq::kBigGroup;
     int spmv_group = 0;
+    int spmv_unroll = 0;
     // graphs: [0] full step (build + H.psi), [1] H.psi on the resident CSR
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_prec[2] = {-1, -1};
@@ -1085,10 +1086,10 @@ void enqueue_apply(dnq_batch_s* b, int precision, cudaStream_t s) {
     if (precision == DNQ_F32) {
         to_f32(b->x.p, b->total, b->x32.p, s);
         spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F32, s, b->x32.p, b->val32.p,
-                     b->diag_op.p, b->spmv_group, b->device);
+                     b->diag_op.p, b->spmv_group, b->device, b->spmv_unroll);
     } else {
         spmv_block_g(nullptr, b->M, b->x.p, b->y.p, DNQ_F64, s, nullptr, nullptr, nullptr,
-                     b->spmv_group, b->device);
+                     b->spmv_group, b->device, b->spmv_unroll);
     }
     k_energy_sys<<<b->n_sys, 256, 0, s>>>(b->row_off.p, b->x.p, b->y.p, b->eloc.p, b->e2.p);
     DNQ_CHECK_LAUNCH();
@@ -1297,18 +1298,21 @@ int dnq_batch_info(dnq_batch_t b, int64_t* info4) {
     DNQ_API_END
 }
 
-int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3) {
+int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg4) {
     DNQ_API_BEGIN
-    require(b && cfg3, DNQ_ERR_INVALID, "null argument");
-    require(cfg3[0] >= 64 && cfg3[0] <= (1 << 20), DNQ_ERR_INVALID, "chunk out of range");
-    require(cfg3[1] >= 32, DNQ_ERR_INVALID, "group threshold out of range");
-    require(cfg3[2] == 0 || cfg3[2] == 4 || cfg3[2] == 8 || cfg3[2] == 16 || cfg3[2] == 32,
+    require(b && cfg4, DNQ_ERR_INVALID, "null argument");
+    require(cfg4[3] == 0 || cfg4[3] == 1 || cfg4[3] == 2 || cfg4[3] == 4, DNQ_ERR_INVALID,
+            "slots per lane must be 0, 1, 2 or 4");
+    require(cfg4[0] >= 64 && cfg4[0] <= (1 << 20), DNQ_ERR_INVALID, "chunk out of range");
+    require(cfg4[1] >= 32, DNQ_ERR_INVALID, "group threshold out of range");
+    require(cfg4[2] == 0 || cfg4[2] == 4 || cfg4[2] == 8 || cfg4[2] == 16 || cfg4[2] == 32,
             DNQ_ERR_INVALID, "lanes per row must be 0, 4, 8, 16 or 32");
     DeviceGuard g(b->device);
-    const bool resize = cfg3[0] > b->chunk;
-    b->chunk = cfg3[0];
-    b->big_group = (u32)cfg3[1];
-    b->spmv_group = (int)cfg3[2];
+    const bool resize = cfg4[0] > b->chunk;
+    b->chunk = cfg4[0];
+    b->big_group = (u32)cfg4[1];
+    b->spmv_group = (int)cfg4[2];
+    b->spmv_unroll = (int)cfg4[3];
     upload_params(b, nullptr);
     if (resize) {   // larger chunks need a larger arena
         const int grid = vv_grid<ManySys>(b->device);
@@ -1328,12 +1332,13 @@ int dnq_batch_timings(dnq_batch_t b, double* ms4) {
     DNQ_API_END
 }
 
-int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3) {
+int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg4) {
     DNQ_API_BEGIN
-    require(b && cfg3, DNQ_ERR_INVALID, "null argument");
-    cfg3[0] = b->chunk;
-    cfg3[1] = b->big_group;
-    cfg3[2] = b->spmv_group;
+    require(b && cfg4, DNQ_ERR_INVALID, "null argument");
+    cfg4[0] = b->chunk;
+    cfg4[1] = b->big_group;
+    cfg4[2] = b->spmv_group;
+    cfg4[3] = b->spmv_unroll;
     DNQ_API_END
 }
 

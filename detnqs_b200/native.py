@@ -32,6 +32,11 @@ POLICY_STATIC = 1
 POLICY_DYNAMIC = 2
 F64 = 0
 F32 = 1
+OPT_FORCE_WALK = 1
+OPT_ARENA_CHUNK = 2
+OPT_ARENA_CAP = 3
+OPT_SPMV_LANES = 4
+OPT_SPMV_UNROLL = 5
 
 # Every symbol the header declares; tests check the library exports them.
 EXPORTS = (

@@ -117,8 +117,14 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          build (0 = default 8192);
  *   DNQ_OPT_ARENA_CAP   n: arena capacity in entries (0 = automatic); a
  *                          too-small arena falls back to an exact two-pass
- *                          build. */
-enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3 };
+ *                          build;
+ *   DNQ_OPT_SPMV_LANES  n: lanes per row of H.psi, 0/4/8/16/32 (0 = by the
+ *                          average row length);
+ *   DNQ_OPT_SPMV_UNROLL n: 4-entry slots each lane keeps in flight, 0/1/2/4
+ *                          (0 = by the average row length).  Results do
+ *                          not depend on it. */
+enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
+       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */
@@ -253,10 +259,11 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
 int dnq_batch_destroy(dnq_batch_t b);
 /* info4 = {n_sys, total rows, nnz, device bytes of the planned buffers} */
 int dnq_batch_info(dnq_batch_t b, int64_t* info4);
-/* cfg3 = {arena chunk entries, part-C search threshold, lanes per row of
- * H.psi (0 = by row length)}: the tunables the autotuner chooses. */
-int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg3);
-int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg3);
+/* cfg4 = {arena chunk entries, part-C search threshold, lanes per row of
+ * H.psi (0 = by row length), 4-entry slots in flight per lane of H.psi
+ * (0 = by row length)}: the tunables the autotuner chooses. */
+int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg4);
+int dnq_batch_get_config(dnq_batch_t b, int64_t* cfg4);
 /* psi: concatenated amplitudes (host or device); eloc (total rows) and
  * energies (2 per system) may be NULL; *step_ms = device time of the step. */
 int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc,

@@ -389,3 +389,37 @@ def test_arena_paths_match(core, chunk, cap):
     np.testing.assert_allclose(B.spmv(x), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
     A.close()
     B.close()
+
+
+def test_spmv_every_lane_and_slot_count(core):
+    """H.psi for every (lanes per row, slots per lane): for fixed lanes the
+    result does not depend on the slots in flight (same order of
+    accumulation), and every form agrees with SciPy."""
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(18, 6, 6, 36, 23)
+    V = S.heat_bath_sample(sysm, 12000, 3)
+    ctx = core.IntCtx.from_arrays(18, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    H = D.build(ctx, V, n_orb=18, policy=1, use_heatbath=True, eps1=1e-7, want_vp=False)
+    x = S.normalized_psi(len(V), 5)
+    ref = H.to_scipy(0).dot(x)
+    scale = np.abs(ref).max()
+    try:
+        for G in (4, 8, 16, 32):
+            N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, G))
+            first = {}
+            for U in (1, 2, 4):
+                N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, U))
+                for prec in (N.F64, N.F32):
+                    y = H.spmv(x, precision=prec)
+                    if prec in first:
+                        np.testing.assert_array_equal(y, first[prec])
+                    else:
+                        first[prec] = y
+                    tol = 1e-12 if prec == N.F64 else 1e-6
+                    np.testing.assert_allclose(y, ref, rtol=0, atol=tol * scale)
+    finally:
+        N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 0))
+        N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, 0))
+    H.close()
