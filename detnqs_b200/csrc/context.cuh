@@ -22,6 +22,7 @@
 // reads at all.
 #pragma once
 
+#include <atomic>
 #include <vector>
 
 #include "common.cuh"
@@ -72,7 +73,7 @@ struct dnq_ctx_s {
     dnq::PairTable tab;
     bool has_hb = false;
     double hb_thr = 0.0;
-    long long vv_nnz_hint = 0;   // largest H_VV built on this context (arena sizing)
+    std::atomic<long long> vv_nnz_hint{0};   // largest H_VV built here (arena sizing)
 
     dnq::CtxView view() const {
         dnq::CtxView c;

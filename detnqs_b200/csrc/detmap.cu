@@ -141,7 +141,8 @@ void build_detmap(DetMap& m, const u64* dets, i64 n, bool strict, cudaStream_t s
     m.full_alpha_idx = full_alpha == ~0ull ? -1 : (long long)full_alpha;
     if (m.full_alpha_idx >= 0) {
         u64 b;
-        DNQ_CUDA(cudaMemcpy(&b, dets + 2 * full_alpha + 1, 8, cudaMemcpyDeviceToHost));
+        DNQ_CUDA(cudaMemcpyAsync(&b, dets + 2 * full_alpha + 1, 8, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
         m.full_alpha_beta = b;
     }
     if (n == 0) return;

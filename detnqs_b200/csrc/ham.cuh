@@ -50,6 +50,23 @@ namespace dnq {
 void sort_rows(Csr& m, cudaStream_t s);
 // sort_rows unless the block is already sorted.
 void ensure_sorted(Csr& m, cudaStream_t s);
+// One operator of a grouped H.psi launch: y = M x (+ diag .* x when diag is
+// given).  val / xg are double (FP64) or float (FP32 values and x).
+struct SpmvDesc {
+    const i64* rp;
+    const u32* col;
+    const void* val;
+    const void* xg;
+    const double* diag;
+    const double* x;
+    double* y;
+    i64 nr, nnz;
+};
+// Lanes per row and slots per lane the H.psi kernels use for m.
+void spmv_shape(const Csr& m, int& G, int& U);
+// One launch over nd descriptors (device array) sharing (G, U, precision).
+void spmv_grouped(const SpmvDesc* d_dev, int nd, i64 max_rows, int G, int U, int precision,
+                  int device, cudaStream_t s);
 // FP32 off-diagonal value copy of a square block (diagonal entries zeroed)
 // and, when diag_out is given, the FP64 diagonal entries (0 where absent).
 void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out = nullptr);

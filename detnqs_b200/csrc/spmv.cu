@@ -121,6 +121,54 @@ __device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
 //   T = float : y_r = Dot2 sum of val32 * x32 + diag_r x_r (FP32 off-diagonal
 //               values, FP64 diagonal term)
 template <int G, int U, class T, class Acc>
+__device__ __forceinline__ Acc row_acc(const i64* __restrict__ rp, const u32* __restrict__ col,
+                                       const T* __restrict__ val, const T* __restrict__ xg,
+                                       i64 r, bool valid, i64 nnz, int sub) {
+    Acc acc;
+    if (valid) {
+        const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
+        for (i64 k0 = (b & ~3ll) + 4 * sub; k0 < e; k0 += 4 * G * U) {
+            u32 c[U][4];
+            T v[U][4];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const i64 k = k0 + (i64)u * 4 * G;
+                if (k + 3 < nnz && k < e) {
+                    const uint4 c4 = __ldcs(reinterpret_cast<const uint4*>(col + k));
+                    c[u][0] = c4.x; c[u][1] = c4.y; c[u][2] = c4.z; c[u][3] = c4.w;
+                    load4(val + k, v[u]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const bool ok = k < e && k + q < nnz;
+                        c[u][q] = ok ? __ldg(&col[k + q]) : 0u;
+                        v[u][q] = ok ? __ldg(&val[k + q]) : T(0);
+                    }
+                }
+            }
+            T xv[U][4];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const i64 kk = k0 + (i64)u * 4 * G + q;
+                    const bool in = kk >= b && kk < e;
+                    xv[u][q] = in ? __ldg(&xg[c[u][q]]) : T(0);
+                    if (!in) v[u][q] = T(0);
+                }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (k0 + (i64)u * 4 * G < e) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc.add_prod(v[u][q], xv[u][q]);
+                }
+        }
+    }
+    acc.reduce(G);
+    return acc;
+}
+
+template <int G, int U, class T, class Acc>
 __global__ void __launch_bounds__(256)
 k_spmv(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restrict__ val,
        const T* __restrict__ xg, const double* __restrict__ diag,
@@ -132,51 +180,34 @@ k_spmv(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
     const i64 rounds = (nr + ngroups - 1) / ngroups;
     for (i64 it = 0; it < rounds; ++it) {
         const i64 r = gid + it * ngroups;
-        Acc acc;
-        if (r < nr) {
-            const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-            for (i64 k0 = (b & ~3ll) + 4 * sub; k0 < e; k0 += 4 * G * U) {
-                u32 c[U][4];
-                T v[U][4];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const i64 k = k0 + (i64)u * 4 * G;
-                    if (k + 3 < nnz && k < e) {
-                        const uint4 c4 = __ldcs(reinterpret_cast<const uint4*>(col + k));
-                        c[u][0] = c4.x; c[u][1] = c4.y; c[u][2] = c4.z; c[u][3] = c4.w;
-                        load4(val + k, v[u]);
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const bool ok = k < e && k + q < nnz;
-                            c[u][q] = ok ? __ldg(&col[k + q]) : 0u;
-                            v[u][q] = ok ? __ldg(&val[k + q]) : T(0);
-                        }
-                    }
-                }
-                T xv[U][4];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const i64 kk = k0 + (i64)u * 4 * G + q;
-                        const bool in = kk >= b && kk < e;
-                        xv[u][q] = in ? __ldg(&xg[c[u][q]]) : T(0);
-                        if (!in) v[u][q] = T(0);
-                    }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (k0 + (i64)u * 4 * G < e) {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc.add_prod(v[u][q], xv[u][q]);
-                    }
-            }
-        }
-        acc.reduce(G);
+        const Acc acc = row_acc<G, U, T, Acc>(rp, col, val, xg, r, r < nr, nnz, sub);
         if (sub == 0 && r < nr) {
             double v = acc.value();
             if (diag) v += diag[r] * x[r];
             y[r] = yadd ? v + yadd[r] : v;
+        }
+    }
+}
+
+// Many independent operators in one launch: blockIdx.y selects the
+// descriptor; every row is computed exactly as by k_spmv with the same
+// (G, U), so a result does not depend on the other members of the group.
+template <int G, int U, class T, class Acc>
+__global__ void __launch_bounds__(256) k_spmv_grouped(const SpmvDesc* __restrict__ descs) {
+    const SpmvDesc d = descs[blockIdx.y];
+    const T* val = static_cast<const T*>(d.val);
+    const T* xg = static_cast<const T*>(d.xg);
+    const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
+    const int sub = threadIdx.x & (G - 1);
+    const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
+    const i64 rounds = (d.nr + ngroups - 1) / ngroups;
+    for (i64 it = 0; it < rounds; ++it) {
+        const i64 r = gid + it * ngroups;
+        const Acc acc = row_acc<G, U, T, Acc>(d.rp, d.col, val, xg, r, r < d.nr, d.nnz, sub);
+        if (sub == 0 && r < d.nr) {
+            double v = acc.value();
+            if (d.diag) v += d.diag[r] * d.x[r];
+            d.y[r] = v;
         }
     }
 }
@@ -326,6 +357,48 @@ void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
                 const double* yadd, int precision, cudaStream_t s, float* x32,
                 const double* diag) {
     launch_spmv(m, x, y, yadd, precision, x32, m.val32.p, diag, 0, 0, h->device, s);
+}
+
+void spmv_shape(const Csr& m, int& G, int& U) {
+    G = g_spmv_lanes ? g_spmv_lanes : group_for(m);
+    U = g_spmv_unroll ? g_spmv_unroll : unroll_for(m, G);
+}
+
+namespace {
+template <int G, int U>
+void grouped_gu(const SpmvDesc* d, int nd, i64 max_rows, int precision, int device,
+                cudaStream_t s) {
+    auto launch = [&](auto kern) {
+        const i64 want = (max_rows * G + 255) / 256;
+        const int cap = blocks_for(kern, device);
+        const dim3 grid((unsigned)std::max<i64>(1, std::min<i64>(want, cap)), (unsigned)nd);
+        kern<<<grid, 256, 0, s>>>(d);
+    };
+    if (precision == DNQ_F64) launch(k_spmv_grouped<G, U, double, AccF64>);
+    else launch(k_spmv_grouped<G, U, float, AccF32>);
+}
+
+template <int G>
+void grouped_g(int U, const SpmvDesc* d, int nd, i64 max_rows, int precision, int device,
+               cudaStream_t s) {
+    switch (U) {
+        case 4: grouped_gu<G, 4>(d, nd, max_rows, precision, device, s); break;
+        case 2: grouped_gu<G, 2>(d, nd, max_rows, precision, device, s); break;
+        default: grouped_gu<G, 1>(d, nd, max_rows, precision, device, s); break;
+    }
+}
+}  // namespace
+
+void spmv_grouped(const SpmvDesc* d_dev, int nd, i64 max_rows, int G, int U, int precision,
+                  int device, cudaStream_t s) {
+    if (nd <= 0) return;
+    switch (G) {
+        case 32: grouped_g<32>(U, d_dev, nd, max_rows, precision, device, s); break;
+        case 16: grouped_g<16>(U, d_dev, nd, max_rows, precision, device, s); break;
+        case 8: grouped_g<8>(U, d_dev, nd, max_rows, precision, device, s); break;
+        default: grouped_g<4>(U, d_dev, nd, max_rows, precision, device, s); break;
+    }
+    DNQ_CHECK_LAUNCH();
 }
 
 void to_f32(const double* x, i64 n, float* o, cudaStream_t s) {

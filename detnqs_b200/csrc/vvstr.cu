@@ -848,9 +848,11 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     DNQ_CUDA(cudaEventRecord(e1, s));
     OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
     double tg = 0, tsc = 0, tc = 0;
-    H->candidates = run_vv(L, n, ctx->vv_nnz_hint, ctx->device, s, H->vv, &tg, &tsc, &tc);
+    H->candidates = run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc);
     H->vv.nc = n;
-    ctx->vv_nnz_hint = std::max<long long>(ctx->vv_nnz_hint, H->vv.nnz);
+    long long prev = ctx->vv_nnz_hint.load();   // shared by builds on other threads
+    while (prev < H->vv.nnz && !ctx->vv_nnz_hint.compare_exchange_weak(prev, H->vv.nnz)) {
+    }
     float ms = 0;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);

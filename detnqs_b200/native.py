@@ -37,6 +37,8 @@ OPT_ARENA_CHUNK = 2
 OPT_ARENA_CAP = 3
 OPT_SPMV_LANES = 4
 OPT_SPMV_UNROLL = 5
+REQ_BUILD = 0
+REQ_ELOC = 1
 
 # Every symbol the header declares; tests check the library exports them.
 EXPORTS = (
@@ -52,6 +54,8 @@ EXPORTS = (
     "dnq_pt2", "dnq_ham_local_energy_noalloc",
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
+    "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
+    "dnq_server_wait", "dnq_server_stats",
 )
 
 
@@ -129,6 +133,12 @@ _sig("dnq_batch_step", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
 _sig("dnq_batch_apply", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
 _sig("dnq_batch_timings", _P, _P)
 _sig("dnq_batch_copy_coo", _P, _I, _P, _P, _P, C.POINTER(_I64))
+_sig("dnq_server_create", _I, _I64, _I, _I, C.POINTER(_P))
+_sig("dnq_server_destroy", _P)
+_sig("dnq_server_add_system", _P, _P, _P, _I64, _I, _I, _I, _D, C.POINTER(_I))
+_sig("dnq_server_submit", _P, _I, _I, _P, _P, _I, C.POINTER(_I64))
+_sig("dnq_server_wait", _P, _I64, _D, _P, C.POINTER(_I64))
+_sig("dnq_server_stats", _P, _P)
 _sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_variational_energy", _P, _P, _I64, _P, _I, _I, _D, C.POINTER(_D), _P)
 _sig("dnq_ham_eff", _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _D, _I, _D, _I, _I,

@@ -70,6 +70,13 @@ def make_integrals(n_orb: int, n_chol: int, seed: int,
     # Symmetric Cholesky vectors, drawn on the packed triangle.
     n1e = n * (n + 1) // 2
     L = rng.normal(0.0, 0.1, size=(n_chol, n1e))
+    return _pack(h, L, n)
+
+
+def _pack(h: np.ndarray, L: np.ndarray, n: int) -> tuple[np.ndarray, np.ndarray]:
+    """Packed h1e from the dense symmetric h, packed ERIs from the Cholesky
+    vectors L[K, pair key]."""
+    n1e = n * (n + 1) // 2
     # G[k1, k2] = sum_K L[K, k1] L[K, k2]: one entry per unordered pair key.
     G = L.T @ L
     k1, k2 = np.tril_indices(n1e)
@@ -79,6 +86,34 @@ def make_integrals(n_orb: int, n_chol: int, seed: int,
     p, q = np.tril_indices(n)
     h1e[key[p, q]] = h[p, q]
     return h1e, eri
+
+
+def scan_family(n_orb: int, n_alpha: int, n_beta: int, n_chol: int, seed: int,
+                points: int = 10, amplitude: float = 0.02) -> list[SyntheticSystem]:
+    """A bond-scan-like family: a seeded base (same recipe as
+    :func:`make_integrals`) and ``points`` geometries whose h and Cholesky
+    vectors are the base scaled element-wise by 1 + amplitude * t * xi, with
+    t running evenly over [-1, 1] and xi ~ U(-1, 1) one seeded direction per
+    family; neighbouring points differ smoothly and the end points by up to
+    +-amplitude.  The ERIs stay positive semi-definite and 8-fold
+    symmetric."""
+    rng = np.random.default_rng(seed)
+    n = n_orb
+    diag = np.sort(rng.uniform(-20.0, 0.0, size=n))
+    off = rng.normal(0.0, 0.05, size=(n, n))
+    h = np.triu(off, 1)
+    h = h + h.T
+    h[np.arange(n), np.arange(n)] = diag
+    n1e = n * (n + 1) // 2
+    L = rng.normal(0.0, 0.1, size=(n_chol, n1e))
+    xi_h = rng.uniform(-1.0, 1.0, size=(n, n))
+    xi_h = np.triu(xi_h) + np.triu(xi_h, 1).T
+    xi_L = rng.uniform(-1.0, 1.0, size=L.shape)
+    out = []
+    for k, t in enumerate(np.linspace(-1.0, 1.0, points)):
+        h1e, eri = _pack(h * (1.0 + amplitude * t * xi_h), L * (1.0 + amplitude * t * xi_L), n)
+        out.append(SyntheticSystem(n, n_alpha, n_beta, h1e, eri, E_CORE, seed * 100 + k))
+    return out
 
 
 def make_system(n_orb: int, n_alpha: int, n_beta: int, n_chol: int,
@@ -355,6 +390,6 @@ def normalized_psi(n: int, seed: int) -> np.ndarray:
 __all__ = [
     "SyntheticSystem", "make_integrals", "make_system", "write_fcidump",
     "read_fcidump", "hf_determinant", "singles_doubles", "hf_sd_space",
-    "heat_bath_sample", "unpack_eri", "unpack_h1e", "normalized_psi",
+    "heat_bath_sample", "unpack_eri", "unpack_h1e", "normalized_psi", "scan_family",
     "pair_index", "E_CORE",
 ]

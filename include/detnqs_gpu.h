@@ -31,6 +31,7 @@ extern "C" {
 typedef struct dnq_ctx_s* dnq_ctx_t;    /* integrals + tables in HBM (IntCtx) */
 typedef struct dnq_ham_s* dnq_ham_t;    /* H_VV / H_VP / P-space in HBM      */
 typedef struct dnq_batch_s* dnq_batch_t;  /* many systems, one launch/phase  */
+typedef struct dnq_server_s* dnq_server_t;  /* device-resident request loop   */
 
 enum {
     DNQ_OK = 0,
@@ -282,6 +283,42 @@ int dnq_batch_timings(dnq_batch_t b, double* ms4);
 /* Sorted COO (local indices) of one system's block; *nnz always set. */
 int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols,
                        double* vals, int64_t* nnz);
+
+/* ---- serving loop (no reference counterpart) --------------------------------
+ * A server keeps screened H_VV blocks resident in device memory between
+ * requests and serves, for registered systems (context + determinant set):
+ *   DNQ_REQ_BUILD  build the system's H_VV (dnq_build, V->V only) and its
+ *                  FP32 operator copy; with psi also answers as ELOC;
+ *   DNQ_REQ_ELOC   local energies of psi on the resident block (built first
+ *                  when absent).
+ * build_slots worker threads build on their own streams; local-energy
+ * requests are grouped into one launch per (precision, H.psi shape) while the
+ * previous group runs (continuous batching).  Builds are admitted while the
+ * resident blocks plus the estimates of the builds in flight stay within
+ * budget_bytes, evicting least-recently-used idle blocks.  A request's result
+ * does not depend on the other requests served with it.
+ * psi (n doubles) and eloc (n doubles, may be NULL) are host memory the caller
+ * keeps valid until dnq_server_wait returns for the request. */
+enum { DNQ_REQ_BUILD = 0, DNQ_REQ_ELOC = 1 };
+int dnq_server_create(int device, int64_t budget_bytes, int build_slots, int max_group,
+                      dnq_server_t* out);
+int dnq_server_destroy(dnq_server_t s);
+/* Copies the determinants; the context must outlive the server. */
+int dnq_server_add_system(dnq_server_t s, dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
+                          int n_orb, int policy, int use_heatbath, double eps1,
+                          int* sys_id);
+int dnq_server_submit(dnq_server_t s, int kind, int sys_id, const double* psi,
+                      double* eloc, int precision, int64_t* req_id);
+/* Waits up to timeout_s; DNQ_ERR_TIMEOUT leaves the request pending.  On
+ * completion out4 = {psi.H psi, psi.psi, latency s (submit -> done), queue s
+ * (submit -> admission)}, *nnz = nnz of the block built by this request (0
+ * if none); the request's own status is returned and it is released. */
+int dnq_server_wait(dnq_server_t s, int64_t req_id, double timeout_s, double* out4,
+                    int64_t* nnz);
+/* st10 = {completed, failed, builds, grouped launches, mean group size,
+ *         largest group, evictions, resident bytes, peak bytes (resident +
+ *         reserved), resident blocks} */
+int dnq_server_stats(dnq_server_t s, double* st10);
 
 #ifdef __cplusplus
 }
