@@ -189,6 +189,7 @@ struct dnq_server_s {
     unsigned long long tick = 0;
     int free_slots = 1;
     bool stop = false;
+    bool paused = false;   // hold grouped launches (requests still admitted)
     std::vector<std::thread> workers;
     std::vector<cudaStream_t> wstreams;
     std::thread sched;
@@ -435,7 +436,7 @@ void scheduler(dnq_server_s* S) {
             else if (q != cudaErrorNotReady) fail_group(S, cudaGetErrorString(q));
         }
         admit(S);
-        if (!S->g_busy && !S->eloc_q.empty()) {
+        if (!S->g_busy && !S->eloc_q.empty() && !S->paused) {
             try {
                 launch_group(S);
             } catch (const std::exception& e) {
@@ -645,22 +646,35 @@ int dnq_server_wait(dnq_server_t S, int64_t req_id, double timeout_s, double* ou
     DNQ_API_END
 }
 
-int dnq_server_stats(dnq_server_t S, double* st10) {
+int dnq_server_pause(dnq_server_t S, int paused) {
     DNQ_API_BEGIN
-    require(S && st10, DNQ_ERR_INVALID, "null argument");
+    require(S, DNQ_ERR_INVALID, "null argument");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->paused = paused != 0;
+    }
+    S->cv_sched.notify_one();
+    DNQ_API_END
+}
+
+int dnq_server_stats(dnq_server_t S, double* st12) {
+    DNQ_API_BEGIN
+    require(S && st12, DNQ_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(S->mu);
     int resident = 0;
     for (auto& p : S->sys) resident += p->H != nullptr;
-    st10[0] = (double)S->n_done;
-    st10[1] = (double)S->n_failed;
-    st10[2] = (double)S->n_builds;
-    st10[3] = (double)S->n_groups;
-    st10[4] = S->n_groups ? (double)S->n_grouped / (double)S->n_groups : 0.0;
-    st10[5] = (double)S->max_seen_group;
-    st10[6] = (double)S->n_evict;
-    st10[7] = (double)S->used;
-    st10[8] = (double)S->peak;
-    st10[9] = (double)resident;
+    st12[0] = (double)S->n_done;
+    st12[1] = (double)S->n_failed;
+    st12[2] = (double)S->n_builds;
+    st12[3] = (double)S->n_groups;
+    st12[4] = S->n_groups ? (double)S->n_grouped / (double)S->n_groups : 0.0;
+    st12[5] = (double)S->max_seen_group;
+    st12[6] = (double)S->n_evict;
+    st12[7] = (double)S->used;
+    st12[8] = (double)S->peak;
+    st12[9] = (double)resident;
+    st12[10] = (double)S->pending.size();
+    st12[11] = (double)S->eloc_q.size();
     DNQ_API_END
 }
 

@@ -102,11 +102,17 @@ class Server:
                     "eloc": t.eloc}
         return t.result
 
+    def pause(self, paused: bool = True):
+        """Hold (or release) grouped local-energy launches; requests are
+        still admitted and builds still run."""
+        N.check(N.lib.dnq_server_pause(self._h, int(bool(paused))))
+
     def stats(self) -> dict:
-        st = np.zeros(10)
+        st = np.zeros(12)
         N.check(N.lib.dnq_server_stats(self._h, st.ctypes.data))
         keys = ("completed", "failed", "builds", "groups", "mean_group", "max_group",
-                "evictions", "resident_bytes", "peak_bytes", "resident_blocks")
+                "evictions", "resident_bytes", "peak_bytes", "resident_blocks", "pending",
+                "ready")
         return dict(zip(keys, (float(x) for x in st)))
 
 

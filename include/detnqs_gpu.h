@@ -315,10 +315,14 @@ int dnq_server_submit(dnq_server_t s, int kind, int sys_id, const double* psi,
  * if none); the request's own status is returned and it is released. */
 int dnq_server_wait(dnq_server_t s, int64_t req_id, double timeout_s, double* out4,
                     int64_t* nnz);
-/* st10 = {completed, failed, builds, grouped launches, mean group size,
+/* paused != 0 holds grouped local-energy launches (requests are still
+ * admitted and builds still run); 0 releases them. */
+int dnq_server_pause(dnq_server_t s, int paused);
+/* st12 = {completed, failed, builds, grouped launches, mean group size,
  *         largest group, evictions, resident bytes, peak bytes (resident +
- *         reserved), resident blocks} */
-int dnq_server_stats(dnq_server_t s, double* st10);
+ *         reserved), resident blocks, requests waiting for admission,
+ *         requests ready for the next grouped launch} */
+int dnq_server_stats(dnq_server_t s, double* st12);
 
 #ifdef __cplusplus
 }

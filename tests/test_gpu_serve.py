@@ -73,7 +73,35 @@ def test_alone_equals_mix(systems):
     mix, st = serve(items, ctxs, reqs, alone=False)
     assert_same(alone, mix)
     assert st["failed"] == 0 and st["completed"] == len(reqs)
-    assert st["max_group"] >= 2          # requests really were grouped
+
+
+def test_burst_is_grouped_and_unchanged(systems):
+    """Local-energy requests that collect while launches are held run as one
+    grouped launch, with the results they get one by one."""
+    import time
+    from detnqs_b200 import native as N
+    from detnqs_b200 import serve as V
+    from detnqs_b200 import synthetic as S
+    items, ctxs = systems
+    burst = [(k, S.normalized_psi(len(d), 500 + k), prec) for k, (_, d) in enumerate(items)
+             for prec in (N.F32, N.F64)]
+    with V.Server(budget_bytes=8e9, build_slots=3) as srv:
+        ids = [srv.add_system(c, d, s.n_orb, eps1=1e-7) for (s, d), c in zip(items, ctxs)]
+        for k in ids:
+            srv.wait(srv.submit(V.BUILD, k))
+        one = [srv.wait(srv.submit(V.ELOC, ids[k], psi, want_eloc=True, precision=p))
+               for k, psi, p in burst]
+        srv.pause(True)
+        ts = [srv.submit(V.ELOC, ids[k], psi, want_eloc=True, precision=p)
+              for k, psi, p in burst]
+        deadline = time.time() + 30
+        while srv.stats()["ready"] < len(burst) and time.time() < deadline:
+            time.sleep(0.01)
+        srv.pause(False)
+        grouped = [srv.wait(t) for t in ts]
+        st = srv.stats()
+    assert st["max_group"] == len(burst)
+    assert_same(one, grouped)
 
 
 def test_results_match_direct_api(systems):
