@@ -646,6 +646,19 @@ int dnq_server_wait(dnq_server_t S, int64_t req_id, double timeout_s, double* ou
     DNQ_API_END
 }
 
+int dnq_server_set_budget(dnq_server_t S, int64_t budget_bytes) {
+    DNQ_API_BEGIN
+    require(S, DNQ_ERR_INVALID, "null argument");
+    require(budget_bytes > 0, DNQ_ERR_INVALID, "budget must be positive");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->budget = budget_bytes;
+        S->peak = 0;   // the peak is tracked against the budget now in force
+    }
+    S->cv_sched.notify_one();
+    DNQ_API_END
+}
+
 int dnq_server_pause(dnq_server_t S, int paused) {
     DNQ_API_BEGIN
     require(S, DNQ_ERR_INVALID, "null argument");

@@ -55,7 +55,7 @@ EXPORTS = (
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
     "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
-    "dnq_server_wait", "dnq_server_pause", "dnq_server_stats",
+    "dnq_server_wait", "dnq_server_set_budget", "dnq_server_pause", "dnq_server_stats",
 )
 
 
@@ -138,6 +138,7 @@ _sig("dnq_server_destroy", _P)
 _sig("dnq_server_add_system", _P, _P, _P, _I64, _I, _I, _I, _D, C.POINTER(_I))
 _sig("dnq_server_submit", _P, _I, _I, _P, _P, _I, C.POINTER(_I64))
 _sig("dnq_server_wait", _P, _I64, _D, _P, C.POINTER(_I64))
+_sig("dnq_server_set_budget", _P, _I64)
 _sig("dnq_server_pause", _P, _I)
 _sig("dnq_server_stats", _P, _P)
 _sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))

@@ -102,6 +102,11 @@ class Server:
                     "eloc": t.eloc}
         return t.result
 
+    def set_budget(self, budget_bytes: float):
+        """New admission budget (idle blocks above it are evicted as builds
+        need room)."""
+        N.check(N.lib.dnq_server_set_budget(self._h, int(budget_bytes)))
+
     def pause(self, paused: bool = True):
         """Hold (or release) grouped local-energy launches; requests are
         still admitted and builds still run."""

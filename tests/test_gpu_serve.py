@@ -17,7 +17,7 @@ def systems():
     from detnqs_b200 import synthetic as S
     w = B.make_batch_workload(n_sys=5, seed=11, n_min=8, n_max=22, dets_min=300, dets_max=5000,
                               workers=1)
-    fam = S.scan_family(14, 5, 5, 28, 3, points=3)
+    fam = S.scan_family(14, 5, 5, 28, 3, points=6)
     Vf = S.heat_bath_sample(fam[0], 2000, 9, max_level=3)
     items = [(bs.sysm, bs.dets) for bs in w] + [(f, Vf) for f in fam]
     ctxs = []
@@ -128,15 +128,33 @@ def test_results_match_direct_api(systems):
 
 
 def test_small_budget_evicts_and_keeps_results(systems):
+    """With six same-size blocks resident (bond-scan points), shrink the
+    budget to half of them: later requests evict idle blocks and rebuild,
+    within the budget, and return what they returned before."""
+    from detnqs_b200 import native as N
+    from detnqs_b200 import serve as V
+    from detnqs_b200 import synthetic as S
     items, ctxs = systems
-    reqs = requests(items)
-    ref, st_ref = serve(items, ctxs, reqs, alone=False)
-    first = max(len(d) * min(len(d), 2048) * 32 + 64 * len(d) for _, d in items)
-    budget = first + 0.25 * st_ref["resident_bytes"]
-    got, st = serve(items, ctxs, reqs, alone=False, budget=budget, slots=2)
-    assert st["evictions"] > 0
+    scan = [k for k in range(len(items)) if len(items[k][1]) == len(items[-1][1])][-6:]
+    reqs = [(k, S.normalized_psi(len(items[k][1]), 700 + k)) for k in scan]
+    with V.Server(budget_bytes=8e9, build_slots=2) as srv:
+        ids = {k: srv.add_system(ctxs[k], items[k][1], items[k][0].n_orb, eps1=1e-7)
+               for k in scan}
+        ref = [srv.wait(srv.submit(V.ELOC, ids[k], psi, want_eloc=True, precision=N.F64))
+               for k, psi in reqs]
+        total = srv.stats()["resident_bytes"]
+        # a rebuild reserves 1.5 x (28 B per entry + 64 B per row)
+        need = max(1.5 * (28 * r["nnz"] + 64 * len(items[k][1])) for (k, _), r in zip(reqs, ref))
+        budget = max(total / 2, 1.05 * need)
+        assert budget < total
+        srv.set_budget(budget)
+        ts = [srv.submit(V.ELOC, ids[k], psi, want_eloc=True, precision=N.F64)
+              for k, psi in reqs * 3]
+        got = [srv.wait(t) for t in ts]
+        st = srv.stats()
+    assert st["evictions"] > 0 and st["failed"] == 0
     assert st["peak_bytes"] <= budget
-    assert_same(ref, got)
+    assert_same(ref * 3, got)
 
 
 def test_errors_are_per_request(systems):
