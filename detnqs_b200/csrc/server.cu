@@ -653,6 +653,7 @@ int dnq_server_set_budget(dnq_server_t S, int64_t budget_bytes) {
     {
         std::lock_guard<std::mutex> lk(S->mu);
         S->budget = budget_bytes;
+        make_room(S, 0, nullptr);   // idle blocks above the new budget go now
         S->peak = 0;   // the peak is tracked against the budget now in force
     }
     S->cv_sched.notify_one();

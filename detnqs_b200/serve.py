@@ -103,8 +103,8 @@ class Server:
         return t.result
 
     def set_budget(self, budget_bytes: float):
-        """New admission budget (idle blocks above it are evicted as builds
-        need room)."""
+        """New admission budget; idle blocks above it are evicted at once,
+        least recently used first."""
         N.check(N.lib.dnq_server_set_budget(self._h, int(budget_bytes)))
 
     def pause(self, paused: bool = True):

@@ -315,8 +315,9 @@ int dnq_server_submit(dnq_server_t s, int kind, int sys_id, const double* psi,
  * if none); the request's own status is returned and it is released. */
 int dnq_server_wait(dnq_server_t s, int64_t req_id, double timeout_s, double* out4,
                     int64_t* nnz);
-/* New admission budget; resident blocks above it are evicted (least recently
- * used, idle ones) as later builds need room.  Resets the peak statistic. */
+/* New admission budget: idle resident blocks above it are evicted at once
+ * (least recently used first), blocks in use as soon as later builds need
+ * room.  Resets the peak statistic. */
 int dnq_server_set_budget(dnq_server_t s, int64_t budget_bytes);
 /* paused != 0 holds grouped local-energy launches (requests are still
  * admitted and builds still run); 0 releases them. */
