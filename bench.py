@@ -767,7 +767,8 @@ def run_serving(args, rank: int, world: int):
     clk = ClockSampler(local)
     clk.start()
     l0 = native.lib.dnq_launch_count()
-    srv = V.Server(device=local, budget_bytes=SERVE_BUDGET, build_slots=4, max_group=64)
+    srv = V.Server(device=local, budget_bytes=SERVE_BUDGET, build_slots=args.serve_slots,
+                   max_group=64)
     ids = [srv.add_system(c, d, s.n_orb, eps1=1e-7) for (s, d), c in zip(systems, ctxs)]
     tickets = [None] * len(reqs)
     t0 = time.perf_counter() + 0.05
@@ -794,6 +795,7 @@ def run_serving(args, rank: int, world: int):
     # ---- plain: one request at a time, FP64, blocks kept resident
     resident = {}
     plain_lat, plain_e = [], []
+    plain_build_s = 0.0
     t0p = time.perf_counter() + 0.05
     for ta, kind, k, j in reqs:
         dt = t0p + ta - time.perf_counter()
@@ -803,9 +805,11 @@ def run_serving(args, rank: int, world: int):
         if kind == V.BUILD or k not in resident:
             if k in resident:
                 resident[k].close()
+            tb = time.perf_counter()
             resident[k] = device.build(ctxs[k], dets, n_orb=sysm.n_orb,
                                        policy=native.POLICY_STATIC, use_heatbath=True,
                                        eps1=1e-7, want_vp=False)
+            plain_build_s += time.perf_counter() - tb
         num = den = None
         if kind == V.ELOC:
             el = np.empty(len(dets))
@@ -839,7 +843,8 @@ def run_serving(args, rank: int, world: int):
         "dtype": "f64 build; f32-compensated H.psi (f64 diagonal and energies)",
         "data": "synthetic (seeded integrals, heat-bath sampled determinants, Poisson arrivals)",
         "config": {"workload": SERVE_WORKLOAD, "systems": len(systems), "requests": n,
-                   "rate_per_s": SERVE_RATE, "budget_bytes": SERVE_BUDGET, "build_slots": 4,
+                   "rate_per_s": SERVE_RATE, "budget_bytes": SERVE_BUDGET,
+                   "build_slots": args.serve_slots,
                    "max_group": 64, "parallelism": f"replicas x{world}",
                    "l2": "requests arrive in real time; inputs (1e3..2e5-row blocks) larger "
                          "than L2 in aggregate"},
@@ -850,7 +855,7 @@ def run_serving(args, rank: int, world: int):
                        "built_elements_per_s": built / span_served},
         "plain_fp64": {"latency_ms": {"p50": _pct(plain_lat, 50) * 1e3,
                                       "p99": _pct(plain_lat, 99) * 1e3},
-                       "requests_per_s": n / span_plain,
+                       "requests_per_s": n / span_plain, "build_seconds": plain_build_s,
                        "what": "same stream, one request at a time: dnq_build + FP64 local "
                                "energy, blocks kept resident, no overlap or grouping"},
         "speedup_vs_plain_fp64": {"p50": _pct(plain_lat, 50) * 1e3 / p50,
@@ -944,6 +949,8 @@ def main():
     ap.add_argument("--n-dets", type=int, default=N_DETS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-slots", type=int, default=2,
+                    help="build worker streams of the served path")
     ap.add_argument("--workload", choices=["single", "batched", "serving"], default="single",
                     help="single: one 30-orbital system, 1e6 dets (default); batched: 64 "
                          "systems of uneven size per step; serving: Poisson request stream")

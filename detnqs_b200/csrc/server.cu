@@ -45,9 +45,8 @@
 #include "ham.cuh"
 
 namespace dnq {
-namespace {
-
 using Clock = std::chrono::steady_clock;
+namespace {
 
 __device__ __forceinline__ void two_sum_d(double a, double b, double& s, double& e) {
     s = __dadd_rn(a, b);
@@ -206,6 +205,8 @@ struct dnq_server_s {
     dnq::Pinned<unsigned char> pin_desc;
     // statistics
     long long n_done = 0, n_failed = 0, n_evict = 0, n_groups = 0, n_grouped = 0, n_builds = 0;
+    double build_s = 0.0, group_s = 0.0;   // worker time in builds; launch -> done of groups
+    dnq::Clock::time_point g_t0;
     int max_seen_group = 0;
 };
 
@@ -394,12 +395,14 @@ void launch_group(dnq_server_s* S) {
     DNQ_CUDA(cudaMemcpyAsync(S->pin_e2.p, S->ge2.p, 2 * take * 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaEventRecord(S->gev, s));
     S->g_busy = true;
+    S->g_t0 = Clock::now();
     ++S->n_groups;
     S->n_grouped += take;
     S->max_seen_group = std::max(S->max_seen_group, take);
 }
 
 void finish_group(dnq_server_s* S) {
+    S->group_s += secs(S->g_t0, Clock::now());
     for (size_t k = 0; k < S->g_ids.size(); ++k) {
         SrvReq* r = S->reqs[S->g_ids[k]].get();
         SrvSystem& y = *S->sys[r->sys];
@@ -460,6 +463,7 @@ void worker(dnq_server_s* S, int slot) {
         SrvReq* r = S->reqs[id].get();
         SrvSystem& y = *S->sys[r->sys];
         lk.unlock();
+        const auto tb = Clock::now();
         dnq_ham_t H = nullptr;
         int rc = dnq_build(y.ctx, y.dets.data(), y.n, nullptr, 0, nullptr, y.n_orb, y.policy,
                            y.use_hb, y.eps1, 0, s, &H);
@@ -478,6 +482,7 @@ void worker(dnq_server_s* S, int slot) {
             }
         }
         lk.lock();
+        S->build_s += secs(tb, Clock::now());
         S->reserved -= r->reserve;
         r->reserve = 0;
         ++S->free_slots;
@@ -533,7 +538,11 @@ int dnq_server_create(int device, int64_t budget_bytes, int build_slots, int max
     S->slots = build_slots;
     S->free_slots = build_slots;
     S->max_group = max_group;
-    DNQ_CUDA(cudaStreamCreateWithFlags(&S->es, cudaStreamNonBlocking));
+    // local-energy groups are short: give their blocks priority over the
+    // long build kernels so they do not wait behind them
+    int lo = 0, hi = 0;
+    DNQ_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    DNQ_CUDA(cudaStreamCreateWithPriority(&S->es, cudaStreamNonBlocking, hi));
     DNQ_CUDA(cudaEventCreateWithFlags(&S->gev, cudaEventDisableTiming));
     S->wstreams.resize(build_slots);
     for (auto& w : S->wstreams) DNQ_CUDA(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
@@ -671,24 +680,26 @@ int dnq_server_pause(dnq_server_t S, int paused) {
     DNQ_API_END
 }
 
-int dnq_server_stats(dnq_server_t S, double* st12) {
+int dnq_server_stats(dnq_server_t S, double* st14) {
     DNQ_API_BEGIN
-    require(S && st12, DNQ_ERR_INVALID, "null argument");
+    require(S && st14, DNQ_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(S->mu);
     int resident = 0;
     for (auto& p : S->sys) resident += p->H != nullptr;
-    st12[0] = (double)S->n_done;
-    st12[1] = (double)S->n_failed;
-    st12[2] = (double)S->n_builds;
-    st12[3] = (double)S->n_groups;
-    st12[4] = S->n_groups ? (double)S->n_grouped / (double)S->n_groups : 0.0;
-    st12[5] = (double)S->max_seen_group;
-    st12[6] = (double)S->n_evict;
-    st12[7] = (double)S->used;
-    st12[8] = (double)S->peak;
-    st12[9] = (double)resident;
-    st12[10] = (double)S->pending.size();
-    st12[11] = (double)S->eloc_q.size();
+    st14[0] = (double)S->n_done;
+    st14[1] = (double)S->n_failed;
+    st14[2] = (double)S->n_builds;
+    st14[3] = (double)S->n_groups;
+    st14[4] = S->n_groups ? (double)S->n_grouped / (double)S->n_groups : 0.0;
+    st14[5] = (double)S->max_seen_group;
+    st14[6] = (double)S->n_evict;
+    st14[7] = (double)S->used;
+    st14[8] = (double)S->peak;
+    st14[9] = (double)resident;
+    st14[10] = (double)S->pending.size();
+    st14[11] = (double)S->eloc_q.size();
+    st14[12] = S->build_s;
+    st14[13] = S->group_s;
     DNQ_API_END
 }
 

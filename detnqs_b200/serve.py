@@ -113,11 +113,11 @@ class Server:
         N.check(N.lib.dnq_server_pause(self._h, int(bool(paused))))
 
     def stats(self) -> dict:
-        st = np.zeros(12)
+        st = np.zeros(14)
         N.check(N.lib.dnq_server_stats(self._h, st.ctypes.data))
         keys = ("completed", "failed", "builds", "groups", "mean_group", "max_group",
                 "evictions", "resident_bytes", "peak_bytes", "resident_blocks", "pending",
-                "ready")
+                "ready", "build_seconds", "group_seconds")
         return dict(zip(keys, (float(x) for x in st)))
 
 

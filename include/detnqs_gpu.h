@@ -322,11 +322,12 @@ int dnq_server_set_budget(dnq_server_t s, int64_t budget_bytes);
 /* paused != 0 holds grouped local-energy launches (requests are still
  * admitted and builds still run); 0 releases them. */
 int dnq_server_pause(dnq_server_t s, int paused);
-/* st12 = {completed, failed, builds, grouped launches, mean group size,
+/* st14 = {completed, failed, builds, grouped launches, mean group size,
  *         largest group, evictions, resident bytes, peak bytes (resident +
  *         reserved), resident blocks, requests waiting for admission,
- *         requests ready for the next grouped launch} */
-int dnq_server_stats(dnq_server_t s, double* st12);
+ *         requests ready for the next grouped launch, worker seconds spent
+ *         in builds, seconds from launch to completion of grouped launches} */
+int dnq_server_stats(dnq_server_t s, double* st14);
 
 #ifdef __cplusplus
 }
