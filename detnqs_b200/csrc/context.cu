@@ -231,6 +231,8 @@ void upload_tables(dnq_ctx_s* c) {
     DNQ_CUDA(cudaStreamSynchronize(s));
 }
 
+}  // namespace
+
 // Keep memory freed by cudaFreeAsync in the device's default pool instead
 // of returning it to the driver at every synchronisation: repeated builds
 // then reuse the same pages (process-local runtime setting).
@@ -240,6 +242,8 @@ void keep_pool(int device) {
     uint64_t thr = ~0ull;
     DNQ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
 }
+
+namespace {
 
 void init_ctx(dnq_ctx_s* c) {
     DeviceGuard g(c->device);

@@ -46,6 +46,7 @@
 
 namespace dnq {
 using Clock = std::chrono::steady_clock;
+void keep_pool(int device);
 namespace {
 
 __device__ __forceinline__ void two_sum_d(double a, double b, double& s, double& e) {
@@ -546,6 +547,23 @@ int dnq_server_create(int device, int64_t budget_bytes, int build_slots, int max
     DNQ_CUDA(cudaEventCreateWithFlags(&S->gev, cudaEventDisableTiming));
     S->wstreams.resize(build_slots);
     for (auto& w : S->wstreams) DNQ_CUDA(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
+    {   // own the budget up front: map it into the stream-ordered pool (kept
+        // after the free) so builds never wait for the pool to grow
+        keep_pool(device);
+        size_t fr = 0, tot = 0;
+        DNQ_CUDA(cudaMemGetInfo(&fr, &tot));
+        const size_t margin = (size_t)4 << 30;
+        const size_t want = std::min<size_t>((size_t)budget_bytes, fr > margin ? fr - margin : 0);
+        if (want >= ((size_t)1 << 20)) {
+            void* p = nullptr;
+            if (cudaMallocAsync(&p, want, S->es) == cudaSuccess) {
+                DNQ_CUDA(cudaFreeAsync(p, S->es));
+            } else {
+                (void)cudaGetLastError();
+            }
+            DNQ_CUDA(cudaStreamSynchronize(S->es));
+        }
+    }
     dnq_server_s* raw = S.get();
     for (int k = 0; k < build_slots; ++k) S->workers.emplace_back(worker, raw, k);
     S->sched = std::thread(scheduler, raw);

@@ -298,7 +298,9 @@ int dnq_batch_copy_coo(dnq_batch_t b, int sys, uint32_t* rows, uint32_t* cols,
  * budget_bytes, evicting least-recently-used idle blocks.  A request's result
  * does not depend on the other requests served with it.
  * psi (n doubles) and eloc (n doubles, may be NULL) are host memory the caller
- * keeps valid until dnq_server_wait returns for the request. */
+ * keeps valid until dnq_server_wait returns for the request.
+ * Creation maps min(budget, free memory - 4 GiB) into the device's
+ * stream-ordered pool, so builds do not wait for the pool to grow. */
 enum { DNQ_REQ_BUILD = 0, DNQ_REQ_ELOC = 1 };
 int dnq_server_create(int device, int64_t budget_bytes, int build_slots, int max_group,
                       dnq_server_t* out);

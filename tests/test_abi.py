@@ -33,6 +33,14 @@ def test_library_exports_every_declared_symbol():
     assert set(native.EXPORTS) <= set(_declared())
 
 
+def test_library_resolves_every_symbol_at_load():
+    """Immediate binding: an internal function referenced across files but
+    never defined (e.g. left in an unnamed namespace) fails here, on CPU."""
+    import os
+    from detnqs_b200 import native
+    ctypes.CDLL(native.LIB_PATH, mode=os.RTLD_NOW)
+
+
 def test_version_and_error_string_without_gpu():
     from detnqs_b200 import native
     assert native.lib.dnq_version() >= 100
