@@ -949,7 +949,7 @@ def main():
     ap.add_argument("--n-dets", type=int, default=N_DETS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-slots", type=int, default=2,
+    ap.add_argument("--serve-slots", type=int, default=4,
                     help="build worker streams of the served path")
     ap.add_argument("--workload", choices=["single", "batched", "serving"], default="single",
                     help="single: one 30-orbital system, 1e6 dets (default); batched: 64 "
