@@ -193,6 +193,7 @@ struct Arena {
     double* aval;
     i64 cap;                          // arena capacity (entries)
     i64 chunk;                        // entries per warp chunk
+    i64 restart;                      // longest row restarted in a fresh chunk
     unsigned long long* cursor;       // next free arena entry
     int* overflow;                    // set when the arena is too small
     i64* row_pos;
@@ -557,11 +558,13 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
                 cpos = out.w;
                 break;
             }
-            // Only rows of at most chunk/4 entries restart in a fresh chunk,
-            // so every retired chunk is at least 3/4 full and the arena
-            // never needs more than 4/3 nnz + (warps + 1) chunks; longer
-            // rows take the exact second pass.
-            if (4 * (i64)out.c > A.chunk || attempt == 1) {
+            // Only rows of at most `restart` entries restart in a fresh
+            // chunk; longer rows take the exact second pass.  With restart =
+            // chunk/4 every retired chunk is at least 3/4 full and the arena
+            // never needs more than 4/3 nnz + (warps + 1) chunks (planned
+            // batches); single builds restart rows up to a whole chunk and
+            // fall back to the exact two-pass build if the arena runs out.
+            if ((i64)out.c > A.restart || attempt == 1) {
                 if (lane == 0) {
                     A.row_len[g] = out.c;
                     A.big[atomicAdd(A.n_big, 1)] = (u32)g;
@@ -732,6 +735,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.aval = aval.p;
     A.cap = cap;
     A.chunk = chunk;
+    A.restart = chunk;
     A.cursor = cursor.p;
     A.overflow = ovf.p;
     A.row_pos = rpos.p;
@@ -1112,6 +1116,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     A.aval = b->aval.p;
     A.cap = b->cap;
     A.chunk = b->chunk;
+    A.restart = b->chunk / 4;
     A.cursor = b->cursor.p;
     A.overflow = b->ovf.p;
     A.row_pos = b->rpos.p;
