@@ -367,6 +367,147 @@ def heat_bath_sample(sysm: SyntheticSystem, n_dets: int, seed: int,
     return np.ascontiguousarray(out[:count])
 
 
+def hf_determinant_wide(n_alpha: int, n_beta: int) -> np.ndarray:
+    """HF determinant as uint64[1, 4] = (alpha lo, alpha hi, beta lo, beta hi)."""
+    return pack_wide(np.arange(n_alpha)[None, :], np.arange(n_beta)[None, :])
+
+
+def pack_wide(occ_a: np.ndarray, occ_b: np.ndarray) -> np.ndarray:
+    """uint64[N, 4] two-word masks (bit i of a spin = orbital i; word 0 holds
+    orbitals 0..63, word 1 orbitals 64..127) from occupied-index tables."""
+    out = np.zeros((occ_a.shape[0], 4), dtype=np.uint64)
+    for col, occ in ((0, occ_a), (2, occ_b)):
+        occ = np.asarray(occ, dtype=np.int64)
+        for w in (0, 1):
+            sel = (occ >> 6) == w
+            bits = np.where(sel, np.uint64(1) << (occ & 63).astype(np.uint64), np.uint64(0))
+            out[:, col + w] = np.bitwise_or.reduce(bits, axis=1) if occ.shape[1] else 0
+    return out
+
+
+def unpack_wide(dets: np.ndarray, n_orb: int) -> tuple[np.ndarray, np.ndarray]:
+    """Boolean occupations (N, n_orb) of the alpha and beta strings of
+    uint64[N, 4] determinants."""
+    d = np.ascontiguousarray(dets, dtype=np.uint64)
+    bits = np.unpackbits(d.view(np.uint8).reshape(-1, 4, 8), axis=2, bitorder="little")
+    a = bits[:, 0:2].reshape(-1, 128)[:, :n_orb].astype(bool)
+    b = bits[:, 2:4].reshape(-1, 128)[:, :n_orb].astype(bool)
+    return a, b
+
+
+def heat_bath_sample_wide(sysm: SyntheticSystem, n_dets: int, seed: int,
+                          max_level: int = 4, batch: int = 1 << 17) -> np.ndarray:
+    """Iterated heat-bath sampling for up to 128 orbitals, two words per
+    spin (uint64[N, 4] = alpha lo, alpha hi, beta lo, beta hi).
+
+    The proposals are those of :func:`heat_bath_sample` (1 in 16 a uniform
+    single; otherwise a double with a uniform occupied pair, same-spin with
+    probability 5/15, and the virtual pair drawn with probability
+    proportional to its heat-bath weight), kept when new and at most
+    ``max_level`` excitations from HF.  Occupations are held as index
+    tables, so any orbital count up to 128 works.  Deterministic for a
+    given ``seed``."""
+    n = sysm.n_orb
+    if n > 128:
+        raise ValueError("two-word determinants hold at most 128 orbitals")
+    na, nb = sysm.n_alpha, sysm.n_beta
+    rng = np.random.default_rng(seed)
+    eri4 = unpack_eri(sysm.eri, n)
+    w_os = np.abs(eri4.transpose(0, 2, 1, 3)).reshape(n * n, n * n)
+    anti = eri4.transpose(0, 2, 1, 3) - eri4.transpose(0, 2, 3, 1)
+    del eri4
+    w_ss = (np.abs(anti) * np.triu(np.ones((n, n)), 1)[None, None]).reshape(n * n, n * n)
+    del anti
+
+    def sampler(w):
+        cs = np.cumsum(w, axis=1)
+        tot = cs[:, -1].copy()
+        base = np.concatenate([[0.0], np.cumsum(tot)[:-1]])
+        cs += base[:, None]
+        return cs.ravel(), base, tot
+
+    os_flat, os_base, os_tot = sampler(w_os)
+    del w_os
+    ss_flat, ss_base, ss_tot = sampler(w_ss)
+    del w_ss
+    nn = n * n
+    A = np.zeros((n_dets, na), dtype=np.int16)
+    B = np.zeros((n_dets, nb), dtype=np.int16)
+    A[0] = np.arange(na)
+    B[0] = np.arange(nb)
+    out = np.zeros((n_dets, 4), dtype=np.uint64)
+    out[0] = hf_determinant_wide(na, nb)[0]
+    seen = {tuple(int(x) for x in out[0])}
+    count, stalled = 1, 0
+    while count < n_dets and stalled < 8:
+        before = count
+        m = batch
+        par = rng.integers(0, count, size=m)
+        pa, pb = A[par].astype(np.int64), B[par].astype(np.int64)
+        r = np.arange(m)
+        oa = np.zeros((m, n), dtype=bool)
+        ob = np.zeros((m, n), dtype=bool)
+        oa[r[:, None], pa] = True
+        ob[r[:, None], pb] = True
+        kind = rng.integers(0, 16, size=m)
+        spin = rng.integers(0, 2, size=m)
+        # opposite-spin double
+        i = pa[r, rng.integers(0, na, size=m)]
+        j = pb[r, rng.integers(0, nb, size=m)]
+        row = i * n + j
+        t = os_base[row] + rng.random(m) * os_tot[row]
+        k = np.minimum(np.searchsorted(os_flat, t, side="right") - row * nn, nn - 1)
+        a, b = k // n, k % n
+        ok_os = ~oa[r, a] & ~ob[r, b] & (os_tot[row] > 0)
+        # same-spin double
+        ns = min(na, nb)
+        ps = np.where(spin[:, None] == 0, pa[:, :ns], pb[:, :ns])
+        p1 = rng.integers(0, max(ns, 1), size=m)
+        p2 = (p1 + rng.integers(1, max(ns, 2), size=m)) % max(ns, 1)
+        si, sj = ps[r, p1], ps[r, p2]
+        srow = np.minimum(si, sj) * n + np.maximum(si, sj)
+        t = ss_base[srow] + rng.random(m) * ss_tot[srow]
+        k = np.minimum(np.searchsorted(ss_flat, t, side="right") - srow * nn, nn - 1)
+        sa, sb = k // n, k % n
+        os_ = np.where(spin[:, None] == 0, oa, ob)
+        ok_ss = ~os_[r, sa] & ~os_[r, sb] & (ss_tot[srow] > 0) & (si != sj) & (sa != sb) & \
+            (ns >= 2)
+        # single
+        hsel = np.where(spin == 0, pa[r, rng.integers(0, na, size=m)],
+                        pb[r, rng.integers(0, nb, size=m)])
+        pv = rng.integers(0, n, size=m)
+        ok_s = ~os_[r, pv]
+        good = np.where(kind == 0, ok_s, np.where(kind <= 5, ok_ss, ok_os))
+        ca, cb = oa.copy(), ob.copy()
+        # apply each kind on its rows
+        sel = good & (kind >= 6)
+        ca[r[sel], i[sel]] = False; ca[r[sel], a[sel]] = True
+        cb[r[sel], j[sel]] = False; cb[r[sel], b[sel]] = True
+        for sp, C in ((0, ca), (1, cb)):
+            sel = good & (kind >= 1) & (kind <= 5) & (spin == sp)
+            C[r[sel], si[sel]] = False; C[r[sel], sj[sel]] = False
+            C[r[sel], sa[sel]] = True; C[r[sel], sb[sel]] = True
+            sel = good & (kind == 0) & (spin == sp)
+            C[r[sel], hsel[sel]] = False; C[r[sel], pv[sel]] = True
+        lev = (~ca[:, :na]).sum(1) + (~cb[:, :nb]).sum(1)
+        keep = good & (lev <= max_level)
+        ca, cb = ca[keep], cb[keep]
+        occa = np.nonzero(ca)[1].reshape(-1, na)
+        occb = np.nonzero(cb)[1].reshape(-1, nb)
+        keys = pack_wide(occa, occb)
+        for q, kk in enumerate(map(tuple, keys.tolist())):
+            if kk not in seen:
+                seen.add(kk)
+                out[count] = keys[q]
+                A[count] = occa[q]
+                B[count] = occb[q]
+                count += 1
+                if count >= n_dets:
+                    break
+        stalled = stalled + 1 if count == before else 0
+    return np.ascontiguousarray(out[:count])
+
+
 def unpack_eri(eri: np.ndarray, n: int) -> np.ndarray:
     """Dense (pq|rs) tensor from the packed 8-fold array."""
     key = pair_index(n)
@@ -391,5 +532,6 @@ __all__ = [
     "SyntheticSystem", "make_integrals", "make_system", "write_fcidump",
     "read_fcidump", "hf_determinant", "singles_doubles", "hf_sd_space",
     "heat_bath_sample", "unpack_eri", "unpack_h1e", "normalized_psi", "scan_family",
+    "heat_bath_sample_wide", "hf_determinant_wide", "pack_wide", "unpack_wide",
     "pair_index", "E_CORE",
 ]

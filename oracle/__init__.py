@@ -353,3 +353,89 @@ class CheckerCtx:
             return self.chk._dets_of(r)
         finally:
             self.lib.dq_res_free(r)
+
+
+# ---------------------------------------------------------------------------
+# Two-word determinants (up to 128 orbitals): oracle/wide.cpp
+# ---------------------------------------------------------------------------
+
+class WideChecker:
+    """The restatement for W-word spin strings (W = 1 or 2), in
+    ``oracle/liboracle.so``.  Determinants are uint64[N, 2W]: alpha words
+    (low word first), then beta words."""
+
+    def __init__(self, n_orb: int, h1e, eri, e_nuc: float):
+        if not os.path.exists(PORT_LIB):
+            raise OracleError(f"checker library not built: {PORT_LIB}")
+        lib = Checker(PORT_LIB).lib
+        if not getattr(lib, "_wide_bound", False):
+            def f(name, res, *args):
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = list(args)
+            f("dqw_ctx_from_arrays", _P, C.c_int, _f64p, _f64p, C.c_double)
+            f("dqw_ctx_free", None, _P)
+            f("dqw_hb_prepare", C.c_int, _P, C.c_double)
+            f("dqw_diag", C.c_int, _P, C.c_int, _u64p, C.c_int64, _f64p)
+            f("dqw_elem", C.c_double, _P, C.c_int, _u64p, _u64p)
+            f("dqw_build", _P, _P, C.c_int, _u64p, C.c_int64, _P, C.c_int, C.c_double,
+              C.c_int64, C.c_int64)
+            lib._wide_bound = True
+        self.lib = lib
+        self.chk = Checker(PORT_LIB)
+        self.n_orb = n_orb
+        self.ptr = lib.dqw_ctx_from_arrays(n_orb, np.ascontiguousarray(h1e, np.float64),
+                                           np.ascontiguousarray(eri, np.float64), e_nuc)
+        if not self.ptr:
+            raise OracleError(lib.dq_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.lib.dqw_ctx_free(self.ptr)
+            self.ptr = None
+
+    def hb_prepare(self, threshold: float = 1e-15):
+        if self.lib.dqw_hb_prepare(self.ptr, threshold):
+            raise OracleError(self.lib.dq_last_error().decode())
+
+    @staticmethod
+    def _words(d: np.ndarray) -> int:
+        if d.ndim != 2 or d.shape[1] not in (2, 4):
+            raise ValueError("determinants must be uint64[N, 2] or uint64[N, 4]")
+        return d.shape[1] // 2
+
+    def diag(self, dets) -> np.ndarray:
+        d = np.ascontiguousarray(dets, np.uint64)
+        out = np.empty(len(d))
+        self.lib.dqw_diag(self.ptr, self._words(d), d, len(d), out)
+        return out
+
+    def elem(self, bra, ket) -> float:
+        b = np.ascontiguousarray(bra, np.uint64).reshape(-1)
+        k = np.ascontiguousarray(ket, np.uint64).reshape(-1)
+        return self.lib.dqw_elem(self.ptr, len(b) // 2, b, k)
+
+    def build(self, dets, psi=None, *, eps1: float, rows=None) -> dict:
+        """Screened blocks of rows [r0, r1) of ``dets`` (all rows by
+        default): static heat-bath policy without ``psi``, the dynamic
+        amplitude policy with it.  Returns H_VV, H_VP (COO dicts), det_P
+        (uint64[N_P, 2W], sorted) and size_P."""
+        d = np.ascontiguousarray(dets, np.uint64)
+        W = self._words(d)
+        r0, r1 = (0, len(d)) if rows is None else rows
+        p = None if psi is None else np.ascontiguousarray(psi, np.float64)
+        r = self.lib.dqw_build(self.ptr, W, d, len(d), None if p is None else p.ctypes.data,
+                               self.n_orb, float(eps1), int(r0), int(r1))
+        if not r:
+            raise OracleError(self.lib.dq_last_error().decode())
+        try:
+            vv = self.chk._coo(r, 0)
+            vp = self.chk._coo(r, 1)
+            m = self.lib.dq_res_size(r, 2) * 2 // (2 * W)
+            P = np.empty((m, 2 * W), np.uint64)
+            if m:
+                self.lib.dq_res_dets(r, P)
+            return {"H_VV": vv, "H_VP": vp, "det_P": P, "size_P": m}
+        finally:
+            self.lib.dq_res_free(r)
+
