@@ -408,6 +408,8 @@ static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1
     return full_cutoff();
 }
 
+void launch_wide_diag(const dnq_ctx_s* ctx, const u64* d, i64 n, double* out, cudaStream_t s);
+
 void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                       double cut, const double* psi, const double* diag, cudaStream_t s,
                       dnq_ham_s* H, double* t_ms);
@@ -686,6 +688,7 @@ extern "C" {
 
 int dnq_ham_diag(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, double* out, void* stream) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx != nullptr && (n == 0 || (dets && out)), DNQ_ERR_INVALID, "null argument");
     require(n >= 0, DNQ_ERR_INVALID, "negative size");
     if (n == 0) return DNQ_OK;
@@ -709,6 +712,7 @@ int dnq_ham_diag(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, double* out, vo
 int dnq_ham_elems(dnq_ctx_t ctx, const uint64_t* bra, const uint64_t* ket, int64_t n,
                   double* out, void* stream) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx != nullptr && (n == 0 || (bra && ket && out)), DNQ_ERR_INVALID, "null argument");
     if (n == 0) return DNQ_OK;
     DeviceGuard g(ctx->device);
@@ -746,6 +750,7 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
               int64_t n_ext, const double* psi, int n_orb, int policy, int use_heatbath,
               double eps1, int want_vp, void* stream, dnq_ham_t* out) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx && out, DNQ_ERR_INVALID, "null argument");
     *out = nullptr;
     require(n_V >= 0 && n_ext >= 0, DNQ_ERR_INVALID, "negative size");
@@ -877,7 +882,7 @@ int dnq_ham_copy_dets_p(dnq_ham_t h, uint64_t* dets, void* stream) {
     require(h != nullptr, DNQ_ERR_INVALID, "null argument");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
-    copy_out(dets, (const uint64_t*)h->dets_p.p, 2 * h->n_p, s);
+    copy_out(dets, (const uint64_t*)h->dets_p.p, 2 * (i64)h->words * h->n_p, s);
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_API_END
 }
@@ -896,7 +901,8 @@ int dnq_ham_p_diag(dnq_ham_t h, dnq_ctx_t ctx, double* out, void* stream) {
         tmp.alloc(h->n_p, s);
         o = tmp.p;
     }
-    launch_diag(ctx, (const u64*)h->dets_p.p, h->n_p, o, s);
+    if (h->words == 2) launch_wide_diag(ctx, (const u64*)h->dets_p.p, h->n_p, o, s);
+    else launch_diag(ctx, (const u64*)h->dets_p.p, h->n_p, o, s);
     if (!dev_out) copy_out(out, o, h->n_p, s);
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_API_END

@@ -306,8 +306,10 @@ void load_fcidump(dnq_ctx_s* c, const char* path) {
     }
 }
 
-dnq_ctx_s* new_ctx(int n_orb, int device) {
-    require(n_orb >= 1 && n_orb <= 64, DNQ_ERR_INVALID, "Number of orbitals must be in [1, 64]");
+dnq_ctx_s* new_ctx(int n_orb, int device, int max_orb = 64) {
+    require(n_orb >= 1 && n_orb <= max_orb, DNQ_ERR_INVALID,
+            max_orb == 64 ? "Number of orbitals must be in [1, 64]"
+                          : "Number of orbitals must be in [1, 128]");
     int ndev = 0;
     DNQ_CUDA(cudaGetDeviceCount(&ndev));
     require(device >= 0 && device < ndev, DNQ_ERR_INVALID, "invalid device ordinal");
@@ -377,6 +379,20 @@ int dnq_ctx_device_bytes(dnq_ctx_t ctx, int64_t* out) {
     DNQ_API_BEGIN
     require(ctx && out, DNQ_ERR_INVALID, "null argument");
     *out = ctx->bytes();
+    DNQ_API_END
+}
+
+int dnq_ctx_create_wide(int n_orb, const double* h1e, const double* eri, double e_nuc,
+                        int device, dnq_ctx_t* out) {
+    DNQ_API_BEGIN
+    require(out && h1e && eri, DNQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<dnq_ctx_s> c(new_ctx(n_orb, device, 128));
+    std::memcpy(c->h1p.data(), h1e, c->h1p.size() * 8);
+    std::memcpy(c->erip.data(), eri, c->erip.size() * 8);
+    c->e_nuc = e_nuc;
+    init_ctx(c.get());
+    *out = c.release();
     DNQ_API_END
 }
 

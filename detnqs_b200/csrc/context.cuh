@@ -96,6 +96,12 @@ struct dnq_ctx_s {
 };
 
 namespace dnq {
+// One-word entry points need spin strings that fit one uint64.
+inline void require_narrow(const dnq_ctx_s* c) {
+    if (c && c->n > 64)
+        throw Error(DNQ_ERR_INVALID,
+                    "context has more than 64 orbitals: use the two-word entry points");
+}
 // Smallest double strictly above 1e-15: "w > 1e-15" == "w >= kFullCut".
 double full_cutoff();
 // Effective heat-bath cutoff of the reference query with_cutoff(eps) on a

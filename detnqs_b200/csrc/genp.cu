@@ -734,6 +734,7 @@ extern "C" {
 int dnq_gen_dets(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, int n_orb, const double* psi,
                  int mode, double eps1, int device, void* stream, dnq_ham_t* out) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(out != nullptr, DNQ_ERR_INVALID, "null argument");
     *out = nullptr;
     require(mode >= -1 && mode <= 2, DNQ_ERR_INVALID, "invalid screen mode");
@@ -760,6 +761,7 @@ int dnq_gen_dets(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, int n_orb, cons
 int dnq_local_connections(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, int n_orb,
                           int use_heatbath, double eps1, void* stream, dnq_ham_t* out) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx && out, DNQ_ERR_INVALID, "null argument");
     *out = nullptr;
     require(n >= 0 && (n == 0 || dets), DNQ_ERR_INVALID, "null determinant array");
@@ -802,6 +804,7 @@ int dnq_conn_copy(dnq_ham_t h, int32_t* offsets, uint64_t* dets, double* values,
 int dnq_pt2(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, const double* coeffs, int n_orb,
             double e_ref, int use_heatbath, double eps1, double* out3, void* stream) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx && out3, DNQ_ERR_INVALID, "null argument");
     out3[0] = out3[1] = out3[2] = 0.0;
     require(n >= 0, DNQ_ERR_INVALID, "negative size");

@@ -28,6 +28,7 @@ struct dnq_ham_s {
     int device = 0;
     cudaStream_t stream = nullptr;
     dnq::i64 n_v = 0, n_p = 0;
+    int words = 1;                    // uint64 words per spin string of V and P
     dnq::Csr vv, vp;
     dnq::Csr pv;                      // transpose of vp, built on first use
     bool pv_ready = false;

@@ -190,6 +190,7 @@ int dnq_variational_energy(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
                            const double* coeffs, int n_orb, int use_heatbath, double eps1,
                            double* out, void* stream) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(ctx && out, DNQ_ERR_INVALID, "null argument");
     require(n >= 0, DNQ_ERR_INVALID, "negative size");
     if (n == 0) { *out = 0.0; return DNQ_OK; }

@@ -600,6 +600,7 @@ int dnq_server_destroy(dnq_server_t S) {
 int dnq_server_add_system(dnq_server_t S, dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
                           int n_orb, int policy, int use_heatbath, double eps1, int* sys_id) {
     DNQ_API_BEGIN
+    require_narrow(ctx);
     require(S && ctx && dets && sys_id, DNQ_ERR_INVALID, "null argument");
     require(n >= 1, DNQ_ERR_INVALID, "a system needs determinants");
     require(ctx->device == S->device, DNQ_ERR_INVALID, "context lives on another device");

@@ -1247,6 +1247,7 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
     for (int k = 0; k < n_sys; ++k) {
         require(ctxs[k] && ctxs[k]->device == device, DNQ_ERR_INVALID,
                 "every context must live on the batch's device");
+        require_narrow(ctxs[k]);
         require(n_orb[k] >= 1 && n_orb[k] < 64 && n_orb[k] <= ctxs[k]->n, DNQ_ERR_INVALID,
                 "n_orb must be in [1, min(63, orbitals of the context)]");
         require(n_dets[k] >= 1 && dets[k], DNQ_ERR_INVALID, "every system needs determinants");

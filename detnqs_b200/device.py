@@ -98,8 +98,10 @@ class DeviceHamiltonian:
         shape = (self.n_v, self.n_v) if block == 0 else (self.n_v, self.n_p)
         return sp.csr_matrix((vals, cols.astype(np.int64), rp), shape=shape)
 
+    words = 1   # uint64 words per spin string (2 for handles of the wide build)
+
     def dets_p(self) -> np.ndarray:
-        out = np.empty((self.n_p, 2), np.uint64)
+        out = np.empty((self.n_p, 2 * self.words), np.uint64)
         N.check(N.lib.dnq_ham_copy_dets_p(self._h, out.ctypes.data, None))
         return out
 

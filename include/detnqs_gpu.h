@@ -331,6 +331,29 @@ int dnq_server_pause(dnq_server_t s, int paused);
  *         in builds, seconds from launch to completion of grouped launches} */
 int dnq_server_stats(dnq_server_t s, double* st14);
 
+/* ---- two-word determinants, up to 128 orbitals (no reference counterpart:
+ * the reference's Det holds one uint64 per spin, det.hpp:30-36, and its
+ * IntegralMO rejects n > 64, integral_mo.cpp:26-28) ---------------------------
+ * A determinant is 4 x uint64: alpha lo, alpha hi, beta lo, beta hi (bit i of
+ * a spin string = orbital i); P is sorted by alpha as a 128-bit integer, then
+ * beta.  Contexts with more than 64 orbitals are accepted only here; the
+ * one-word entry points reject them. */
+int dnq_ctx_create_wide(int n_orb, const double* h1e, const double* eri,
+                        double e_nuc, int device, dnq_ctx_t* out);
+/* Diagonal elements (ham_eval.cpp:53-86) of n two-word determinants. */
+int dnq_wide_diag(dnq_ctx_t ctx, const uint64_t* dets, int64_t n, double* out,
+                  void* stream);
+/* Screened V->{V,P} build of two-word determinants: get_ham_conn with the
+ * heat-bath table when psi == NULL (singles kept, doubles w >= eps1), else
+ * get_ham_conn_amp (singles |h psi_i| >= eps1, doubles w >= eps1 /
+ * max(|psi_i|, 1e-12)); build_ham.cpp:139-196, :256-312, :346-380.  The
+ * handle holds H_VV, H_VP and P (dnq_ham_copy_dets_p copies 4 words per
+ * determinant; dnq_ham_p_diag gives diag(H_PP)), so dnq_ham_spmv,
+ * dnq_ham_proxy_spmv and dnq_ham_eff_from apply to it unchanged. */
+int dnq_wide_build(dnq_ctx_t ctx, const uint64_t* dets, int64_t n,
+                   const double* psi, int n_orb, double eps1, void* stream,
+                   dnq_ham_t* out);
+
 #ifdef __cplusplus
 }
 #endif
