@@ -12,8 +12,11 @@
 //      bitmap of touched columns; the k loop is sequential so every output
 //      element is summed in the reference's order.  FP64 mode uses
 //      unfused multiply/add like the reference build; FP32 mode reads FP32
-//      H_VP values and keeps a TwoSum/TwoProduct-compensated FP32 pair per
-//      element.
+//      H_VP values and keeps a float-float accumulator per element: each
+//      product's rounding error (TwoProduct) and each sum's (TwoSum) go to
+//      the error word, which is renormalised against the sum after every
+//      add (FastTwoSum; Dekker 1971), so ~1e6 terms into one element stay
+//      accurate to a few FP32 ulps squared.
 //   4. The H_VV row is added, entries with |v| <= 1e-15 dropped
 //      (csr_add, ham_utils.cpp:330-442), and the row is compacted in column
 //      order from the bitmap.
@@ -187,8 +190,12 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                         float2 cur = acc2[j];
                         float s2, e;
                         f_two_sum(cur.x, p, s2, e);
-                        cur.x = s2;
-                        cur.y = __fadd_rn(cur.y, __fadd_rn(e, pe));
+                        const float c = __fadd_rn(cur.y, __fadd_rn(e, pe));
+                        // renormalise (FastTwoSum, |s2| >= |c|): the error word
+                        // stays below half an ulp of the sum, so its own
+                        // rounding does not pile up over ~1e6 terms
+                        cur.x = __fadd_rn(s2, c);
+                        cur.y = __fsub_rn(c, __fsub_rn(cur.x, s2));
                         acc2[j] = cur;
                     }
                 }
