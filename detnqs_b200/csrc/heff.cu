@@ -179,14 +179,18 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                     if (need) acc[j] = __dadd_rn(acc[j], __dmul_rn(as, P.pvval[q]));
                 }
             } else {
-                const float as = (float)__dmul_rn((double)P.vpval32[t], s);
+                // a * D^-1 in FP64, carried as a float pair hi + lo (the FP64
+                // shift keeps its precision; only the stored values are FP32)
+                const double asd = __dmul_rn((double)P.vpval32[t], s);
+                const float as = (float)asd;
+                const float as_lo = (float)(asd - (double)as);
                 for (i64 q = q0 + lane; q < q1; q += 32) {
                     const u32 j = P.pvcol[q];
                     atomicOr(&bits[j >> 5], 1u << (j & 31));
                     if (need) {
                         const float b = P.pvval32[q];
                         const float p = __fmul_rn(as, b);
-                        const float pe = fmaf(as, b, -p);
+                        const float pe = fmaf(as, b, -p) + __fmul_rn(as_lo, b);
                         float2 cur = acc2[j];
                         float s2, e;
                         f_two_sum(cur.x, p, s2, e);
