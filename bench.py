@@ -30,6 +30,11 @@ bond-scan families) served by the device-resident loop with continuous
 batching, beside the same stream served one request at a time in FP64;
 p50/p99 latency.
 
+`--workload downfold`: 100 orbitals (two-word determinants), S = 1e5,
+dynamic amplitude screening at eps1 = 1e-5 into C ~ 1e7 external
+determinants, and the downfolded H_eff in FP64 and FP32 values; |dE| of the
+lowest eigenvalue (device Lanczos) between the two.
+
 `--impl reference` times the reference DetNQS C++ core (compiled from its
 sources into oracle/_ref) on a bounded sample of rows of the same workload.
 """
@@ -874,6 +879,225 @@ def run_serving(args, rank: int, world: int):
     return result
 
 
+# ---------------------------------------------------------------------------
+# Downfolding workload: 100 orbitals, two-word determinants
+# ---------------------------------------------------------------------------
+
+DF_N, DF_NE, DF_K, DF_S = 100, 20, 200, 100_000
+DF_EPS, DF_TAIL, DF_SIGMA = 1e-5, 2e-6, 0.1
+DF_WORKLOAD = ("100 orbitals, 20a/20b, K=200, two-word determinants; S = 1e5 heat-bath-sampled "
+               "dets (<= 4 excitations); psi_S: HF amplitude 1 and a N(0,1) tail of scale 2e-6 "
+               "(normalised); C = screened singles/doubles of S with dynamic amplitude "
+               "screening eps1 = 1e-5; H_eff = H_SS + H_SC (e_ref - D_CC)^-1 H_CS with "
+               "e_ref = <psi|H_SS|psi>, sigma regularisation 0.1 Ha, FP64 and FP32 values")
+
+
+def downfold_workload(rank: int):
+    from detnqs_b200 import synthetic as S
+    seed = 4004 + 10 * rank
+    sysm = S.make_system(DF_N, DF_NE, DF_NE, DF_K, seed)
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"df_{DF_N}_{DF_S}_{seed}.npy")
+    if os.path.exists(path):
+        V = np.load(path)
+    else:
+        V = S.heat_bath_sample_wide(sysm, DF_S, seed + 1, max_level=4)
+        np.save(path, V)
+    rng = np.random.default_rng(seed + 2)
+    psi = DF_TAIL * rng.normal(size=len(V))
+    psi[0] = 1.0
+    psi /= np.linalg.norm(psi)
+    return sysm, V, psi
+
+
+def cpu_wide_rows(sysm, V, psi, target_s: float = 15.0, seed: int = 5):
+    """Two-word restatement (oracle/wide.cpp, the only CPU form: the
+    reference stops at 64 orbitals) on a sample of rows.  Returns
+    (elements/s, rows, elements, seconds, threads)."""
+    from oracle import WideChecker
+    chk = WideChecker(DF_N, sysm.h1e, sysm.eri, sysm.e_core)
+    chk.hb_prepare(1e-15)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(np.arange(1, len(V)))
+    nnz = 0
+    t_all = 0.0
+    rows = 0
+    for r in order:
+        t0 = time.perf_counter()
+        o = chk.build(V, psi, eps1=DF_EPS, rows=(int(r), int(r) + 1))
+        t_all += time.perf_counter() - t0
+        nnz += len(o["H_VV"]["val"]) + len(o["H_VP"]["val"])
+        rows += 1
+        if t_all >= target_s:
+            break
+    return nnz / t_all, rows, nnz, t_all, os.cpu_count() or 1
+
+
+def run_downfold(args, rank: int, world: int):
+    sysm, V, psi = downfold_workload(rank)
+    import torch
+    from detnqs_b200 import eigen as E
+    from detnqs_b200 import native
+    from detnqs_b200 import wide as Wd
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    ctx = Wd.IntCtxWide.from_arrays(DF_N, sysm.h1e, sysm.eri, sysm.e_core, device=local)
+    ctx.hb_prepare(1e-15)
+    ctx_s = time.perf_counter() - t0
+    Vd = torch.from_numpy(V.view(np.int64)).to(dev)
+    pd = torch.from_numpy(psi).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def step():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        ev[0].record()
+        H = Wd.build_wide(ctx, Vd, pd, n_orb=DF_N, eps1=DF_EPS)
+        ev[1].record()
+        hpp = torch.empty(H.n_p, dtype=torch.float64, device=dev)
+        Wd.p_diag(H, ctx, hpp)
+        num, den = H.local_energy(pd)
+        e_ref = num / den
+        ev[2].record()
+        E64 = Wd.ham_eff_wide(H, hpp, e_ref, epsilon=DF_SIGMA, precision=native.F64)
+        ev[3].record()
+        E32 = Wd.ham_eff_wide(H, hpp, e_ref, epsilon=DF_SIGMA, precision=native.F32)
+        ev[4].record()
+        ev[5].record()
+        return H, hpp, e_ref, E64, E32, ev
+
+    for _ in range(args.warmup):
+        H, hpp, e_ref, E64, E32, _ = step()
+        for h in (H, E64, E32):
+            h.close()
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = native.lib.dnq_launch_count()
+    t_step, t_build, t_diag, t_h64, t_h32 = [], [], [], [], []
+    for k in range(args.steps):
+        flush.zero_()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        H, hpp, e_ref, E64, E32, ev = step()
+        b.record()
+        torch.cuda.synchronize()
+        t_step.append(a.elapsed_time(b))
+        t_build.append(ev[0].elapsed_time(ev[1]))
+        t_diag.append(ev[1].elapsed_time(ev[2]))
+        t_h64.append(ev[2].elapsed_time(ev[3]))
+        t_h32.append(ev[3].elapsed_time(ev[4]))
+        if k < args.steps - 1:
+            for h in (H, E64, E32):
+                h.close()
+    clocks = clk.stop()
+    launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
+    ms_step = max_over_ranks(float(np.mean(t_step)), world, dev)
+    n_s, nnz_ss, n_c, nnz_sc = H.n_v, H.nnz_vv, H.n_p, H.nnz_vp
+    # SpGEMM work: sum over C columns of (entries in the column)^2
+    _, ccols, _ = H.to_csr_arrays(1)
+    m_k = np.bincount(ccols.astype(np.int64), minlength=n_c)
+    work = int((m_k.astype(np.int64) ** 2).sum())
+    nnz_eff = E32.nnz_vv
+
+    # lowest eigenvalue of the symmetric part of each H_eff (device Lanczos)
+    te = time.perf_counter()
+    S64, S32 = E.symmetric_part(E64), E.symmetric_part(E32)
+    lam64, it64 = E.lowest_eigenvalue(S64, device=local)
+    lam32, it32 = E.lowest_eigenvalue(S32, device=local)
+    eig_s = time.perf_counter() - te
+    for h in (S64, S32):
+        h.close()
+
+    # end to end through the public API: host determinants and psi in,
+    # host diag(H_CC) and the FP32 H_eff (CSR) out
+    pin_V = torch.from_numpy(V.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    pin_p = torch.from_numpy(psi).pin_memory().numpy()
+    e2e = []
+    d2h = 0
+    for _ in range(max(1, args.steps)):
+        flush.zero_()
+        barrier()
+        a = time.perf_counter()
+        He = Wd.build_wide(ctx, pin_V, pin_p, n_orb=DF_N, eps1=DF_EPS)
+        hp = Wd.p_diag(He, ctx)
+        nu, de = He.local_energy(pin_p)
+        Ee = Wd.ham_eff_wide(He, hp, nu / de, epsilon=DF_SIGMA, precision=native.F32)
+        rp, cc, vv = Ee.to_csr_arrays(0)
+        e2e.append((time.perf_counter() - a) * 1e3)
+        d2h = hp.nbytes + rp.nbytes + cc.nbytes + vv.nbytes + 16
+        for h in (He, Ee):
+            h.close()
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), world, dev)
+
+    peak, peak_kind = measured_peaks()
+    build_ms, h32_ms = float(np.mean(t_build)), float(np.mean(t_h32))
+    alg_build = n_s * 32 + (n_s + 1) * 16 + (nnz_ss + nnz_sc) * 12 + nnz_sc * 32
+    alg_spgemm = nnz_sc * (4 + 4) * 2 + n_c * 8 + nnz_eff * (4 + 8) + n_s * 8
+    result = {
+        "metric": "screened H elements/s (H_SS + H_SC nnz per second of the downfolding step: "
+                  "build, diag(H_CC), FP64 and FP32 H_eff)",
+        "value": world * (nnz_ss + nnz_sc) / (ms_step * 1e-3),
+        "unit": "elements/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 build; H_eff in f64 and in f32 values with float-float accumulation",
+        "data": "synthetic (seeded integrals, heat-bath sampled two-word determinants)",
+        "config": {"workload": DF_WORKLOAD, "n_orb": DF_N, "S": n_s, "C": n_c,
+                   "nnz_H_SS": nnz_ss, "nnz_H_SC": nnz_sc, "nnz_H_eff": nnz_eff,
+                   "spgemm_multiply_adds": work, "e_ref": e_ref, "context_s": ctx_s,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps"},
+        "phase_ms": {"build": build_ms, "diag_cc_and_e_ref": float(np.mean(t_diag)),
+                     "h_eff_f64": float(np.mean(t_h64)), "h_eff_f32": h32_ms},
+        "lowest_eigenvalue": {"f64": lam64, "f32": lam32, "lanczos_steps": [it64, it32],
+                              "seconds": eig_s,
+                              "of": "0.5 (H_eff + H_eff^T), device Lanczos in FP64"},
+        "dE_fp32_vs_fp64_Ha": abs(lam32 - lam64),
+        "spgemm_multiply_adds_per_s": work / (h32_ms * 1e-3),
+        "roofline": {"bound": "hbm", "kernel": "k_wide_build (count + fill)",
+                     "achieved": alg_build / (build_ms * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg_build / (build_ms * 1e-3) / 1e9 / peak,
+                     "traffic": ncu_traffic("k_wide_build"), "peak_kind": peak_kind,
+                     "note": "generation is integer/L2-latency bound; bytes are dets read, "
+                             "CSR and C keys written"},
+        "roofline_spgemm": {"bound": "hbm", "kernel": "k_heff<F32> (FP32 H_eff)",
+                            "achieved": alg_spgemm / (h32_ms * 1e-3) / 1e9, "peak": peak,
+                            "unit": "GB/s",
+                            "frac": alg_spgemm / (h32_ms * 1e-3) / 1e9 / peak,
+                            "traffic": ncu_traffic("k_heff_f32"), "peak_kind": peak_kind},
+        "e2e": {"value": world * (nnz_ss + nnz_sc) / (e2e_ms * 1e-3), "unit": "elements/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": n_s * 40 + n_c * 8,
+                "d2h_bytes_per_step": int(d2h),
+                "note": "FP32 H_eff only; host dets/psi in, diag(H_CC) and H_eff CSR out"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, rows, cnnz, t, threads = cpu_wide_rows(sysm, V, psi, args.cpu_seconds)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "elements/s", "cores": threads, "kind": "port",
+            "sample": f"{rows} random non-HF rows of S (two-word restatement; the reference "
+                      f"cannot represent 100 orbitals), {cnnz} elements in {t:.1f} s"}
+    for h in (H, E64, E32):
+        h.close()
+    return result
+
+
 def run_reference(args, rank: int, world: int):
     """Reference CPU implementation on the same workload (rank 0 only)."""
     if rank != 0:
@@ -951,7 +1175,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-slots", type=int, default=4,
                     help="build worker streams of the served path")
-    ap.add_argument("--workload", choices=["single", "batched", "serving"], default="single",
+    ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold"],
+                    default="single",
                     help="single: one 30-orbital system, 1e6 dets (default); batched: 64 "
                          "systems of uneven size per step; serving: Poisson request stream")
     args = ap.parse_args()
@@ -967,7 +1192,8 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    run = {"single": run_ours, "batched": run_batched, "serving": run_serving}[args.workload]
+    run = {"single": run_ours, "batched": run_batched, "serving": run_serving,
+           "downfold": run_downfold}[args.workload]
     res = run(args, rank, world)
     if world > 1:
         import torch

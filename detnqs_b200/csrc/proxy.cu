@@ -4,6 +4,8 @@
 // H_PV is the transpose of H_VP, built once per handle on first use.
 #include <cub/cub.cuh>
 
+#include <memory>
+
 #include "ham.cuh"
 
 namespace dnq {
@@ -91,6 +93,73 @@ void transpose_csr(const Csr& a, Csr& t, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
 }
 
+namespace {
+// 0.5 (A + A^T) of a square block with column-sorted rows: one thread merges
+// row r of A with row r of A^T (both sorted); absent entries count as 0.
+template <bool FILL>
+__global__ void k_sym_merge(const i64* arp, const u32* acol, const double* aval, const i64* trp,
+                            const u32* tcol, const double* tval, i64 n, u32* cnt,
+                            const i64* off, u32* ocol, double* oval) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < n;
+         r += (i64)gridDim.x * blockDim.x) {
+        i64 p = arp[r], pe = arp[r + 1], q = trp[r], qe = trp[r + 1];
+        i64 w = FILL ? off[r] : 0;
+        u32 c = 0;
+        while (p < pe || q < qe) {
+            u32 col;
+            double x = 0.0, y = 0.0;
+            if (q >= qe || (p < pe && acol[p] < tcol[q])) {
+                col = acol[p];
+                x = aval[p++];
+            } else if (p >= pe || tcol[q] < acol[p]) {
+                col = tcol[q];
+                y = tval[q++];
+            } else {
+                col = acol[p];
+                x = aval[p++];
+                y = tval[q++];
+            }
+            if (FILL) {
+                ocol[w] = col;
+                oval[w] = 0.5 * (x + y);
+                ++w;
+            }
+            ++c;
+        }
+        if (!FILL) cnt[r] = c;
+    }
+}
+}  // namespace
+
+void symmetrize_csr(Csr& a, Csr& out, cudaStream_t s) {
+    ensure_sorted(a, s);
+    Csr t;
+    transpose_csr(a, t, s);
+    const i64 n = a.nr;
+    DBuf<u32> cnt(n + 1, s);
+    DNQ_CUDA(cudaMemsetAsync(cnt.p + n, 0, 4, s));
+    const int grid = gsz(n);
+    k_sym_merge<false><<<grid, 256, 0, s>>>(a.rowptr.p, a.col.p, a.val.p, t.rowptr.p, t.col.p,
+                                            t.val.p, n, cnt.p, nullptr, nullptr, nullptr);
+    DNQ_CHECK_LAUNCH();
+    out.nr = out.nc = n;
+    out.rowptr.alloc(n + 1, s);
+    size_t tmp = 0;
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, out.rowptr.p, n + 1, s));
+    DBuf<u8> tb(tmp, s);
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, cnt.p, out.rowptr.p, n + 1, s));
+    DNQ_CUDA(cudaMemcpyAsync(&out.nnz, out.rowptr.p + n, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    out.col.alloc(out.nnz, s);
+    out.val.alloc(out.nnz, s);
+    k_sym_merge<true><<<grid, 256, 0, s>>>(a.rowptr.p, a.col.p, a.val.p, t.rowptr.p, t.col.p,
+                                           t.val.p, n, nullptr, out.rowptr.p, out.col.p,
+                                           out.val.p);
+    DNQ_CHECK_LAUNCH();
+    out.sorted = true;
+    DNQ_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace dnq
 
 namespace dnq {
@@ -101,6 +170,22 @@ void ensure_f32_all(Csr& m, cudaStream_t s);
 using namespace dnq;
 
 extern "C" {
+
+int dnq_ham_symmetrize(dnq_ham_t h, void* stream, dnq_ham_t* out) {
+    DNQ_API_BEGIN
+    require(h && out, DNQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    require(h->vv.nr == h->vv.nc, DNQ_ERR_INVALID, "block is not square");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    std::unique_ptr<dnq_ham_s> H(new dnq_ham_s);
+    H->device = h->device;
+    H->stream = s;
+    H->n_v = h->n_v;
+    symmetrize_csr(h->vv, H->vv, s);
+    *out = H.release();
+    DNQ_API_END
+}
 
 int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp, const double* diag_p,
                        double* yv, double* yp, int precision, void* stream) {

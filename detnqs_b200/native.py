@@ -56,7 +56,7 @@ EXPORTS = (
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
     "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
     "dnq_server_wait", "dnq_server_set_budget", "dnq_server_pause", "dnq_server_stats",
-    "dnq_ctx_create_wide", "dnq_wide_diag", "dnq_wide_build",
+    "dnq_ctx_create_wide", "dnq_wide_diag", "dnq_wide_build", "dnq_ham_symmetrize",
 )
 
 
@@ -145,6 +145,7 @@ _sig("dnq_server_stats", _P, _P)
 _sig("dnq_ctx_create_wide", _I, _P, _P, _D, _I, C.POINTER(_P))
 _sig("dnq_wide_diag", _P, _P, _I64, _P, _P)
 _sig("dnq_wide_build", _P, _P, _I64, _P, _I, _D, _P, C.POINTER(_P))
+_sig("dnq_ham_symmetrize", _P, _P, C.POINTER(_P))
 _sig("dnq_ham_eff_from", _P, _P, _D, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_variational_energy", _P, _P, _I64, _P, _I, _I, _D, C.POINTER(_D), _P)
 _sig("dnq_ham_eff", _P, _P, _P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _D, _I, _D, _I, _I,

@@ -241,6 +241,11 @@ int dnq_ham_eff(const uint32_t* vv_rows, const uint32_t* vv_cols,
                 double epsilon, int precision, int device, void* stream,
                 dnq_ham_t* out);
 
+/* 0.5 (H + H^T) of the V block as a new handle (no reference counterpart:
+ * the screened blocks of the dynamic policy, and so H_eff built from them,
+ * are not symmetric; eigen-solvers take this symmetric part). */
+int dnq_ham_symmetrize(dnq_ham_t h, void* stream, dnq_ham_t* out);
+
 /* ---- batched engine (no reference counterpart) ------------------------------
  * Many independent systems (each with its own integral context and V, any
  * n_orb < 64) built and contracted together: the rows of all systems form

@@ -142,3 +142,26 @@ def test_one_word_entry_points_refuse_wide_context(n100):
     sysm, V, ctx, chk = n100
     with pytest.raises(ValueError, match="more than 64 orbitals"):
         core.get_ham_diag(np.zeros((1, 2), np.uint64), ctx)
+
+
+def test_symmetric_part_and_lanczos(n100):
+    """0.5 (H + H^T) on the device equals the same sum on the host bit for
+    bit, and device Lanczos finds its lowest eigenvalue."""
+    from detnqs_b200 import eigen as E
+    from detnqs_b200 import native as N
+    from detnqs_b200 import wide as Wd
+    sysm, V, ctx, chk = n100
+    psi = hf_dominated_psi(len(V), 7, 2e-5)
+    H = Wd.build_wide(ctx, V, psi, n_orb=100, eps1=1e-5)
+    hpp = Wd.p_diag(H, ctx)
+    num, den = H.local_energy(psi)
+    Heff = Wd.ham_eff_wide(H, hpp, num / den, epsilon=0.1, precision=N.F64)
+    Hs = E.symmetric_part(Heff)
+    A = Heff.to_scipy(0).toarray()
+    ref = 0.5 * (A + A.T)
+    np.testing.assert_array_equal(Hs.to_scipy(0).toarray(), ref)
+    lam, steps = E.lowest_eigenvalue(Hs)
+    exact = np.linalg.eigvalsh(ref)[0]
+    assert abs(lam - exact) <= 1e-10 * abs(exact), (lam, exact, steps)
+    for h in (H, Heff, Hs):
+        h.close()
