@@ -103,16 +103,25 @@ __global__ void k_screen(const i64* rp, const double* val, i64 n, const double* 
     }
 }
 
+// Capacity of output row i: its H_VV entries plus the sum of the H_PV
+// column lengths it scatters (warp per row, so rows with millions of
+// entries do not serialise on one thread).
 __global__ void k_cap(const i64* vprp, const u32* vpcol, const i64* pvrp, const u8* skip,
                       const i64* vvrp, i64 nv, i64* cap) {
-    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nv;
-         i += (i64)gridDim.x * blockDim.x) {
-        i64 c = vvrp[i + 1] - vvrp[i];
-        for (i64 t = vprp[i]; t < vprp[i + 1]; ++t) {
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    for (i64 i = gw; i < nv; i += nw) {
+        i64 c = 0;
+        for (i64 t = vprp[i] + lane; t < vprp[i + 1]; t += 32) {
             const u32 k = vpcol[t];
             if (!skip[k]) c += pvrp[k + 1] - pvrp[k];
         }
-        cap[i] = c < nv ? c : nv;
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) {
+            c += vvrp[i + 1] - vvrp[i];
+            cap[i] = c < nv ? c : nv;
+        }
     }
 }
 
@@ -163,49 +172,106 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
         if (lane == 0) i = atomicAdd(P.next_row, 1);
         i = __shfl_sync(0xffffffffu, i, 0);
         if (i >= P.nv) break;
-        // ---- scatter H_VP row i, k ascending
-        for (i64 t = P.vprp[i]; t < P.vprp[i + 1]; ++t) {
-            const u32 k = P.vpcol[t];
-            if (P.skip[k]) continue;
-            const double s = P.dinv[k];
-            const double a = P.vpval[t];
-            const bool need = !(a == 0.0 || s == 0.0);
-            const i64 q0 = P.pvrp[k], q1 = P.pvrp[k + 1];
-            if (!F32) {
-                const double as = __dmul_rn(a, s);
-                for (i64 q = q0 + lane; q < q1; q += 32) {
-                    const u32 j = P.pvcol[q];
-                    atomicOr(&bits[j >> 5], 1u << (j & 31));
-                    if (need) acc[j] = __dadd_rn(acc[j], __dmul_rn(as, P.pvval[q]));
+        // ---- scatter H_VP row i, k ascending.  Every H_PV column k of this
+        // row holds row i itself, so the diagonal element receives one term
+        // per k: it is kept in lane 0's registers (same order of additions).
+        // The metadata of 32 k's is fetched at once by the lanes; columns
+        // that hold only row i need no slab access at all.
+        double dacc = 0.0;             // FP64 diagonal sum
+        float dhi = 0.0f, dlo = 0.0f;  // FP32 float-float diagonal sum
+        bool dtouch = false;
+        const i64 t_end = P.vprp[i + 1];
+        for (i64 t0 = P.vprp[i]; t0 < t_end; t0 += 32) {
+            const i64 tl = t0 + lane;
+            u32 kl = 0;
+            bool sk = true;
+            double al = 0.0, sl = 0.0;
+            i64 q0l = 0, q1l = 0, qdl = -1;
+            if (tl < t_end) {
+                kl = P.vpcol[tl];
+                sk = P.skip[kl] != 0;
+                sl = P.dinv[kl];
+                al = F32 ? (double)P.vpval32[tl] : P.vpval[tl];
+                q0l = P.pvrp[kl];
+                q1l = P.pvrp[kl + 1];
+                i64 lo = q0l, hi = q1l;   // position of row i in column k
+                while (lo < hi) {
+                    const i64 mid = (lo + hi) >> 1;
+                    if (P.pvcol[mid] < (u32)i) lo = mid + 1; else hi = mid;
                 }
-            } else {
-                // a * D^-1 in FP64, carried as a float pair hi + lo (the FP64
-                // shift keeps its precision; only the stored values are FP32)
-                const double asd = __dmul_rn((double)P.vpval32[t], s);
-                const float as = (float)asd;
-                const float as_lo = (float)(asd - (double)as);
-                for (i64 q = q0 + lane; q < q1; q += 32) {
-                    const u32 j = P.pvcol[q];
-                    atomicOr(&bits[j >> 5], 1u << (j & 31));
-                    if (need) {
-                        const float b = P.pvval32[q];
+                qdl = lo;
+            }
+            const double bdl = (tl < t_end && !sk) ? (F32 ? (double)P.pvval32[qdl] : P.pvval[qdl])
+                                                   : 0.0;
+            const int cnt = (int)min((i64)32, t_end - t0);
+            for (int u = 0; u < cnt; ++u) {
+                if (__shfl_sync(0xffffffffu, (int)sk, u)) continue;
+                const double s = __shfl_sync(0xffffffffu, sl, u);
+                const double a = __shfl_sync(0xffffffffu, al, u);
+                const i64 q0 = __shfl_sync(0xffffffffu, q0l, u);
+                const i64 q1 = __shfl_sync(0xffffffffu, q1l, u);
+                const i64 qd = __shfl_sync(0xffffffffu, qdl, u);
+                const double bd = __shfl_sync(0xffffffffu, bdl, u);
+                const bool need = !(a == 0.0 || s == 0.0);
+                if (!F32) {
+                    const double as = __dmul_rn(a, s);
+                    if (lane == 0) {
+                        dtouch = true;
+                        if (need) dacc = __dadd_rn(dacc, __dmul_rn(as, bd));
+                    }
+                    if (q1 - q0 > 1) {
+                        for (i64 q = q0 + lane; q < q1; q += 32) {
+                            if (q == qd) continue;
+                            const u32 j = P.pvcol[q];
+                            atomicOr(&bits[j >> 5], 1u << (j & 31));
+                            if (need) acc[j] = __dadd_rn(acc[j], __dmul_rn(as, P.pvval[q]));
+                        }
+                    }
+                } else {
+                    // a * D^-1 in FP64, carried as a float pair hi + lo (the
+                    // FP64 shift keeps its precision; only stored values are
+                    // FP32)
+                    const double asd = __dmul_rn(a, s);
+                    const float as = (float)asd;
+                    const float as_lo = (float)(asd - (double)as);
+                    auto add = [&](float& hi, float& lo, float b) {
+                        // float-float accumulation: TwoProduct and TwoSum errors
+                        // go to the error word, renormalised after each add
+                        // (FastTwoSum; Dekker 1971)
                         const float p = __fmul_rn(as, b);
                         const float pe = fmaf(as, b, -p) + __fmul_rn(as_lo, b);
-                        float2 cur = acc2[j];
                         float s2, e;
-                        f_two_sum(cur.x, p, s2, e);
-                        const float c = __fadd_rn(cur.y, __fadd_rn(e, pe));
-                        // renormalise (FastTwoSum, |s2| >= |c|): the error word
-                        // stays below half an ulp of the sum, so its own
-                        // rounding does not pile up over ~1e6 terms
-                        cur.x = __fadd_rn(s2, c);
-                        cur.y = __fsub_rn(c, __fsub_rn(cur.x, s2));
-                        acc2[j] = cur;
+                        f_two_sum(hi, p, s2, e);
+                        const float c = __fadd_rn(lo, __fadd_rn(e, pe));
+                        hi = __fadd_rn(s2, c);
+                        lo = __fsub_rn(c, __fsub_rn(hi, s2));
+                    };
+                    if (lane == 0) {
+                        dtouch = true;
+                        if (need) add(dhi, dlo, (float)bd);
+                    }
+                    if (q1 - q0 > 1) {
+                        for (i64 q = q0 + lane; q < q1; q += 32) {
+                            if (q == qd) continue;
+                            const u32 j = P.pvcol[q];
+                            atomicOr(&bits[j >> 5], 1u << (j & 31));
+                            if (need) {
+                                float2 cur = acc2[j];
+                                add(cur.x, cur.y, P.pvval32[q]);
+                                acc2[j] = cur;
+                            }
+                        }
                     }
                 }
+                __syncwarp();
             }
-            __syncwarp();
         }
+        if (lane == 0 && dtouch) {
+            atomicOr(&bits[i >> 5], 1u << (i & 31));
+            if (F32) acc2[i] = make_float2(dhi, dlo);
+            else acc[i] = dacc;
+        }
+        __syncwarp();
         if (F32) {   // fold (sum, err) pairs to FP64
             for (int wd = lane; wd < P.words; wd += 32)
                 for (u32 m = bits[wd]; m; m &= m - 1) {

@@ -21,6 +21,7 @@
 #include <cuda/std/tuple>
 
 #include <memory>
+#include <vector>
 
 #include "context.cuh"
 #include "ham.cuh"
@@ -274,15 +275,69 @@ struct WParams {
     const double* psi;
     const double* diag;
     int* next_row;
-    u32* cnt_vv;
+    // work units: a whole row, or for rows with very many candidates one
+    // segment each (segment 0 = diagonal + singles, 1 + p = occupied pair p
+    // in the order x = 1.., y < x, p = x(x-1)/2 + y)
+    const uint4* units;   // {row, first segment, end segment, 0}
+    i64 n_units;
+    u32* cnt_vv;          // per unit
     u32* cnt_vp;
-    const i64* off_vv;
+    const i64* off_vv;    // per unit
     const i64* off_vp;
     u32* vv_col;
     double* vv_val;
     Key4* vp_key;
     double* vp_val;
 };
+
+constexpr u32 kAllSegments = 0xffffffffu;
+
+__device__ __forceinline__ double row_cut(const WParams& P, int r, double& psr) {
+    psr = 0.0;
+    if (!P.dynamic) return P.cut;
+    psr = P.psi[r];
+    return fmax(P.eps1 / fmax(fabs(psr), kAmpDelta), P.cut);   // build_ham.cpp:161-186
+}
+
+// Candidates of a row: singles + the table prefix of every occupied pair
+// (lane-parallel binary searches); rows above a threshold are split into
+// per-pair units.
+__global__ void k_wide_work(WParams P, unsigned long long* work) {
+    __shared__ WRow rows[kWW];
+    const int lane = threadIdx.x & 31;
+    WRow& R = rows[threadIdx.x >> 5];
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    for (i64 r = gw; r < P.n; r += nw) {
+        const u64* d = P.dets + 4 * r;
+        load_wrow(R, M2{d[0], d[1]}, M2{d[2], d[3]}, P.n_orb);
+        double psr;
+        const double cut = row_cut(P, (int)r, psr);
+        const int npairs = R.ne * (R.ne - 1) / 2;
+        unsigned long long w = 0;
+        for (int p = lane; p < npairs; p += 32) {
+            int x = (int)((1.0 + sqrt(1.0 + 8.0 * p)) * 0.5);
+            while (x * (x - 1) / 2 > p) --x;
+            while ((x + 1) * x / 2 <= p) ++x;
+            const int y = p - x * (x - 1) / 2;
+            const i64 row = pair_row(R.occ[x], R.occ[y]);
+            const i64 lo = __ldg(&P.C.tab.off[row]), len = __ldg(&P.C.tab.off[row + 1]) - lo;
+            i64 L = 0, H = len;
+            if (cut > 0.0) {
+                while (L < H) {
+                    const i64 mid = (L + H) >> 1;
+                    if (fabs(__ldg(&P.C.tab.v[lo + mid])) >= cut) L = mid + 1; else H = mid;
+                }
+            } else {
+                L = len;
+            }
+            w += (unsigned long long)L;
+        }
+        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0) work[r] = w + (unsigned long long)(R.na * R.nva + R.nb * R.nvb);
+        __syncwarp();
+    }
+}
 
 template <bool FILL>
 __global__ void __launch_bounds__(kWW * 32) k_wide_build(WParams P) {
@@ -291,28 +346,21 @@ __global__ void __launch_bounds__(kWW * 32) k_wide_build(WParams P) {
     WRow& R = rows[threadIdx.x >> 5];
     const unsigned lt = lanemask_lt();
     for (;;) {
-        int r = 0;
-        if (lane == 0) r = atomicAdd(P.next_row, 1);
-        r = __shfl_sync(0xffffffffu, r, 0);
-        if (r >= P.n) break;
+        int ui = 0;
+        if (lane == 0) ui = atomicAdd(P.next_row, 1);
+        ui = __shfl_sync(0xffffffffu, ui, 0);
+        if (ui >= P.n_units) break;
+        const uint4 U = P.units[ui];
+        const int r = (int)U.x;
         const u64* d = P.dets + 4 * (i64)r;
         load_wrow(R, M2{d[0], d[1]}, M2{d[2], d[3]}, P.n_orb);
-        double psr = 0.0, cut = P.cut;
-        if (P.dynamic) {
-            psr = P.psi[r];
-            cut = fmax(P.eps1 / fmax(fabs(psr), kAmpDelta), P.cut);   // build_ham.cpp:161-186
-        }
+        double psr;
+        const double cut = row_cut(P, r, psr);
+        const int npairs = R.ne * (R.ne - 1) / 2;
+        const u32 seg_lo = U.y;
+        const u32 seg_hi = U.z == kAllSegments ? (u32)npairs + 1 : U.z;
         u32 nvv = 0, nvp = 0;
-        i64 wvv = FILL ? P.off_vv[r] : 0, wvp = FILL ? P.off_vp[r] : 0;
-        const double dg = P.diag[r];
-        if (fabs(dg) > kElemThresh) {
-            if (FILL && lane == 0) {
-                P.vv_col[wvv] = (u32)r;
-                P.vv_val[wvv] = dg;
-            }
-            if (FILL) wvv += 1;
-            else if (lane == 0) nvv = 1;
-        }
+        i64 wvv = FILL ? P.off_vv[ui] : 0, wvp = FILL ? P.off_vp[ui] : 0;
         // one step of 32 candidates: route, count or write in candidate order
         auto emit = [&](bool valid, const M2& ka, const M2& kb, double h) {
             int route = 0;
@@ -343,72 +391,102 @@ __global__ void __launch_bounds__(kWW * 32) k_wide_build(WParams P) {
             }
             wvp += __popc(mp);
         };
-        // singles: alpha then beta, holes outer, particles inner
-        const int nsa = R.na * R.nva, nst = nsa + R.nb * R.nvb;
-        for (int t0 = 0; t0 < nst; t0 += 32) {
-            const int t = t0 + lane;
-            bool valid = t < nst;
-            M2 ka = R.a, kb = R.b;
-            double h = 0.0;
-            if (valid) {
-                int s, hh, pp;
-                if (t < nsa) {
-                    s = 0; hh = R.occa[t / R.nva]; pp = R.vira[t % R.nva];
-                    flip(ka, hh); flip(ka, pp);
-                } else {
-                    const int u = t - nsa;
-                    s = 1; hh = R.occb[u / R.nvb]; pp = R.virb[u % R.nvb];
-                    flip(kb, hh); flip(kb, pp);
+        if (seg_lo == 0) {
+            const double dg = P.diag[r];
+            if (fabs(dg) > kElemThresh) {
+                if (FILL && lane == 0) {
+                    P.vv_col[wvv] = (u32)r;
+                    P.vv_val[wvv] = dg;
                 }
-                h = single2(P.C, R, s, hh, pp);
-                if (P.dynamic && !(fabs(h * psr) >= P.eps1)) valid = false;   // :190-192
+                if (FILL) wvv += 1;
+                else if (lane == 0) nvv = 1;
             }
-            emit(valid, ka, kb, h);
+            // singles: alpha then beta, holes outer, particles inner
+            const int nsa = R.na * R.nva, nst = nsa + R.nb * R.nvb;
+            for (int t0 = 0; t0 < nst; t0 += 32) {
+                const int t = t0 + lane;
+                bool valid = t < nst;
+                M2 ka = R.a, kb = R.b;
+                double h = 0.0;
+                if (valid) {
+                    int sp, hh, pp;
+                    if (t < nsa) {
+                        sp = 0; hh = R.occa[t / R.nva]; pp = R.vira[t % R.nva];
+                        flip(ka, hh); flip(ka, pp);
+                    } else {
+                        const int u = t - nsa;
+                        sp = 1; hh = R.occb[u / R.nvb]; pp = R.virb[u % R.nvb];
+                        flip(kb, hh); flip(kb, pp);
+                    }
+                    h = single2(P.C, R, sp, hh, pp);
+                    if (P.dynamic && !(fabs(h * psr) >= P.eps1)) valid = false;   // :190-192
+                }
+                emit(valid, ka, kb, h);
+            }
         }
         // heat-bath doubles over occupied pairs (ham_utils.hpp:280-313)
-        for (int x = 1; x < R.ne; ++x) {
+        const int p_lo = seg_lo == 0 ? 0 : (int)seg_lo - 1;
+        const int p_hi = (int)seg_hi - 1;
+        int x = 1, y = 0;
+        {
+            int xx = (int)((1.0 + sqrt(1.0 + 8.0 * p_lo)) * 0.5);
+            while (xx * (xx - 1) / 2 > p_lo) --xx;
+            while ((xx + 1) * xx / 2 <= p_lo) ++xx;
+            x = max(xx, 1);
+            y = p_lo - x * (x - 1) / 2;
+        }
+        for (int p = p_lo; p < p_hi; ++p) {
             const int i = R.occ[x];
-            for (int y = 0; y < x; ++y) {
-                const int jj0 = R.occ[y];
-                const i64 row = pair_row(i, jj0);
-                const i64 lo = __ldg(&P.C.tab.off[row]);
-                const i64 len = prefix_len(P.C.tab.v + lo, __ldg(&P.C.tab.off[row + 1]) - lo, cut);
-                const int ii = max(i, jj0), jj = min(i, jj0);
-                for (i64 e0 = 0; e0 < len; e0 += 32) {
-                    const i64 e = e0 + lane;
-                    bool valid = e < len;
-                    M2 ka = R.a, kb = R.b;
-                    double h = 0.0;
-                    if (valid) {
-                        const u16 ab = __ldg(&P.C.tab.ab[lo + e]);
-                        const int A = ab & 0xff, B = ab >> 8;
-                        const bool oA = (A >> 1) >= P.n_orb || bit((A & 1) ? R.b : R.a, A >> 1);
-                        const bool oB = (B >> 1) >= P.n_orb || bit((B & 1) ? R.b : R.a, B >> 1);
-                        if (oA || oB) {
-                            valid = false;
-                        } else {
-                            M2* w[2] = {&ka, &kb};
-                            flip(*w[ii & 1], ii >> 1);
-                            flip(*w[jj & 1], jj >> 1);
-                            flip(*w[A & 1], A >> 1);
-                            flip(*w[B & 1], B >> 1);
-                            h = double2(R.a, R.b, ii, jj, A, B, __ldg(&P.C.tab.v[lo + e]));
-                        }
+            const int jj0 = R.occ[y];
+            const i64 row = pair_row(i, jj0);
+            const i64 lo = __ldg(&P.C.tab.off[row]);
+            const i64 len = prefix_len(P.C.tab.v + lo, __ldg(&P.C.tab.off[row + 1]) - lo, cut);
+            const int ii = max(i, jj0), jj = min(i, jj0);
+            for (i64 e0 = 0; e0 < len; e0 += 32) {
+                const i64 e = e0 + lane;
+                bool valid = e < len;
+                M2 ka = R.a, kb = R.b;
+                double h = 0.0;
+                if (valid) {
+                    const u16 ab = __ldg(&P.C.tab.ab[lo + e]);
+                    const int A = ab & 0xff, B = ab >> 8;
+                    const bool oA = (A >> 1) >= P.n_orb || bit((A & 1) ? R.b : R.a, A >> 1);
+                    const bool oB = (B >> 1) >= P.n_orb || bit((B & 1) ? R.b : R.a, B >> 1);
+                    if (oA || oB) {
+                        valid = false;
+                    } else {
+                        M2* w[2] = {&ka, &kb};
+                        flip(*w[ii & 1], ii >> 1);
+                        flip(*w[jj & 1], jj >> 1);
+                        flip(*w[A & 1], A >> 1);
+                        flip(*w[B & 1], B >> 1);
+                        h = double2(R.a, R.b, ii, jj, A, B, __ldg(&P.C.tab.v[lo + e]));
                     }
-                    emit(valid, ka, kb, h);
                 }
+                emit(valid, ka, kb, h);
+            }
+            if (++y == x) {
+                ++x;
+                y = 0;
             }
         }
         if (!FILL) {
             const u32 a = __reduce_add_sync(0xffffffffu, nvv);
             const u32 b = __reduce_add_sync(0xffffffffu, nvp);
             if (lane == 0) {
-                P.cnt_vv[r] = a;
-                P.cnt_vp[r] = b;
+                P.cnt_vv[ui] = a;
+                P.cnt_vp[ui] = b;
             }
         }
         __syncwarp();
     }
+}
+
+// Row pointers from unit offsets: row r starts at its first unit.
+__global__ void k_row_starts(const i64* uoff, const u32* first_unit, i64 n, i64* rowptr) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r <= n;
+         r += (i64)gridDim.x * blockDim.x)
+        rowptr[r] = uoff[first_unit[r]];
 }
 
 __global__ void k_iota4(u32* p, i64 n) {
@@ -515,35 +593,77 @@ void wide_build(dnq_ctx_s* ctx, const u64* V_in, i64 n, const double* psi_in, in
     P.cut = P.dynamic ? ctx->hb_thr : hb_cutoff(ctx, eps1);
     P.psi = psi.p;
     P.diag = H->diag.p;
+    const int sms = sm_count(ctx->device);
+
+    // ---- units: rows above kHeavy candidates are split per occupied pair
+    constexpr unsigned long long kHeavy = 1ull << 15;
+    std::vector<uint4> units;
+    std::vector<u32> first(n + 1);
+    {
+        DBuf<unsigned long long> work(n, s);
+        k_wide_work<<<sms * 16, kWW * 32, 0, s>>>(P, work.p);
+        DNQ_CHECK_LAUNCH();
+        std::vector<unsigned long long> hw(n);
+        std::vector<u64> hd(4 * n);
+        DNQ_CUDA(cudaMemcpyAsync(hw.data(), work.p, 8 * n, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaMemcpyAsync(hd.data(), V.p, 32 * n, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        units.reserve(n);
+        for (i64 r = 0; r < n; ++r) {
+            first[r] = (u32)units.size();
+            if (hw[r] > kHeavy) {
+                int ne = 0;
+                for (int q = 0; q < 4; ++q) ne += __builtin_popcountll(hd[4 * r + q]);
+                const u32 np = (u32)(ne * (ne - 1) / 2);
+                for (u32 g = 0; g <= np; ++g) units.push_back(make_uint4((u32)r, g, g + 1, 0));
+            } else {
+                units.push_back(make_uint4((u32)r, 0, kAllSegments, 0));
+            }
+        }
+        first[n] = (u32)units.size();
+    }
+    const i64 nu = (i64)units.size();
+    DBuf<uint4> ud(nu, s);
+    DBuf<u32> fd(n + 1, s);
+    DNQ_CUDA(cudaMemcpyAsync(ud.p, units.data(), 16 * nu, cudaMemcpyHostToDevice, s));
+    DNQ_CUDA(cudaMemcpyAsync(fd.p, first.data(), 4 * (n + 1), cudaMemcpyHostToDevice, s));
+    P.units = ud.p;
+    P.n_units = nu;
+
     DBuf<int> next(1, s);
-    DBuf<u32> cvv(n + 1, s), cvp(n + 1, s);
-    DNQ_CUDA(cudaMemsetAsync(cvv.p + n, 0, 4, s));
-    DNQ_CUDA(cudaMemsetAsync(cvp.p + n, 0, 4, s));
+    DBuf<u32> cvv(nu + 1, s), cvp(nu + 1, s);
+    DNQ_CUDA(cudaMemsetAsync(cvv.p + nu, 0, 4, s));
+    DNQ_CUDA(cudaMemsetAsync(cvp.p + nu, 0, 4, s));
     P.next_row = next.p;
     P.cnt_vv = cvv.p;
     P.cnt_vp = cvp.p;
     int per_sm = 0;
     DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wide_build<false>, kWW * 32,
                                                            0));
-    const int grid = std::max(1, per_sm) * sm_count(ctx->device);
+    const int grid = std::max(1, per_sm) * sms;
     DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
     k_wide_build<false><<<grid, kWW * 32, 0, s>>>(P);
     DNQ_CHECK_LAUNCH();
 
+    DBuf<i64> uvv(nu + 1, s), uvp(nu + 1, s);
+    exscan(cvv.p, uvv.p, nu + 1, s);
+    exscan(cvp.p, uvp.p, nu + 1, s);
     H->vv.nr = H->vv.nc = n;
     H->vv.rowptr.alloc(n + 1, s);
-    exscan(cvv.p, H->vv.rowptr.p, n + 1, s);
     DBuf<i64> offp(n + 1, s);
-    exscan(cvp.p, offp.p, n + 1, s);
-    H->vv.nnz = fetch(H->vv.rowptr.p + n, s);
-    const i64 nvp = fetch(offp.p + n, s);
+    k_row_starts<<<blocks(n + 1), 256, 0, s>>>(uvv.p, fd.p, n, H->vv.rowptr.p);
+    DNQ_CHECK_LAUNCH();
+    k_row_starts<<<blocks(n + 1), 256, 0, s>>>(uvp.p, fd.p, n, offp.p);
+    DNQ_CHECK_LAUNCH();
+    H->vv.nnz = fetch(uvv.p + nu, s);
+    const i64 nvp = fetch(uvp.p + nu, s);
     require(nvp < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "H_VP has more than 2^32 entries");
     H->vv.col.alloc(H->vv.nnz, s);
     H->vv.val.alloc(H->vv.nnz, s);
     DBuf<Key4> keys(nvp, s);
     DBuf<double> vpv(nvp, s);
-    P.off_vv = H->vv.rowptr.p;
-    P.off_vp = offp.p;
+    P.off_vv = uvv.p;
+    P.off_vp = uvp.p;
     P.vv_col = H->vv.col.p;
     P.vv_val = H->vv.val.p;
     P.vp_key = keys.p;
