@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include <memory>
+#include <vector>
 
 #include "ham.cuh"
 
@@ -143,6 +144,14 @@ struct HeffParams {
     double* gacc;    // per-warp dense accumulators when not in shared memory
     u32* gbits;
     int words;       // bitmap words per warp
+    // rows with very many H_VP entries: diagonal precomputed, walk limited
+    // to the k's whose H_PV column holds other rows
+    const int* long_id;          // per row: long-row index or -1 (null: none)
+    const i64* long_off;         // per long row: range in long_list
+    const u32* long_list;        // VP positions t, ascending
+    const double* long_diag;     // FP64 diagonal sum
+    const float2* long_diag2;    // FP32 float-float diagonal sum
+    const u32* long_touch;       // any k of the row not screened out
 };
 
 // F32 = false: acc holds FP64 sums.  F32 = true: during the scatter acc
@@ -180,14 +189,20 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
         double dacc = 0.0;             // FP64 diagonal sum
         float dhi = 0.0f, dlo = 0.0f;  // FP32 float-float diagonal sum
         bool dtouch = false;
-        const i64 t_end = P.vprp[i + 1];
-        for (i64 t0 = P.vprp[i]; t0 < t_end; t0 += 32) {
-            const i64 tl = t0 + lane;
+        const int lid = P.long_id ? P.long_id[i] : -1;
+        const u32* list = lid >= 0 ? P.long_list + P.long_off[lid] : nullptr;
+        const i64 t_base = P.vprp[i];
+        const i64 n_items = lid >= 0 ? P.long_off[lid + 1] - P.long_off[lid]
+                                     : P.vprp[i + 1] - t_base;
+        for (i64 x0 = 0; x0 < n_items; x0 += 32) {
+            const i64 xl = x0 + lane;
+            const bool inr = xl < n_items;
+            const i64 tl = inr ? (list ? (i64)list[xl] : t_base + xl) : 0;
             u32 kl = 0;
             bool sk = true;
             double al = 0.0, sl = 0.0;
             i64 q0l = 0, q1l = 0, qdl = -1;
-            if (tl < t_end) {
+            if (inr) {
                 kl = P.vpcol[tl];
                 sk = P.skip[kl] != 0;
                 sl = P.dinv[kl];
@@ -201,9 +216,8 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                 }
                 qdl = lo;
             }
-            const double bdl = (tl < t_end && !sk) ? (F32 ? (double)P.pvval32[qdl] : P.pvval[qdl])
-                                                   : 0.0;
-            const int cnt = (int)min((i64)32, t_end - t0);
+            const double bdl = (inr && !sk) ? (F32 ? (double)P.pvval32[qdl] : P.pvval[qdl]) : 0.0;
+            const int cnt = (int)min((i64)32, n_items - x0);
             for (int u = 0; u < cnt; ++u) {
                 if (__shfl_sync(0xffffffffu, (int)sk, u)) continue;
                 const double s = __shfl_sync(0xffffffffu, sl, u);
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                 const bool need = !(a == 0.0 || s == 0.0);
                 if (!F32) {
                     const double as = __dmul_rn(a, s);
-                    if (lane == 0) {
+                    if (lane == 0 && lid < 0) {
                         dtouch = true;
                         if (need) dacc = __dadd_rn(dacc, __dmul_rn(as, bd));
                     }
@@ -246,7 +260,7 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                         hi = __fadd_rn(s2, c);
                         lo = __fsub_rn(c, __fsub_rn(hi, s2));
                     };
-                    if (lane == 0) {
+                    if (lane == 0 && lid < 0) {
                         dtouch = true;
                         if (need) add(dhi, dlo, (float)bd);
                     }
@@ -265,6 +279,13 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
                 }
                 __syncwarp();
             }
+        }
+        if (lid >= 0 && lane == 0) {
+            dtouch = P.long_touch[lid] != 0u;
+            dacc = P.long_diag[lid];
+            const float2 d2 = P.long_diag2[lid];
+            dhi = d2.x;
+            dlo = d2.y;
         }
         if (lane == 0 && dtouch) {
             atomicOr(&bits[i >> 5], 1u << (i & 31));
@@ -339,6 +360,86 @@ __global__ void k_compact(const i64* capoff, const u32* tcol, const double* tval
             val[dst + t] = tval[src + t];
         }
     }
+}
+
+// Long rows.  For t in [t0, t1) of H_VP row i: the diagonal term of k =
+// col[t] (H_PV[k, i] is the same stored value as H_VP[i, k], the transpose
+// copies it), a flag for k's whose column holds other rows, and whether any
+// k is kept.  FP64 terms are a*D^-1*a with the kernel's unfused operations;
+// FP32 terms are the TwoProduct pair of the float-pair a*D^-1 and a.
+__global__ void k_long_terms(const u32* vpcol, const double* vpval, const float* vpval32,
+                             const i64* pvrp, const double* dinv, const u8* skip, i64 t0, i64 t1,
+                             bool f32, double* term, float2* term2, u8* multi, u32* touch) {
+    for (i64 t = t0 + blockIdx.x * (i64)blockDim.x + threadIdx.x; t < t1;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 k = vpcol[t];
+        const bool sk = skip[k] != 0;
+        const double s = dinv[k];
+        const double a = f32 ? (double)vpval32[t] : vpval[t];
+        const bool need = !sk && !(a == 0.0 || s == 0.0);
+        const i64 x = t - t0;
+        multi[x] = (!sk && pvrp[k + 1] - pvrp[k] > 1) ? 1 : 0;
+        if (!sk) atomicOr(touch, 1u);
+        if (!f32) {
+            term[x] = need ? __dmul_rn(__dmul_rn(a, s), a) : 0.0;
+        } else {
+            const double asd = __dmul_rn(a, s);
+            const float as = (float)asd;
+            const float as_lo = (float)(asd - (double)as);
+            const float b = (float)a;
+            const float p = __fmul_rn(as, b);
+            const float pe = fmaf(as, b, -p) + __fmul_rn(as_lo, b);
+            term2[x] = need ? make_float2(p, pe) : make_float2(0.0f, 0.0f);
+        }
+    }
+}
+
+// FP64: the terms summed in k order by one thread (the order of the
+// reference's accumulation, so the result is bit-identical).
+__global__ void k_long_sum64(const double* term, i64 n, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double acc = 0.0;
+    i64 t = 0;
+    for (; t + 8 <= n; t += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = term[t + q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc = __dadd_rn(acc, v[q]);
+    }
+    for (; t < n; ++t) acc = __dadd_rn(acc, term[t]);
+    *out = acc;
+}
+
+// FP32: float-float sums per lane (terms strided by 32), merged in lane
+// order: deterministic, accurate to a few FP32 ulps squared.
+__global__ void k_long_sum32(const float2* term, i64 n, float2* out) {
+    const int lane = threadIdx.x & 31;
+    float hi = 0.0f, lo = 0.0f;
+    auto add = [&](float p, float pe) {
+        float s2, e;
+        f_two_sum(hi, p, s2, e);
+        const float c = __fadd_rn(lo, __fadd_rn(e, pe));
+        hi = __fadd_rn(s2, c);
+        lo = __fsub_rn(c, __fsub_rn(hi, s2));
+    };
+    for (i64 t = lane; t < n; t += 32) add(term[t].x, term[t].y);
+    __shared__ float sh[2][32];
+    sh[0][lane] = hi;
+    sh[1][lane] = lo;
+    __syncwarp();
+    if (lane == 0) {
+        hi = 0.0f;
+        lo = 0.0f;
+        for (int q = 0; q < 32; ++q) add(sh[0][q], sh[1][q]);
+        *out = make_float2(hi, lo);
+    }
+}
+
+__global__ void k_iota_u32(u32* p, i64 n, i64 base) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        p[t] = (u32)(base + t);
 }
 
 __global__ void k_to_f32v(const double* v, i64 n, float* o) {
@@ -479,6 +580,76 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
         DNQ_CHECK_LAUNCH();
         P.vpval32 = vp32.p;
         P.pvval32 = pv32.p;
+    }
+    // ---- rows with very many H_VP entries
+    constexpr i64 kLong = 1 << 16;
+    std::vector<i64> vrp(nv + 1);
+    DNQ_CUDA(cudaMemcpyAsync(vrp.data(), VP.rowptr.p, (nv + 1) * 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    std::vector<i64> longs;
+    for (i64 r = 0; r < nv; ++r)
+        if (vrp[r + 1] - vrp[r] > kLong) longs.push_back(r);
+    const int nl = (int)longs.size();
+    DBuf<int> lid;
+    DBuf<i64> loff;
+    DBuf<u32> llist, ltouch;
+    DBuf<double> ldiag;
+    DBuf<float2> ldiag2;
+    if (nl) {
+        std::vector<int> hid(nv, -1);
+        for (int q = 0; q < nl; ++q) hid[longs[q]] = q;
+        lid.alloc(nv, s);
+        DNQ_CUDA(cudaMemcpyAsync(lid.p, hid.data(), 4 * nv, cudaMemcpyHostToDevice, s));
+        ldiag.alloc(nl, s);
+        ldiag2.alloc(nl, s);
+        ltouch.alloc(nl, s);
+        DNQ_CUDA(cudaMemsetAsync(ltouch.p, 0, 4 * nl, s));
+        DNQ_CUDA(cudaMemsetAsync(ldiag.p, 0, 8 * nl, s));
+        DNQ_CUDA(cudaMemsetAsync(ldiag2.p, 0, 8 * nl, s));
+        std::vector<i64> hoff(nl + 1, 0);
+        std::vector<DBuf<u32>> parts(nl);
+        for (int q = 0; q < nl; ++q) {
+            const i64 t0 = vrp[longs[q]], t1 = vrp[longs[q] + 1], m = t1 - t0;
+            DBuf<double> term;
+            DBuf<float2> term2;
+            if (precision == DNQ_F32) term2.alloc(m, s);
+            else term.alloc(m, s);
+            DBuf<u8> multi(m, s);
+            k_long_terms<<<gs(m), 256, 0, s>>>(VP.col.p, VP.val.p, P.vpval32, PV.rowptr.p, dinv.p,
+                                               skip.p, t0, t1, precision == DNQ_F32, term.p,
+                                               term2.p, multi.p, ltouch.p + q);
+            DNQ_CHECK_LAUNCH();
+            if (precision == DNQ_F32) k_long_sum32<<<1, 32, 0, s>>>(term2.p, m, ldiag2.p + q);
+            else k_long_sum64<<<1, 32, 0, s>>>(term.p, m, ldiag.p + q);
+            DNQ_CHECK_LAUNCH();
+            DBuf<u32> idx(m, s), sel(m, s);
+            DBuf<i64> nsel(1, s);
+            k_iota_u32<<<gs(m), 256, 0, s>>>(idx.p, m, t0);
+            DNQ_CHECK_LAUNCH();
+            size_t tmp = 0;
+            DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, idx.p, multi.p, sel.p, nsel.p, m, s));
+            DBuf<u8> tb(tmp, s);
+            DNQ_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, idx.p, multi.p, sel.p, nsel.p, m, s));
+            i64 ns = 0;
+            DNQ_CUDA(cudaMemcpyAsync(&ns, nsel.p, 8, cudaMemcpyDeviceToHost, s));
+            DNQ_CUDA(cudaStreamSynchronize(s));
+            hoff[q + 1] = hoff[q] + ns;
+            parts[q] = std::move(sel);
+        }
+        llist.alloc(std::max<i64>(1, hoff[nl]), s);
+        for (int q = 0; q < nl; ++q)
+            if (hoff[q + 1] > hoff[q])
+                DNQ_CUDA(cudaMemcpyAsync(llist.p + hoff[q], parts[q].p,
+                                         4 * (hoff[q + 1] - hoff[q]), cudaMemcpyDeviceToDevice, s));
+        loff.alloc(nl + 1, s);
+        DNQ_CUDA(cudaMemcpyAsync(loff.p, hoff.data(), 8 * (nl + 1), cudaMemcpyHostToDevice, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        P.long_id = lid.p;
+        P.long_off = loff.p;
+        P.long_list = llist.p;
+        P.long_diag = ldiag.p;
+        P.long_diag2 = ldiag2.p;
+        P.long_touch = ltouch.p;
     }
     const size_t per_warp = (((size_t)P.words * 4 + 15) & ~(size_t)15) + (size_t)nv * 8;
     const bool smem = per_warp * kHW <= 200 * 1024;
