@@ -105,24 +105,23 @@ __global__ void k_screen(const i64* rp, const double* val, i64 n, const double* 
 }
 
 // Capacity of output row i: its H_VV entries plus the sum of the H_PV
-// column lengths it scatters (warp per row, so rows with millions of
-// entries do not serialise on one thread).
-__global__ void k_cap(const i64* vprp, const u32* vpcol, const i64* pvrp, const u8* skip,
-                      const i64* vvrp, i64 nv, i64* cap) {
-    const int lane = threadIdx.x & 31;
-    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
-    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
-    for (i64 i = gw; i < nv; i += nw) {
-        i64 c = 0;
-        for (i64 t = vprp[i] + lane; t < vprp[i + 1]; t += 32) {
-            const u32 k = vpcol[t];
-            if (!skip[k]) c += pvrp[k + 1] - pvrp[k];
-        }
-        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        if (lane == 0) {
-            c += vvrp[i + 1] - vvrp[i];
-            cap[i] = c < nv ? c : nv;
-        }
+// column lengths it scatters.  Per-entry column lengths first (one thread
+// per H_VP entry), then a segmented sum per row, so a row with millions of
+// entries is spread over the whole GPU.
+__global__ void k_cap_terms(const u32* vpcol, i64 nnz, const i64* pvrp, const u8* skip,
+                            i64* len) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nnz;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 k = vpcol[t];
+        len[t] = skip[k] ? 0 : pvrp[k + 1] - pvrp[k];
+    }
+}
+
+__global__ void k_cap_finish(const i64* sum, const i64* vvrp, i64 nv, i64* cap) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < nv;
+         i += (i64)gridDim.x * blockDim.x) {
+        const i64 c = sum[i] + (vvrp[i + 1] - vvrp[i]);
+        cap[i] = c < nv ? c : nv;
     }
 }
 
@@ -147,8 +146,10 @@ struct HeffParams {
     // rows with very many H_VP entries: diagonal precomputed, walk limited
     // to the k's whose H_PV column holds other rows
     const int* long_id;          // per row: long-row index or -1 (null: none)
-    const i64* long_off;         // per long row: range in long_list
-    const u32* long_list;        // VP positions t, ascending
+    const i64* long_off;         // per long row: range in long_j / long_v / long_v2
+    const u32* long_j;           // output columns j != i of the row, ascending
+    const double* long_v;        // their FP64 sums (k order)
+    const float2* long_v2;       // their FP32 float-float sums
     const double* long_diag;     // FP64 diagonal sum
     const float2* long_diag2;    // FP32 float-float diagonal sum
     const u32* long_touch;       // any k of the row not screened out
@@ -190,14 +191,21 @@ __global__ void __launch_bounds__(kHW * 32) k_heff(HeffParams P) {
         float dhi = 0.0f, dlo = 0.0f;  // FP32 float-float diagonal sum
         bool dtouch = false;
         const int lid = P.long_id ? P.long_id[i] : -1;
-        const u32* list = lid >= 0 ? P.long_list + P.long_off[lid] : nullptr;
+        if (lid >= 0) {   // precomputed sums of a long row (same order, same values)
+            for (i64 x = P.long_off[lid] + lane; x < P.long_off[lid + 1]; x += 32) {
+                const u32 j = P.long_j[x];
+                atomicOr(&bits[j >> 5], 1u << (j & 31));
+                if (F32) acc2[j] = P.long_v2[x];
+                else acc[j] = P.long_v[x];
+            }
+            __syncwarp();
+        }
         const i64 t_base = P.vprp[i];
-        const i64 n_items = lid >= 0 ? P.long_off[lid + 1] - P.long_off[lid]
-                                     : P.vprp[i + 1] - t_base;
+        const i64 n_items = lid >= 0 ? 0 : P.vprp[i + 1] - t_base;
         for (i64 x0 = 0; x0 < n_items; x0 += 32) {
             const i64 xl = x0 + lane;
             const bool inr = xl < n_items;
-            const i64 tl = inr ? (list ? (i64)list[xl] : t_base + xl) : 0;
+            const i64 tl = inr ? t_base + xl : 0;
             u32 kl = 0;
             bool sk = true;
             double al = 0.0, sl = 0.0;
@@ -395,20 +403,28 @@ __global__ void k_long_terms(const u32* vpcol, const double* vpval, const float*
 }
 
 // FP64: the terms summed in k order by one thread (the order of the
-// reference's accumulation, so the result is bit-identical).
-__global__ void k_long_sum64(const double* term, i64 n, double* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// reference's accumulation, so the result is bit-identical).  The block
+// stages chunks of the terms in shared memory so the summing thread reads
+// them at shared-memory latency.
+constexpr int kSumChunk = 4096;
+__global__ void __launch_bounds__(1024) k_long_sum64(const double* term, i64 n, double* out) {
+    __shared__ double sh[kSumChunk];
     double acc = 0.0;
-    i64 t = 0;
-    for (; t + 8 <= n; t += 8) {
-        double v[8];
+    for (i64 c0 = 0; c0 < n; c0 += kSumChunk) {
+        const int m = (int)min((i64)kSumChunk, n - c0);
+        for (int t = threadIdx.x; t < m; t += blockDim.x) sh[t] = term[c0 + t];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (; t + 8 <= m; t += 8) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = term[t + q];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc = __dadd_rn(acc, v[q]);
+                for (int q = 0; q < 8; ++q) acc = __dadd_rn(acc, sh[t + q]);
+            }
+            for (; t < m; ++t) acc = __dadd_rn(acc, sh[t]);
+        }
+        __syncthreads();
     }
-    for (; t < n; ++t) acc = __dadd_rn(acc, term[t]);
-    *out = acc;
+    if (threadIdx.x == 0) *out = acc;
 }
 
 // FP32: float-float sums per lane (terms strided by 32), merged in lane
@@ -433,6 +449,84 @@ __global__ void k_long_sum32(const float2* term, i64 n, float2* out) {
         lo = 0.0f;
         for (int q = 0; q < 32; ++q) add(sh[0][q], sh[1][q]);
         *out = make_float2(hi, lo);
+    }
+}
+
+// Expansion of a long row's shared columns: for each kept k (list of VP
+// positions t, ascending) every H_PV entry (j != i) of column k gives one
+// term; FP64 terms a*D^-1*b with the kernel's unfused operations, FP32
+// terms the TwoProduct pair of the float-pair a*D^-1 and b.
+__global__ void k_esc_count(const u32* list, i64 n, const u32* vpcol, const i64* pvrp, u32* cnt) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n;
+         x += (i64)gridDim.x * blockDim.x) {
+        const u32 k = vpcol[list[x]];
+        cnt[x] = (u32)(pvrp[k + 1] - pvrp[k] - 1);
+    }
+}
+
+__global__ void k_esc_fill(const u32* list, i64 n, const i64* off, u32 row, const u32* vpcol,
+                           const double* vpval, const float* vpval32, const i64* pvrp,
+                           const u32* pvcol, const double* pvval, const float* pvval32,
+                           const double* dinv, bool f32, u32* key, double* term, float2* term2) {
+    for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n;
+         x += (i64)gridDim.x * blockDim.x) {
+        const i64 t = list[x];
+        const u32 k = vpcol[t];
+        const double s = dinv[k];
+        const double a = f32 ? (double)vpval32[t] : vpval[t];
+        const bool need = !(a == 0.0 || s == 0.0);
+        const double asd = __dmul_rn(a, s);
+        const float as = (float)asd;
+        const float as_lo = (float)(asd - (double)as);
+        i64 w = off[x];
+        for (i64 q = pvrp[k]; q < pvrp[k + 1]; ++q) {
+            const u32 j = pvcol[q];
+            if (j == row) continue;
+            key[w] = j;
+            if (!f32) {
+                term[w] = need ? __dmul_rn(asd, pvval[q]) : 0.0;
+            } else {
+                const float b = pvval32[q];
+                const float p = __fmul_rn(as, b);
+                const float pe = fmaf(as, b, -p) + __fmul_rn(as_lo, b);
+                term2[w] = need ? make_float2(p, pe) : make_float2(0.0f, 0.0f);
+            }
+            ++w;
+        }
+    }
+}
+
+__global__ void k_run_heads(const u32* key, i64 n, u32* flag) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        flag[t] = (t == 0 || key[t] != key[t - 1]) ? 1u : 0u;
+}
+
+// One thread per run of equal j: the run's terms (k order, by the stable
+// sort) summed from 0 exactly as the kernel would sum them.
+__global__ void k_run_sums(const u32* key, const u32* perm, const u32* head_pos, i64 nruns,
+                           i64 n, const double* term, const float2* term2, bool f32, u32* oj,
+                           double* ov, float2* ov2) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nruns;
+         r += (i64)gridDim.x * blockDim.x) {
+        const i64 b = head_pos[r], e = r + 1 < nruns ? head_pos[r + 1] : n;
+        oj[r] = key[b];
+        if (!f32) {
+            double acc = 0.0;
+            for (i64 t = b; t < e; ++t) acc = __dadd_rn(acc, term[perm[t]]);
+            ov[r] = acc;
+        } else {
+            float hi = 0.0f, lo = 0.0f;
+            for (i64 t = b; t < e; ++t) {
+                const float2 pp = term2[perm[t]];
+                float s2, er;
+                f_two_sum(hi, pp.x, s2, er);
+                const float c = __fadd_rn(lo, __fadd_rn(er, pp.y));
+                hi = __fadd_rn(s2, c);
+                lo = __fsub_rn(c, __fsub_rn(hi, s2));
+            }
+            ov2[r] = make_float2(hi, lo);
+        }
     }
 }
 
@@ -544,9 +638,21 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
     DNQ_CHECK_LAUNCH();
     DBuf<i64> cap(nv + 1, s), capoff(nv + 1, s);
     DNQ_CUDA(cudaMemsetAsync(cap.p + nv, 0, 8, s));
-    k_cap<<<gs(nv), 256, 0, s>>>(VP.rowptr.p, VP.col.p, PV.rowptr.p, skip.p, VV.rowptr.p, nv,
-                                 cap.p);
-    DNQ_CHECK_LAUNCH();
+    {
+        DBuf<i64> len(std::max<i64>(1, VP.nnz), s), rsum(nv, s);
+        if (VP.nnz) {
+            k_cap_terms<<<gs(VP.nnz), 256, 0, s>>>(VP.col.p, VP.nnz, PV.rowptr.p, skip.p, len.p);
+            DNQ_CHECK_LAUNCH();
+        }
+        size_t tmp = 0;
+        DNQ_CUDA(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, len.p, rsum.p, (int)nv,
+                                                 VP.rowptr.p, VP.rowptr.p + 1, s));
+        DBuf<u8> tb(tmp, s);
+        DNQ_CUDA(cub::DeviceSegmentedReduce::Sum(tb.p, tmp, len.p, rsum.p, (int)nv, VP.rowptr.p,
+                                                 VP.rowptr.p + 1, s));
+        k_cap_finish<<<gs(nv), 256, 0, s>>>(rsum.p, VV.rowptr.p, nv, cap.p);
+        DNQ_CHECK_LAUNCH();
+    }
     scan_excl(cap.p, capoff.p, nv + 1, s);
     i64 captot = 0;
     DNQ_CUDA(cudaMemcpyAsync(&captot, capoff.p + nv, 8, cudaMemcpyDeviceToHost, s));
@@ -592,9 +698,9 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
     const int nl = (int)longs.size();
     DBuf<int> lid;
     DBuf<i64> loff;
-    DBuf<u32> llist, ltouch;
-    DBuf<double> ldiag;
-    DBuf<float2> ldiag2;
+    DBuf<u32> lj, ltouch;
+    DBuf<double> ldiag, lv;
+    DBuf<float2> ldiag2, lv2;
     if (nl) {
         std::vector<int> hid(nv, -1);
         for (int q = 0; q < nl; ++q) hid[longs[q]] = q;
@@ -607,7 +713,9 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
         DNQ_CUDA(cudaMemsetAsync(ldiag.p, 0, 8 * nl, s));
         DNQ_CUDA(cudaMemsetAsync(ldiag2.p, 0, 8 * nl, s));
         std::vector<i64> hoff(nl + 1, 0);
-        std::vector<DBuf<u32>> parts(nl);
+        std::vector<DBuf<u32>> pj(nl);
+        std::vector<DBuf<double>> pv(nl);
+        std::vector<DBuf<float2>> pv2(nl);
         for (int q = 0; q < nl; ++q) {
             const i64 t0 = vrp[longs[q]], t1 = vrp[longs[q] + 1], m = t1 - t0;
             DBuf<double> term;
@@ -620,8 +728,9 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
                                                term2.p, multi.p, ltouch.p + q);
             DNQ_CHECK_LAUNCH();
             if (precision == DNQ_F32) k_long_sum32<<<1, 32, 0, s>>>(term2.p, m, ldiag2.p + q);
-            else k_long_sum64<<<1, 32, 0, s>>>(term.p, m, ldiag.p + q);
+            else k_long_sum64<<<1, 1024, 0, s>>>(term.p, m, ldiag.p + q);
             DNQ_CHECK_LAUNCH();
+            // kept k's whose column holds other rows, in order
             DBuf<u32> idx(m, s), sel(m, s);
             DBuf<i64> nsel(1, s);
             k_iota_u32<<<gs(m), 256, 0, s>>>(idx.p, m, t0);
@@ -633,20 +742,92 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             i64 ns = 0;
             DNQ_CUDA(cudaMemcpyAsync(&ns, nsel.p, 8, cudaMemcpyDeviceToHost, s));
             DNQ_CUDA(cudaStreamSynchronize(s));
-            hoff[q + 1] = hoff[q] + ns;
-            parts[q] = std::move(sel);
+            // expand (j, term), stable sort by j, ordered sum per j
+            i64 ne = 0;
+            DBuf<u32> ecnt(ns + 1, s);
+            DBuf<i64> eoff(ns + 1, s);
+            DNQ_CUDA(cudaMemsetAsync(ecnt.p + ns, 0, 4, s));
+            if (ns) {
+                k_esc_count<<<gs(ns), 256, 0, s>>>(sel.p, ns, VP.col.p, PV.rowptr.p, ecnt.p);
+                DNQ_CHECK_LAUNCH();
+            }
+            scan_excl(ecnt.p, eoff.p, ns + 1, s);
+            DNQ_CUDA(cudaMemcpyAsync(&ne, eoff.p + ns, 8, cudaMemcpyDeviceToHost, s));
+            DNQ_CUDA(cudaStreamSynchronize(s));
+            require(ne < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "long-row expansion exceeds 2^32");
+            DBuf<u32> ekey(std::max<i64>(1, ne), s), skey(std::max<i64>(1, ne), s);
+            DBuf<u32> eperm(std::max<i64>(1, ne), s), sperm(std::max<i64>(1, ne), s);
+            DBuf<double> eterm;
+            DBuf<float2> eterm2;
+            if (precision == DNQ_F32) eterm2.alloc(std::max<i64>(1, ne), s);
+            else eterm.alloc(std::max<i64>(1, ne), s);
+            i64 nruns = 0;
+            if (ne) {
+                k_esc_fill<<<gs(ns), 256, 0, s>>>(sel.p, ns, eoff.p, (u32)longs[q], VP.col.p,
+                                                  VP.val.p, P.vpval32, PV.rowptr.p, PV.col.p,
+                                                  PV.val.p, P.pvval32, dinv.p,
+                                                  precision == DNQ_F32, ekey.p, eterm.p,
+                                                  eterm2.p);
+                DNQ_CHECK_LAUNCH();
+                k_iota_u32<<<gs(ne), 256, 0, s>>>(eperm.p, ne, 0);
+                DNQ_CHECK_LAUNCH();
+                size_t t2 = 0;
+                DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, ekey.p, skey.p, eperm.p,
+                                                         sperm.p, ne, 0, 32, s));
+                DBuf<u8> tb2(t2, s);
+                DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb2.p, t2, ekey.p, skey.p, eperm.p,
+                                                         sperm.p, ne, 0, 32, s));
+                DBuf<u32> head(ne, s), hpos(ne, s);
+                DBuf<i64> nh(1, s);
+                k_run_heads<<<gs(ne), 256, 0, s>>>(skey.p, ne, head.p);
+                DNQ_CHECK_LAUNCH();
+                DBuf<u32> pos(ne, s);
+                k_iota_u32<<<gs(ne), 256, 0, s>>>(pos.p, ne, 0);
+                DNQ_CHECK_LAUNCH();
+                size_t t3 = 0;
+                DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, t3, pos.p, head.p, hpos.p, nh.p, ne, s));
+                DBuf<u8> tb3(t3, s);
+                DNQ_CUDA(cub::DeviceSelect::Flagged(tb3.p, t3, pos.p, head.p, hpos.p, nh.p, ne, s));
+                DNQ_CUDA(cudaMemcpyAsync(&nruns, nh.p, 8, cudaMemcpyDeviceToHost, s));
+                DNQ_CUDA(cudaStreamSynchronize(s));
+                DBuf<u32> oj(nruns, s);
+                DBuf<double> ov;
+                DBuf<float2> ov2;
+                if (precision == DNQ_F32) ov2.alloc(nruns, s);
+                else ov.alloc(nruns, s);
+                k_run_sums<<<gs(nruns), 256, 0, s>>>(skey.p, sperm.p, hpos.p, nruns, ne, eterm.p,
+                                                     eterm2.p, precision == DNQ_F32, oj.p, ov.p,
+                                                     ov2.p);
+                DNQ_CHECK_LAUNCH();
+                pj[q] = std::move(oj);
+                pv[q] = std::move(ov);
+                pv2[q] = std::move(ov2);
+            }
+            hoff[q + 1] = hoff[q] + nruns;
         }
-        llist.alloc(std::max<i64>(1, hoff[nl]), s);
-        for (int q = 0; q < nl; ++q)
-            if (hoff[q + 1] > hoff[q])
-                DNQ_CUDA(cudaMemcpyAsync(llist.p + hoff[q], parts[q].p,
-                                         4 * (hoff[q + 1] - hoff[q]), cudaMemcpyDeviceToDevice, s));
+        const i64 ntot = std::max<i64>(1, hoff[nl]);
+        lj.alloc(ntot, s);
+        if (precision == DNQ_F32) lv2.alloc(ntot, s);
+        else lv.alloc(ntot, s);
+        for (int q = 0; q < nl; ++q) {
+            const i64 m = hoff[q + 1] - hoff[q];
+            if (!m) continue;
+            DNQ_CUDA(cudaMemcpyAsync(lj.p + hoff[q], pj[q].p, 4 * m, cudaMemcpyDeviceToDevice, s));
+            if (precision == DNQ_F32)
+                DNQ_CUDA(cudaMemcpyAsync(lv2.p + hoff[q], pv2[q].p, 8 * m,
+                                         cudaMemcpyDeviceToDevice, s));
+            else
+                DNQ_CUDA(cudaMemcpyAsync(lv.p + hoff[q], pv[q].p, 8 * m,
+                                         cudaMemcpyDeviceToDevice, s));
+        }
         loff.alloc(nl + 1, s);
         DNQ_CUDA(cudaMemcpyAsync(loff.p, hoff.data(), 8 * (nl + 1), cudaMemcpyHostToDevice, s));
         DNQ_CUDA(cudaStreamSynchronize(s));
         P.long_id = lid.p;
         P.long_off = loff.p;
-        P.long_list = llist.p;
+        P.long_j = lj.p;
+        P.long_v = lv.p;
+        P.long_v2 = lv2.p;
         P.long_diag = ldiag.p;
         P.long_diag2 = ldiag2.p;
         P.long_touch = ltouch.p;

@@ -17,10 +17,18 @@ void to_f32(const double* x, i64 n, float* o, cudaStream_t s);
 
 namespace {
 
-__global__ void k_rows_of(const i64* rowptr, i64 nr, u32* rows) {
-    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
-         r += (i64)gridDim.x * blockDim.x)
-        for (i64 k = rowptr[r]; k < rowptr[r + 1]; ++k) rows[k] = (u32)r;
+// Row of every entry: one thread per entry, binary search of the row
+// pointers (rows of any length, no serial walk).
+__global__ void k_rows_of(const i64* rowptr, i64 nr, i64 nnz, u32* rows) {
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < nnz;
+         k += (i64)gridDim.x * blockDim.x) {
+        i64 lo = 0, hi = nr;   // last r with rowptr[r] <= k
+        while (hi - lo > 1) {
+            const i64 mid = (lo + hi) >> 1;
+            if (rowptr[mid] <= k) lo = mid; else hi = mid;
+        }
+        rows[k] = (u32)lo;
+    }
 }
 
 __global__ void k_iota32(u32* p, i64 n) {
@@ -77,7 +85,7 @@ void transpose_csr(const Csr& a, Csr& t, cudaStream_t s) {
         return;
     }
     DBuf<u32> rows(a.nnz, s), perm(a.nnz, s), perm2(a.nnz, s), skey(a.nnz, s);
-    k_rows_of<<<gsz(a.nr), 256, 0, s>>>(a.rowptr.p, a.nr, rows.p);
+    k_rows_of<<<gsz(a.nnz), 256, 0, s>>>(a.rowptr.p, a.nr, a.nnz, rows.p);
     DNQ_CHECK_LAUNCH();
     k_iota32<<<gsz(a.nnz), 256, 0, s>>>(perm.p, a.nnz);
     DNQ_CHECK_LAUNCH();
