@@ -291,6 +291,41 @@ void ensure_sorted(Csr& m, cudaStream_t s) {
     if (!m.sorted) sort_rows(m, s);
 }
 
+namespace {
+__global__ void k_max_rowlen(const i64* rowptr, i64 nr, unsigned long long* out) {
+    unsigned long long m = 0;
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
+         r += (i64)gridDim.x * blockDim.x)
+        m = max(m, (unsigned long long)(rowptr[r + 1] - rowptr[r]));
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// (row << 32 | col) of every entry; the row by binary search of rowptr.
+__global__ void k_row_col_keys(const i64* rowptr, i64 nr, const u32* col, i64 nnz, u64* key,
+                               u32* idx) {
+    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < nnz;
+         k += (i64)gridDim.x * blockDim.x) {
+        i64 lo = 0, hi = nr;
+        while (hi - lo > 1) {
+            const i64 mid = (lo + hi) >> 1;
+            if (rowptr[mid] <= k) lo = mid; else hi = mid;
+        }
+        key[k] = ((u64)lo << 32) | col[k];
+        idx[k] = (u32)k;
+    }
+}
+
+__global__ void k_gather_sorted(const u64* skey, const u32* perm, const double* val, i64 n,
+                                u32* col, double* oval) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        col[t] = (u32)(skey[t] & 0xffffffffull);
+        oval[t] = val[perm[t]];
+    }
+}
+}  // namespace
+
 void sort_rows(Csr& m, cudaStream_t s) {
     m.sorted = true;
     m.val32.release();   // an FP32 copy follows the old order: rebuilt on next use
@@ -299,6 +334,37 @@ void sort_rows(Csr& m, cudaStream_t s) {
             "block has more than 2^31-1 entries for the segmented sort");
     DBuf<u32> col2(m.nnz, s);
     DBuf<double> val2(m.nnz, s);
+    {   // a row longer than 65536 entries would occupy one block of the
+        // segmented sort: sort all entries by (row, column) instead
+        DBuf<unsigned long long> mx(1, s);
+        DNQ_CUDA(cudaMemsetAsync(mx.p, 0, 8, s));
+        k_max_rowlen<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.nr, mx.p);
+        DNQ_CHECK_LAUNCH();
+        unsigned long long longest = 0;
+        DNQ_CUDA(cudaMemcpyAsync(&longest, mx.p, 8, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        if (longest > (1ull << 16)) {
+            DBuf<u64> key(m.nnz, s), skey(m.nnz, s);
+            DBuf<u32> idx(m.nnz, s), perm(m.nnz, s);
+            k_row_col_keys<<<grid_for(m.nnz), 256, 0, s>>>(m.rowptr.p, m.nr, m.col.p, m.nnz,
+                                                          key.p, idx.p);
+            DNQ_CHECK_LAUNCH();
+            int hb = 33;
+            while (hb < 64 && ((u64)1 << (hb - 32)) <= (u64)m.nr) ++hb;
+            size_t tmp = 0;
+            DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, skey.p, idx.p, perm.p,
+                                                     m.nnz, 0, hb, s));
+            DBuf<u8> tb(tmp, s);
+            DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, key.p, skey.p, idx.p, perm.p,
+                                                     m.nnz, 0, hb, s));
+            k_gather_sorted<<<grid_for(m.nnz), 256, 0, s>>>(skey.p, perm.p, m.val.p, m.nnz,
+                                                           col2.p, val2.p);
+            DNQ_CHECK_LAUNCH();
+            m.col = std::move(col2);
+            m.val = std::move(val2);
+            return;
+        }
+    }
     size_t tmp = 0;
     DNQ_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp, m.col.p, col2.p, m.val.p,
                                                  val2.p, (int)m.nnz, (int)m.nr,

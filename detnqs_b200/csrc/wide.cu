@@ -280,6 +280,8 @@ struct WParams {
     // in the order x = 1.., y < x, p = x(x-1)/2 + y)
     const uint4* units;   // {row, first segment, end segment, 0}
     i64 n_units;
+    u32* smask;           // per unit: survivor bits of each 32-single step
+    int smask_words;      // words per unit
     u32* cnt_vv;          // per unit
     u32* cnt_vp;
     const i64* off_vv;    // per unit
@@ -401,11 +403,15 @@ __global__ void __launch_bounds__(kWW * 32) k_wide_build(WParams P) {
                 if (FILL) wvv += 1;
                 else if (lane == 0) nvv = 1;
             }
-            // singles: alpha then beta, holes outer, particles inner
+            // singles: alpha then beta, holes outer, particles inner.  The
+            // count pass records which lanes survive screening, so the fill
+            // pass evaluates only those
             const int nsa = R.na * R.nva, nst = nsa + R.nb * R.nvb;
+            u32* sm = P.smask + (i64)ui * P.smask_words;
             for (int t0 = 0; t0 < nst; t0 += 32) {
                 const int t = t0 + lane;
                 bool valid = t < nst;
+                if (FILL) valid = valid && ((sm[t0 >> 5] >> lane) & 1u);
                 M2 ka = R.a, kb = R.b;
                 double h = 0.0;
                 if (valid) {
@@ -420,6 +426,10 @@ __global__ void __launch_bounds__(kWW * 32) k_wide_build(WParams P) {
                     }
                     h = single2(P.C, R, sp, hh, pp);
                     if (P.dynamic && !(fabs(h * psr) >= P.eps1)) valid = false;   // :190-192
+                }
+                if (!FILL) {
+                    const unsigned keep = __ballot_sync(0xffffffffu, valid && fabs(h) > kElemThresh);
+                    if (lane == 0) sm[t0 >> 5] = keep;
                 }
                 emit(valid, ka, kb, h);
             }
@@ -621,6 +631,14 @@ void wide_build(dnq_ctx_s* ctx, const u64* V_in, i64 n, const double* psi_in, in
             }
         }
         first[n] = (u32)units.size();
+        int max_nst = 0;
+        for (i64 r = 0; r < n; ++r) {
+            int na = 0, nb = 0;
+            na = __builtin_popcountll(hd[4 * r]) + __builtin_popcountll(hd[4 * r + 1]);
+            nb = __builtin_popcountll(hd[4 * r + 2]) + __builtin_popcountll(hd[4 * r + 3]);
+            max_nst = std::max(max_nst, na * (n_orb - na) + nb * (n_orb - nb));
+        }
+        P.smask_words = std::max(1, (max_nst + 31) / 32);
     }
     const i64 nu = (i64)units.size();
     DBuf<uint4> ud(nu, s);
@@ -629,6 +647,8 @@ void wide_build(dnq_ctx_s* ctx, const u64* V_in, i64 n, const double* psi_in, in
     DNQ_CUDA(cudaMemcpyAsync(fd.p, first.data(), 4 * (n + 1), cudaMemcpyHostToDevice, s));
     P.units = ud.p;
     P.n_units = nu;
+    DBuf<u32> smask((size_t)nu * P.smask_words, s);
+    P.smask = smask.p;
 
     DBuf<int> next(1, s);
     DBuf<u32> cvv(nu + 1, s), cvp(nu + 1, s);
