@@ -466,6 +466,7 @@ bool g_force_walk = false;
 extern i64 g_arena_chunk;
 extern i64 g_arena_cap;
 void spmv_set_option(int lanes, int unroll);
+void spmv_set_panels(int mode);
 
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
@@ -843,7 +844,9 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
 
 int dnq_set_option(int option, int64_t value) {
     DNQ_API_BEGIN
-    require(option >= 1 && option <= 5, DNQ_ERR_INVALID, "unknown option");
+    require(option >= 1 && option <= 6, DNQ_ERR_INVALID, "unknown option");
+    if (option == 6)
+        require(value <= 2, DNQ_ERR_INVALID, "panel mode must be 0, 1 or 2");
     require(value >= 0, DNQ_ERR_INVALID, "option value must be >= 0");
     if (option == 4)
         require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
@@ -856,6 +859,7 @@ int dnq_set_option(int option, int64_t value) {
     if (option == 3) g_arena_cap = value;
     if (option == 4) spmv_set_option((int)value, -1);
     if (option == 5) spmv_set_option(-1, (int)value);
+    if (option == 6) spmv_set_panels((int)value);
     DNQ_API_END
 }
 

@@ -22,6 +22,23 @@ struct Csr {
     }
 };
 
+// Column-panel layout of a square FP32 operator block (panel.cu).
+struct Panels {
+    i64 nr = 0, nc = 0, nnz = 0, nblocks = 0, npanels = 0, nseg = 0;
+    int group = 1;             // lanes per row
+    bool ready = false;
+    DBuf<i64> blk_seg;         // per row block: its segments
+    DBuf<u32> seg_panel;       // per segment: panel
+    DBuf<i64> seg_base;        // per segment: first entry
+    DBuf<u16> seg_len;         // per segment: length of each row of the block
+    DBuf<u16> col;             // per entry: column offset in the panel
+    DBuf<float> val;           // per entry: FP32 value
+    size_t bytes() const {
+        return blk_seg.bytes() + seg_panel.bytes() + seg_base.bytes() + seg_len.bytes() +
+               col.bytes() + val.bytes();
+    }
+};
+
 }  // namespace dnq
 
 struct dnq_ham_s {
@@ -29,6 +46,8 @@ struct dnq_ham_s {
     cudaStream_t stream = nullptr;
     dnq::i64 n_v = 0, n_p = 0;
     int words = 1;                    // uint64 words per spin string of V and P
+    dnq::Panels pan;                  // panel layout of the FP32 V block (repeated H.psi)
+    int f32_uses = 0;                 // FP32 H.psi calls so far
     dnq::Csr vv, vp;
     dnq::Csr pv;                      // transpose of vp, built on first use
     bool pv_ready = false;
@@ -42,7 +61,8 @@ struct dnq_ham_s {
     // [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total
     double t_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     size_t bytes() const {
-        return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + diag_op.bytes() + x32.bytes() + dets_p.bytes();
+        return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + diag_op.bytes() + x32.bytes() +
+               dets_p.bytes() + pan.bytes();
     }
 };
 
@@ -63,6 +83,10 @@ struct SpmvDesc {
     double* y;
     i64 nr, nnz;
 };
+// Panel layout of a square block from its FP32 values; y = M x with it.
+void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s);
+void spmv_panels(const Panels& P, const float* x32, const double* diag, const double* x,
+                 double* y, int device, cudaStream_t s);
 // Lanes per row and slots per lane the H.psi kernels use for m.
 void spmv_shape(const Csr& m, int& G, int& U);
 // One launch over nd descriptors (device array) sharing (G, U, precision).

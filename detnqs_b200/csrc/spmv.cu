@@ -338,6 +338,12 @@ void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, i
 
 }  // namespace
 
+// When the FP32 V block gets its panel layout: 0 never, 1 from its second
+// FP32 H.psi (repeated use pays for the reordering), 2 from the first.
+int g_spmv_panels = 1;
+
+void spmv_set_panels(int mode) { g_spmv_panels = mode; }
+
 void spmv_set_option(int lanes, int unroll) {
     if (lanes >= 0) g_spmv_lanes = lanes;
     if (unroll >= 0) g_spmv_unroll = unroll;
@@ -460,9 +466,24 @@ void ensure_f32_all(Csr& m, cudaStream_t s) {
 
 // Prepare the FP32 operator buffers of the V block.
 void ensure_f32(dnq_ham_s* h, cudaStream_t s) {
-    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
+    bool fresh = false;
+    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v) {
         make_f32(h->vv, s, &h->diag_op);
+        h->pan.ready = false;
+        fresh = true;
+    }
     if ((i64)h->x32.n < h->n_v) h->x32.alloc(h->n_v, s);
+    ++h->f32_uses;
+    const bool want = g_spmv_panels == 2 || (g_spmv_panels == 1 && h->f32_uses >= 2);
+    if (want && (!h->pan.ready || fresh) && h->vv.nr == h->vv.nc)
+        build_panels(h->vv, h->vv.val32.p, h->pan, s);
+    if (!want) h->pan.ready = false;
+}
+
+// FP32 V-block operator of a handle: the panel layout when present.
+void spmv_vv_f32(dnq_ham_s* h, const double* x, double* y, cudaStream_t s) {
+    if (h->pan.ready) spmv_panels(h->pan, h->x32.p, h->diag_op.p, x, y, h->device, s);
+    else spmv_block(h, h->vv, x, y, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
 }
 
 }  // namespace dnq
@@ -487,7 +508,7 @@ int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision, void* s
     if (precision == DNQ_F32) {
         ensure_f32(h, s);
         to_f32(xd.p, n, h->x32.p, s);
-        spmv_block(h, h->vv, xd.p, yd, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
+        spmv_vv_f32(h, xd.p, yd, s);
     } else {
         spmv_block(h, h->vv, xd.p, yd, nullptr, DNQ_F64, s, nullptr, nullptr);
     }
@@ -551,7 +572,7 @@ int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc, double* out
     if (precision == DNQ_F32) {
         ensure_f32(h, s);
         to_f32(xd.p, n, h->x32.p, s);
-        spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
+        spmv_vv_f32(h, xd.p, y.p, s);
     } else {
         spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F64, s, nullptr, nullptr);
     }

@@ -37,6 +37,7 @@ OPT_ARENA_CHUNK = 2
 OPT_ARENA_CAP = 3
 OPT_SPMV_LANES = 4
 OPT_SPMV_UNROLL = 5
+OPT_SPMV_PANELS = 6
 REQ_BUILD = 0
 REQ_ELOC = 1
 

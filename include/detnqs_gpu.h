@@ -123,9 +123,12 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          average row length);
  *   DNQ_OPT_SPMV_UNROLL n: 4-entry slots each lane keeps in flight, 0/1/2/4
  *                          (0 = by the average row length).  Results do
- *                          not depend on it. */
+ *                          not depend on it;
+ *   DNQ_OPT_SPMV_PANELS n: column-panel layout of the FP32 V block (x staged
+ *                          in shared memory): 0 never, 1 from a handle's
+ *                          second FP32 H.psi (default), 2 from the first. */
 enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
-       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5 };
+       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */
