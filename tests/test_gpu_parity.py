@@ -405,6 +405,7 @@ def test_spmv_every_lane_and_slot_count(core):
     x = S.normalized_psi(len(V), 5)
     ref = H.to_scipy(0).dot(x)
     scale = np.abs(ref).max()
+    N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 0))   # the CSR kernels only
     try:
         for G in (4, 8, 16, 32):
             N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, G))
@@ -422,6 +423,7 @@ def test_spmv_every_lane_and_slot_count(core):
     finally:
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 0))
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, 0))
+        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 1))
     H.close()
 
 
