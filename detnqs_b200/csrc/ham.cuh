@@ -33,9 +33,11 @@ struct Panels {
     DBuf<u16> seg_len;         // per segment: length of each row of the block
     DBuf<u16> col;             // per entry: column offset in the panel
     DBuf<float> val;           // per entry: FP32 value
+    DBuf<float> part;          // per panel group and row: Dot2 partial (2 floats)
+    DBuf<u8> flag;             // per (row block, panel group): partial written
     size_t bytes() const {
         return blk_seg.bytes() + seg_panel.bytes() + seg_base.bytes() + seg_len.bytes() +
-               col.bytes() + val.bytes();
+               col.bytes() + val.bytes() + part.bytes() + flag.bytes();
     }
 };
 

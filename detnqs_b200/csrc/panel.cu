@@ -154,27 +154,51 @@ struct PanelView {
     const float* val;
 };
 
+constexpr int kPGS = 8;   // panels per task: a CTA sums one group of panels of one row block
+
+// One CTA per (row block, group of kPGS panels): the group's segments of the
+// block are summed into per-row Dot2 pairs, written as the group's partial
+// (flag[task] says whether the group had any segment).
 template <int G>
-__global__ void __launch_bounds__(kPT) k_spmv_panel(PanelView P, const float* __restrict__ x32,
-                                                    const double* __restrict__ diag,
-                                                    const double* __restrict__ x,
-                                                    double* __restrict__ y) {
+__global__ void __launch_bounds__(kPT) k_spmv_panel(PanelView P, i64 ngroups_p,
+                                                    const float* __restrict__ x32,
+                                                    float2* __restrict__ part,
+                                                    u8* __restrict__ flag) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* xs = reinterpret_cast<float*>(smem);                         // kPW
     float2* acc = reinterpret_cast<float2*>(smem + kPW * 4);            // kRB
     u32* offs = reinterpret_cast<u32*>(smem + kPW * 4 + kRB * 8);       // kRB + 1
     using Scan = cub::BlockScan<u32, kPT>;
     __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ i64 seg_lo, seg_hi;
     const int tid = threadIdx.x, lane = tid & 31;
     const int sub = lane & (G - 1);
     const int group = tid / G, ngroups = kPT / G;
-    for (i64 b = blockIdx.x; b < P.nblocks; b += gridDim.x) {
+    const i64 ntasks = P.nblocks * ngroups_p;
+    for (i64 task = blockIdx.x; task < ntasks; task += gridDim.x) {
+        const i64 b = task / ngroups_p, pg = task % ngroups_p;
         const i64 row0 = b * kRB;
         const int nrow = (int)min((i64)kRB, P.nr - row0);
+        if (tid == 0) {   // segments of block b with panel in [pg*kPGS, (pg+1)*kPGS)
+            const i64 s0 = P.blk_seg[b], s1 = P.blk_seg[b + 1];
+            i64 lo = s0, hi = s1;
+            while (lo < hi) {
+                const i64 mid = (lo + hi) >> 1;
+                if ((i64)P.seg_panel[mid] < pg * kPGS) lo = mid + 1; else hi = mid;
+            }
+            seg_lo = lo;
+            hi = s1;
+            while (lo < hi) {
+                const i64 mid = (lo + hi) >> 1;
+                if ((i64)P.seg_panel[mid] < (pg + 1) * kPGS) lo = mid + 1; else hi = mid;
+            }
+            seg_hi = lo;
+        }
         for (int r = tid; r < kRB; r += kPT) acc[r] = make_float2(0.0f, 0.0f);
-        const i64 s0 = P.blk_seg[b], s1 = P.blk_seg[b + 1];
-        for (i64 sg = s0; sg < s1; ++sg) {
-            __syncthreads();   // previous segment done with xs / offs
+        __syncthreads();
+        const i64 g0 = seg_lo, g1 = seg_hi;
+        if (tid == 0) flag[task] = g1 > g0 ? 1 : 0;
+        for (i64 sg = g0; sg < g1; ++sg) {
             const i64 c0 = (i64)P.seg_panel[sg] << kPShift;
             const int ncol = (int)min((i64)kPW, P.nc - c0);
             const float* xp = x32 + c0;
@@ -216,32 +240,45 @@ __global__ void __launch_bounds__(kPT) k_spmv_panel(PanelView P, const float* __
                     acc[r] = make_float2(t.s, t.c);
                 }
             }
+            __syncthreads();   // xs / offs free for the next segment
         }
+        if (g1 > g0)
+            for (int r = tid; r < nrow; r += kPT) part[pg * P.nr + row0 + r] = acc[r];
         __syncthreads();
-        for (int r = tid; r < nrow; r += kPT) {
-            const i64 g = row0 + r;
-            double v = (double)acc[r].x + (double)acc[r].y;
-            if (diag) v += diag[g] * x[g];
-            y[g] = v;
-        }
-        __syncthreads();
+    }
+}
+
+// y = merge of the groups' partials in group order + diag * x (FP64).
+__global__ void k_panel_finish(const float2* part, const u8* flag, i64 nr, i64 ngroups_p,
+                               const double* diag, const double* x, double* y) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
+         r += (i64)gridDim.x * blockDim.x) {
+        const i64 b = r / kRB;
+        Pair32 a;
+        for (i64 pg = 0; pg < ngroups_p; ++pg)
+            if (flag[b * ngroups_p + pg]) {
+                const float2 p = part[pg * nr + r];
+                a.merge(p.x, p.y);
+            }
+        double v = (double)a.s + (double)a.c;
+        if (diag) v += diag[r] * x[r];
+        y[r] = v;
     }
 }
 
 size_t panel_smem() { return (size_t)kPW * 4 + (size_t)kRB * 8 + (size_t)(kRB + 1) * 4; }
 
 template <int G>
-void launch_panel(const PanelView& v, const float* x32, const double* diag, const double* x,
-                  double* y, int device, cudaStream_t s) {
+void launch_panel(const PanelView& v, i64 ngroups_p, const float* x32, float2* part, u8* flag,
+                  int device, cudaStream_t s) {
     auto kern = k_spmv_panel<G>;
     const size_t sm = panel_smem();
-    static thread_local int configured = -1;
-    (void)configured;
     DNQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
     DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, sm));
-    const i64 grid = std::min<i64>(v.nblocks, (i64)std::max(1, per_sm) * sm_count(device));
-    kern<<<(unsigned)std::max<i64>(1, grid), kPT, sm, s>>>(v, x32, diag, x, y);
+    const i64 ntasks = v.nblocks * ngroups_p;
+    const i64 grid = std::min<i64>(ntasks, (i64)std::max(1, per_sm) * sm_count(device) * 8);
+    kern<<<(unsigned)std::max<i64>(1, grid), kPT, sm, s>>>(v, ngroups_p, x32, part, flag);
     DNQ_CHECK_LAUNCH();
 }
 
@@ -266,6 +303,9 @@ void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s) {
         P.seg_panel.alloc(1, s);
         P.seg_base.alloc(1, s);
         P.seg_len.alloc(1, s);
+        P.part.alloc(2 * std::max<i64>(1, m.nr), s);
+        P.flag.alloc(std::max<i64>(1, P.nblocks), s);
+        DNQ_CUDA(cudaMemsetAsync(P.flag.p, 0, std::max<i64>(1, P.nblocks), s));
         P.ready = true;
         return;
     }
@@ -330,6 +370,11 @@ void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s) {
     // lanes per row by the average entries of a (row, segment)
     const double avg = (double)n / ((double)nseg * kRB);
     P.group = avg >= 48 ? 32 : avg >= 16 ? 8 : avg >= 6 ? 4 : 1;
+    {
+        const i64 ngp = (npanels + kPGS - 1) / kPGS;
+        P.part.alloc((size_t)ngp * m.nr * 2, s);
+        P.flag.alloc((size_t)P.nblocks * ngp, s);
+    }
     DNQ_CUDA(cudaStreamSynchronize(s));
     P.ready = true;
 }
@@ -340,12 +385,16 @@ void spmv_panels(const Panels& P, const float* x32, const double* diag, const do
     if (P.nr == 0) return;
     PanelView v{P.nr, P.nc, P.nblocks, P.blk_seg.p, P.seg_panel.p, P.seg_base.p, P.seg_len.p,
                 P.col.p, P.val.p};
+    const i64 ngp = (P.npanels + kPGS - 1) / kPGS;
+    float2* part = reinterpret_cast<float2*>(P.part.p);
     switch (P.group) {
-        case 32: launch_panel<32>(v, x32, diag, x, y, device, s); break;
-        case 8: launch_panel<8>(v, x32, diag, x, y, device, s); break;
-        case 4: launch_panel<4>(v, x32, diag, x, y, device, s); break;
-        default: launch_panel<1>(v, x32, diag, x, y, device, s); break;
+        case 32: launch_panel<32>(v, ngp, x32, part, P.flag.p, device, s); break;
+        case 8: launch_panel<8>(v, ngp, x32, part, P.flag.p, device, s); break;
+        case 4: launch_panel<4>(v, ngp, x32, part, P.flag.p, device, s); break;
+        default: launch_panel<1>(v, ngp, x32, part, P.flag.p, device, s); break;
     }
+    k_panel_finish<<<pg(P.nr), 256, 0, s>>>(part, P.flag.p, P.nr, ngp, diag, x, y);
+    DNQ_CHECK_LAUNCH();
 }
 
 }  // namespace dnq
