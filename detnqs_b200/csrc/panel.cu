@@ -159,8 +159,8 @@ constexpr int kPGS = 8;   // panels per task: a CTA sums one group of panels of 
 // One CTA per (row block, group of kPGS panels): the group's segments of the
 // block are summed into per-row Dot2 pairs, written as the group's partial
 // (flag[task] says whether the group had any segment).
-template <int G>
-__global__ void __launch_bounds__(kPT) k_spmv_panel(PanelView P, i64 ngroups_p,
+template <int G, int D, int RR>
+__global__ void __launch_bounds__(kPT, 2) k_spmv_panel(PanelView P, i64 ngroups_p,
                                                     const float* __restrict__ x32,
                                                     float2* __restrict__ part,
                                                     u8* __restrict__ flag) {
@@ -220,24 +220,62 @@ __global__ void __launch_bounds__(kPT) k_spmv_panel(PanelView P, i64 ngroups_p,
             __syncthreads();
             const u16* cp = P.col + P.seg_base[sg];
             const float* vp = P.val + P.seg_base[sg];
-            // rows handed out in rounds of ngroups so every lane of a warp runs
-            // the same number of rounds (the group shuffles need all lanes)
-            for (int r0 = 0; r0 < nrow; r0 += ngroups) {
-                const int r = r0 + group;
-                const bool on = r < nrow;
-                const u32 b0 = on ? offs[r] : 0u, e0 = on ? offs[r + 1] : 0u;
-                Pair32 a;
-                for (u32 k = b0 + sub; k < e0; k += G) a.add_prod(__ldcs(vp + k), xs[__ldcs(cp + k)]);
+            // rows handed out in rounds of ngroups (every lane of a warp runs
+            // the same rounds: the group shuffles need all lanes).  RR rounds
+            // at a time, D slots per lane each, are loaded before any is
+            // used, so one memory latency covers RR*D entries per lane.
+            for (int r0 = 0; r0 < nrow; r0 += ngroups * RR) {
+                u32 bb[RR], ee[RR];
 #pragma unroll
-                for (int o = G / 2; o; o >>= 1)
-                    a.merge(__shfl_xor_sync(0xffffffffu, a.s, o, G),
-                            __shfl_xor_sync(0xffffffffu, a.c, o, G));
-                if (sub == 0 && e0 > b0) {
-                    Pair32 t;
-                    t.s = acc[r].x;
-                    t.c = acc[r].y;
-                    t.merge(a.s, a.c);
-                    acc[r] = make_float2(t.s, t.c);
+                for (int q = 0; q < RR; ++q) {
+                    const int r = r0 + q * ngroups + group;
+                    const bool on = r < nrow;
+                    bb[q] = on ? offs[r] : 0u;
+                    ee[q] = on ? offs[r + 1] : 0u;
+                }
+                Pair32 a[RR];
+                u32 kb[RR];
+#pragma unroll
+                for (int q = 0; q < RR; ++q) kb[q] = bb[q] + sub;
+                bool more = true;
+                while (more) {
+                    float v[RR][D];
+                    u32 c[RR][D];
+#pragma unroll
+                    for (int q = 0; q < RR; ++q)
+#pragma unroll
+                        for (int d = 0; d < D; ++d) {
+                            const u32 k = kb[q] + (u32)(d * G);
+                            const bool ok = k < ee[q];
+                            v[q][d] = ok ? __ldcs(vp + k) : 0.0f;
+                            c[q][d] = ok ? (u32)__ldcs(cp + k) : 0u;
+                        }
+                    more = false;
+#pragma unroll
+                    for (int q = 0; q < RR; ++q) {
+#pragma unroll
+                        for (int d = 0; d < D; ++d)
+                            if (kb[q] + (u32)(d * G) < ee[q]) a[q].add_prod(v[q][d], xs[c[q][d]]);
+                        kb[q] += (u32)(D * G);
+                        more = more || kb[q] < ee[q];
+                    }
+                    more = __any_sync(0xffffffffu, more);
+                }
+#pragma unroll
+                for (int q = 0; q < RR; ++q) {
+                    Pair32 t = a[q];
+#pragma unroll
+                    for (int o = G / 2; o; o >>= 1)
+                        t.merge(__shfl_xor_sync(0xffffffffu, t.s, o, G),
+                                __shfl_xor_sync(0xffffffffu, t.c, o, G));
+                    const int r = r0 + q * ngroups + group;
+                    if (sub == 0 && r < nrow && ee[q] > bb[q]) {
+                        Pair32 u;
+                        u.s = acc[r].x;
+                        u.c = acc[r].y;
+                        u.merge(t.s, t.c);
+                        acc[r] = make_float2(u.s, u.c);
+                    }
                 }
             }
             __syncthreads();   // xs / offs free for the next segment
@@ -268,10 +306,10 @@ __global__ void k_panel_finish(const float2* part, const u8* flag, i64 nr, i64 n
 
 size_t panel_smem() { return (size_t)kPW * 4 + (size_t)kRB * 8 + (size_t)(kRB + 1) * 4; }
 
-template <int G>
+template <int G, int D, int RR>
 void launch_panel(const PanelView& v, i64 ngroups_p, const float* x32, float2* part, u8* flag,
                   int device, cudaStream_t s) {
-    auto kern = k_spmv_panel<G>;
+    auto kern = k_spmv_panel<G, D, RR>;
     const size_t sm = panel_smem();
     DNQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     int per_sm = 0;
@@ -388,10 +426,10 @@ void spmv_panels(const Panels& P, const float* x32, const double* diag, const do
     const i64 ngp = (P.npanels + kPGS - 1) / kPGS;
     float2* part = reinterpret_cast<float2*>(P.part.p);
     switch (P.group) {
-        case 32: launch_panel<32>(v, ngp, x32, part, P.flag.p, device, s); break;
-        case 8: launch_panel<8>(v, ngp, x32, part, P.flag.p, device, s); break;
-        case 4: launch_panel<4>(v, ngp, x32, part, P.flag.p, device, s); break;
-        default: launch_panel<1>(v, ngp, x32, part, P.flag.p, device, s); break;
+        case 32: launch_panel<32, 4, 1>(v, ngp, x32, part, P.flag.p, device, s); break;
+        case 8: launch_panel<8, 2, 2>(v, ngp, x32, part, P.flag.p, device, s); break;
+        case 4: launch_panel<4, 2, 4>(v, ngp, x32, part, P.flag.p, device, s); break;
+        default: launch_panel<1, 4, 4>(v, ngp, x32, part, P.flag.p, device, s); break;
     }
     k_panel_finish<<<pg(P.nr), 256, 0, s>>>(part, P.flag.p, P.nr, ngp, diag, x, y);
     DNQ_CHECK_LAUNCH();
