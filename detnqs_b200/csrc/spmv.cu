@@ -338,9 +338,11 @@ void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, i
 
 }  // namespace
 
-// When the FP32 V block gets its panel layout: 0 never, 1 from its second
-// FP32 H.psi (repeated use pays for the reordering), 2 from the first.
-int g_spmv_panels = 1;
+// When the FP32 V block gets its panel layout: 0 never (default), 1 from
+// its second FP32 H.psi, 2 from the first.  The layout is correct but, on
+// the heat-bath spaces measured, slower than the CSR kernel: rows of very
+// different lengths share each block's barriers (see panel.cu).
+int g_spmv_panels = 0;
 
 void spmv_set_panels(int mode) { g_spmv_panels = mode; }
 

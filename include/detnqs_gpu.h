@@ -125,8 +125,8 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          (0 = by the average row length).  Results do
  *                          not depend on it;
  *   DNQ_OPT_SPMV_PANELS n: column-panel layout of the FP32 V block (x staged
- *                          in shared memory): 0 never, 1 from a handle's
- *                          second FP32 H.psi (default), 2 from the first. */
+ *                          in shared memory): 0 never (default), 1 from a
+ *                          handle's second FP32 H.psi, 2 from the first. */
 enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
        DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6 };
 int dnq_set_option(int option, int64_t value);

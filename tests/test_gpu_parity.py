@@ -405,7 +405,6 @@ def test_spmv_every_lane_and_slot_count(core):
     x = S.normalized_psi(len(V), 5)
     ref = H.to_scipy(0).dot(x)
     scale = np.abs(ref).max()
-    N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 0))   # the CSR kernels only
     try:
         for G in (4, 8, 16, 32):
             N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, G))
@@ -423,7 +422,6 @@ def test_spmv_every_lane_and_slot_count(core):
     finally:
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 0))
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, 0))
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 1))
     H.close()
 
 
@@ -450,7 +448,7 @@ def test_fp32_panel_layout_matches_csr_and_scipy(core):
         y_pan2 = B.spmv(x, precision=N.F32)
         num, den = B.local_energy(x, precision=N.F32)
     finally:
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 1))
+        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 0))
     ref = A.to_scipy(0).dot(x)
     scale = np.abs(ref).max()
     np.testing.assert_array_equal(y_pan, y_pan2)
