@@ -893,16 +893,16 @@ DF_WORKLOAD = ("100 orbitals, 20a/20b, K=200, two-word determinants; S = 1e5 hea
                "e_ref = <psi|H_SS|psi>, sigma regularisation 0.1 Ha, FP64 and FP32 values")
 
 
-def downfold_workload(rank: int):
+def downfold_workload(rank: int, n_s: int = DF_S):
     from detnqs_b200 import synthetic as S
     seed = 4004 + 10 * rank
     sysm = S.make_system(DF_N, DF_NE, DF_NE, DF_K, seed)
     os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, f"df_{DF_N}_{DF_S}_{seed}.npy")
+    path = os.path.join(CACHE, f"df_{DF_N}_{n_s}_{seed}.npy")
     if os.path.exists(path):
         V = np.load(path)
     else:
-        V = S.heat_bath_sample_wide(sysm, DF_S, seed + 1, max_level=4)
+        V = S.heat_bath_sample_wide(sysm, n_s, seed + 1, max_level=4)
         np.save(path, V)
     rng = np.random.default_rng(seed + 2)
     psi = DF_TAIL * rng.normal(size=len(V))
@@ -935,7 +935,7 @@ def cpu_wide_rows(sysm, V, psi, target_s: float = 15.0, seed: int = 5):
 
 
 def run_downfold(args, rank: int, world: int):
-    sysm, V, psi = downfold_workload(rank)
+    sysm, V, psi = downfold_workload(rank, args.df_dets)
     import torch
     from detnqs_b200 import eigen as E
     from detnqs_b200 import native
@@ -1174,6 +1174,8 @@ def main():
     ap.add_argument("--n-dets", type=int, default=N_DETS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--df-dets", type=int, default=DF_S,
+                    help="size of S for --workload downfold (a smaller S for profiling)")
     ap.add_argument("--serve-slots", type=int, default=4,
                     help="build worker streams of the served path")
     ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold"],
