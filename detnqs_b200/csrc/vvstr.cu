@@ -29,6 +29,11 @@
 
 namespace dnq {
 
+// Part C walk over the short groups: 0 = packed across the groups of a
+// round (default), 1 = one group at a time.  Both give the same entries in
+// the same order.
+int g_partc_groupwalk = 0;
+
 namespace {
 
 constexpr int kWS = 8;               // warps per block
@@ -56,8 +61,16 @@ struct StrMapView {
 struct StrIndex {
     DBuf<u64> other;     // sorted companion string (alpha for beta groups, ...)
     DBuf<u32> idx;       // original position in V
+    DBuf<u32> gid;       // group number of every sorted position
+    DBuf<u32> gstart;    // first sorted position of every group
+    i64 ngroups = 0;
     DBuf<ulonglong2> slots;
     u64 mask = 0;
+    // Presence rows (alpha index only): one bit per beta group for every
+    // alpha group longer than pres_min; prow[group] = its row or ~0u.
+    DBuf<u32> prow, pres;
+    u32 pres_words = 0;
+    u32 pres_min = 0xffffffffu;
     StrMapView view() const { return StrMapView{slots.p, mask}; }
 };
 
@@ -85,11 +98,15 @@ __global__ void k_split_sorted(const ulonglong2* k, i64 n, u64* other, unsigned*
     }
 }
 
-// Start position of every group (gid = exclusive scan of the head flags).
-__global__ void k_group_starts(const unsigned* head, const u32* gid, i64 n, u32* gstart) {
+// Start position of every group; gid arrives as the inclusive scan of the
+// head flags and leaves as the group number of every position.
+__global__ void k_group_starts(const unsigned* head, u32* gid, i64 n, u32* gstart) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
-         t += (i64)gridDim.x * blockDim.x)
-        if (head[t]) gstart[gid[t]] = (u32)t;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 g = gid[t] - 1;
+        gid[t] = g;
+        if (head[t]) gstart[g] = (u32)t;
+    }
 }
 
 // Insert one slot per group: (string, start << 32 | len).
@@ -121,6 +138,13 @@ int gsz(i64 n) {
 
 // major 0: groups by alpha (companion beta); major 1: groups by beta.
 void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s) {
+    if (n == 0) {   // no groups: an empty table
+        X.ngroups = 0;
+        X.mask = 1023;
+        X.slots.alloc(1024, s);
+        DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, 1024 * sizeof(ulonglong2), s));
+        return;
+    }
     DBuf<ulonglong2> k(n, s), ks(n, s);
     DBuf<u32> id(n, s);
     X.idx.alloc(n, s);
@@ -136,18 +160,21 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s
     DBuf<unsigned> head(n, s);
     k_split_sorted<<<gsz(n), 256, 0, s>>>(ks.p, n, X.other.p, head.p);
     DNQ_CHECK_LAUNCH();
-    DBuf<u32> gid(n + 1, s), gstart(n, s);
+    X.gid.alloc(n, s);
+    X.gstart.alloc(n, s);
+    DBuf<u32>& gid = X.gid;
+    DBuf<u32>& gstart = X.gstart;
     {
         size_t t2 = 0;
-        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, head.p, gid.p, n, s));
+        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t2, head.p, gid.p, n, s));
         DBuf<u8> tb2(t2, s);
-        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb2.p, t2, head.p, gid.p, n, s));
+        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb2.p, t2, head.p, gid.p, n, s));
     }
-    u32 last_gid = 0, last_head = 0;
+    u32 last_gid = 0;
     DNQ_CUDA(cudaMemcpyAsync(&last_gid, gid.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
-    DNQ_CUDA(cudaMemcpyAsync(&last_head, head.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
-    const i64 ngroups = (i64)last_gid + last_head;
+    const i64 ngroups = (i64)last_gid;
+    X.ngroups = ngroups;
     k_group_starts<<<gsz(n), 256, 0, s>>>(head.p, gid.p, n, gstart.p);
     DNQ_CHECK_LAUNCH();
     u64 cap = 1024;
@@ -157,6 +184,80 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s
     DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, cap * sizeof(ulonglong2), s));
     k_group_insert<<<gsz(ngroups), 256, 0, s>>>(ks.p, gstart.p, ngroups, n, X.slots.p, X.mask);
     DNQ_CHECK_LAUNCH();
+}
+
+constexpr u32 kPresMin = 128;                    // presence rows for alpha groups longer than this
+constexpr i64 kPresBytes = 256ll << 20;          // cap on the presence rows of one index
+
+__global__ void k_long_groups(const u32* gstart, i64 ngroups, i64 n, u32 thr, u32* flag,
+                              unsigned long long* count) {
+    u32 c = 0;
+    for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < ngroups;
+         g += (i64)gridDim.x * blockDim.x) {
+        const i64 e = g + 1 < ngroups ? (i64)gstart[g + 1] : n;
+        const u32 f = (e - (i64)gstart[g]) > (i64)thr ? 1u : 0u;
+        if (flag) flag[g] = f;
+        c += f;
+    }
+    if (count && c) atomicAdd(count, (unsigned long long)c);
+}
+
+__global__ void k_prow(const u32* flag, const u32* rank, i64 ngroups, u32* prow) {
+    for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < ngroups;
+         g += (i64)gridDim.x * blockDim.x)
+        prow[g] = flag[g] ? rank[g] : 0xffffffffu;
+}
+
+// One bit per member of every long alpha group: its beta string's group.
+__global__ void k_pres_fill(const u32* a_gid, const u64* a_other, const u32* prow, i64 n,
+                            StrMapView bmap, const u32* b_gid, u32 words, u32* pres) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 r = prow[a_gid[t]];
+        if (r == 0xffffffffu) continue;
+        u32 st = 0, ln = 0;
+        if (!bmap.find(a_other[t], st, ln)) continue;   // every member's beta is indexed
+        const u32 bid = b_gid[st];
+        atomicOr(&pres[(i64)r * words + (bid >> 5)], 1u << (bid & 31));
+    }
+}
+
+// Presence rows of the alpha index A over the beta groups of B.  The
+// threshold starts at kPresMin and doubles until the rows fit kPresBytes.
+void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
+    if (n == 0 || A.ngroups == 0) return;
+    const u32 words = (u32)((B.ngroups + 31) / 32);
+    DBuf<unsigned long long> cnt(1, s);
+    u32 thr = kPresMin;
+    unsigned long long nl = 0;
+    for (;;) {
+        DNQ_CUDA(cudaMemsetAsync(cnt.p, 0, 8, s));
+        k_long_groups<<<gsz(A.ngroups), 256, 0, s>>>(A.gstart.p, A.ngroups, n, thr, nullptr,
+                                                     cnt.p);
+        DNQ_CHECK_LAUNCH();
+        DNQ_CUDA(cudaMemcpyAsync(&nl, cnt.p, 8, cudaMemcpyDeviceToHost, s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        if ((i64)nl * words * 4 <= kPresBytes || (i64)thr >= n) break;
+        thr *= 2;
+    }
+    if (nl == 0 || (i64)nl * words * 4 > kPresBytes) return;
+    DBuf<u32> flag(A.ngroups, s), rank(A.ngroups, s);
+    k_long_groups<<<gsz(A.ngroups), 256, 0, s>>>(A.gstart.p, A.ngroups, n, thr, flag.p, nullptr);
+    DNQ_CHECK_LAUNCH();
+    size_t tmp = 0;
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag.p, rank.p, A.ngroups, s));
+    DBuf<u8> tb(tmp, s);
+    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, flag.p, rank.p, A.ngroups, s));
+    A.prow.alloc(A.ngroups, s);
+    k_prow<<<gsz(A.ngroups), 256, 0, s>>>(flag.p, rank.p, A.ngroups, A.prow.p);
+    DNQ_CHECK_LAUNCH();
+    A.pres.alloc((size_t)nl * words, s);
+    DNQ_CUDA(cudaMemsetAsync(A.pres.p, 0, (size_t)nl * words * 4, s));
+    k_pres_fill<<<gsz(n), 256, 0, s>>>(A.gid.p, A.other.p, A.prow.p, n, B.view(), B.gid.p,
+                                       words, A.pres.p);
+    DNQ_CHECK_LAUNCH();
+    A.pres_words = words;
+    A.pres_min = thr;
 }
 
 __device__ __forceinline__ i64 tri2(i64 p, i64 q) {
@@ -183,6 +284,15 @@ struct VVParams {
     double cut;             // doubles: keep w >= cut (and > 1e-15)
     const double* psi;
     u32 big_group;          // part C: binary search for groups longer than this
+    int c_groupwalk;        // part C: short groups one at a time instead of packed
+    // part C presence rows: alpha groups longer than pres_min test the beta
+    // singles of the row against one bit per beta group
+    const u32* a_gid;       // group number of every alpha-sorted position
+    const u32* a_prow;      // presence row of every alpha group (~0u: none)
+    const u32* b_gid;       // group number of every beta-sorted position
+    const u32* pres;
+    u32 pres_words;
+    u32 pres_min;
 };
 
 // Where rows are written.  Single pass: rows appended to warp-private
@@ -335,10 +445,14 @@ __device__ __forceinline__ bool keep_single(const VVParams& P, double psr, doubl
 }
 
 // Per-warp shared state.
+constexpr int kBS = 512;   // beta singles of one row kept for the presence rows
+
 struct WarpShared {
-    u32 start[32], len[32];
+    u32 start[32], pre[32];    // part C: group starts, exclusive prefix of lengths
     u8 h[32], p[32];
     u8 occa[64], vira[64], occb[64], virb[64];
+    u32 bs_id[kBS];            // beta group of each indexed beta single of the row
+    u16 bs_hp[kBS];            // its excitation, hole | particle << 8
 };
 
 __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, u64 all) {
@@ -351,6 +465,57 @@ __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, u64 all)
         for (u64 m = b; m; m &= m - 1) S.occb[k++] = (u8)(__ffsll(m) - 1);
         k = 0;
         for (u64 m = ~b & all; m; m &= m - 1) S.virb[k++] = (u8)(__ffsll(m) - 1);
+    }
+    __syncwarp();
+}
+
+// Part C over the short groups of one round of 32 alpha singles, packed:
+// the members of all of them are numbered in group order and each step
+// tests 32 consecutive members; a lane finds its member's group by a
+// five-step search of the exclusive prefix of the group lengths.
+template <class Out>
+__device__ void part_c_packed(const VVParams& P, u64 a, u64 b, double cut, WarpShared& S,
+                              Out& out, unsigned long long& tests, u32 gs, u32 sl, int hh,
+                              int pp) {
+    const int lane = threadIdx.x & 31;
+    u32 incl = sl;   // inclusive prefix over lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const u32 v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    S.start[lane] = gs;
+    S.pre[lane] = incl - sl;
+    S.h[lane] = (u8)hh;
+    S.p[lane] = (u8)pp;
+    __syncwarp();
+    tests += total;
+    for (u32 t0 = 0; t0 < total; t0 += 32) {
+        const u32 m = t0 + lane;
+        bool keep = false;
+        double h = 0.0;
+        u32 j = 0;
+        if (m < total) {
+            int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
+#pragma unroll
+            for (int bit = 16; bit; bit >>= 1)
+                if (S.pre[l + bit] <= m) l += bit;
+            const u32 at = S.start[l] + (m - S.pre[l]);
+            const u64 y = __ldg(&P.a_other[at]);
+            const u64 x = b ^ y;
+            if (__popcll(x) == 2) {
+                const int ha = S.h[l], pa = S.p[l];
+                const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
+                const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
+                const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
+                h = (perm & 1) ? -raw : raw;
+                keep = keep_double(cut, h);
+                if (keep) j = __ldg(&P.a_idx[at]);
+            }
+        }
+        out.put(keep, j, h);
     }
     __syncwarp();
 }
@@ -416,6 +581,9 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
     const int na = __popcll(a), nva = __popcll(~a & all);
     const int nsa = na * nva;
     const int nb = __popcll(b), nvb = __popcll(~b & all);
+    const int nbv = nb * nvb;
+    const bool usep = P.pres != nullptr && nbv <= kBS;
+    int nbs = -1;   // indexed beta singles listed in S (-1: not yet)
     for (int s0 = 0; s0 < nsa; s0 += 32) {
         const int sidx = s0 + lane;
         u32 gs = 0, gl = 0;
@@ -425,49 +593,125 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
             pp = S.vira[sidx % nva];
             if (!P.amap.find(a ^ (1ull << hh) ^ (1ull << pp), gs, gl)) gl = 0;
         }
-        const bool big = gl > P.big_group;
-        const u32 sl = big ? 0u : gl;
-        S.start[lane] = gs;
-        S.len[lane] = sl;
-        S.h[lane] = (u8)hh;
-        S.p[lane] = (u8)pp;
-        __syncwarp();
-        const u32 total = __reduce_add_sync(0xffffffffu, sl);
-        tests += total;
-        // lane-private cursor (group l, offset o) advanced 32 members per step
-        int l = 0;
-        u32 o = lane;
-        while (l < 32 && o >= S.len[l]) { o -= S.len[l]; ++l; }
-        for (u32 t0 = 0; t0 < total; t0 += 32) {
-            bool keep = false;
-            double h = 0.0;
-            u32 j = 0;
-            if (l < 32) {
-                const u32 at = S.start[l] + o;
-                const u64 y = __ldg(&P.a_other[at]);
-                const u64 x = b ^ y;
-                if (__popcll(x) == 2) {
-                    const int ha = S.h[l], pa = S.p[l];
-                    const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
-                    const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
-                    const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
-                    h = (perm & 1) ? -raw : raw;
-                    keep = keep_double(cut, h);
-                    if (keep) j = __ldg(&P.a_idx[at]);
+        // presence rows for long groups (when the row's beta singles fit the
+        // warp's list), binary search above big_group otherwise, else a scan
+        const bool pbig = usep && gl > P.pres_min && gl > (u32)nbv;
+        const bool big = !pbig && gl > P.big_group;
+        const bool small = gl != 0 && !pbig && !big;
+        if (!P.c_groupwalk) {
+            part_c_packed(P, a, b, cut, S, out, tests, gs, small ? gl : 0u, hh, pp);
+        } else {
+            // one group at a time: start, length and the alpha excitation are
+            // warp-uniform, members in order 32 per step
+            unsigned m = __ballot_sync(0xffffffffu, small);
+            while (m) {
+                const int L = __ffs(m) - 1;
+                m &= m - 1;
+                const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
+                const u32 gn = __shfl_sync(0xffffffffu, gl, L);
+                const int ha = __shfl_sync(0xffffffffu, hh, L);
+                const int pa = __shfl_sync(0xffffffffu, pp, L);
+                const i64 hp = tri2(ha, pa);
+                const int perm_a = occ_between(a, pa, ha);
+                tests += gn;
+                for (u32 t0 = 0; t0 < gn; t0 += 32) {
+                    const u32 t = t0 + lane;
+                    bool keep = false;
+                    double h = 0.0;
+                    u32 j = 0;
+                    if (t < gn) {
+                        const u64 y = __ldg(&P.a_other[g0 + t]);
+                        const u64 x = b ^ y;
+                        if (__popcll(x) == 2) {
+                            const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
+                            const double raw = __ldg(&P.E[tri2(hp, tri2(hb, pb))]);   // (a i|b j)
+                            const int perm = perm_a + occ_between(b, pb, hb);
+                            h = (perm & 1) ? -raw : raw;
+                            keep = keep_double(cut, h);
+                            if (keep) j = __ldg(&P.a_idx[g0 + t]);
+                        }
+                    }
+                    out.put(keep, j, h);
                 }
             }
-            out.put(keep, j, h);
-            o += 32;
-            while (l < 32 && o >= S.len[l]) { o -= S.len[l]; ++l; }
+        }
+        unsigned pm = __ballot_sync(0xffffffffu, pbig);
+        if (pm && nbs < 0) {   // the row's indexed beta singles, once per row, in order
+            nbs = 0;
+            for (int q0 = 0; q0 < nbv; q0 += 32) {
+                const int q = q0 + lane;
+                bool f = false;
+                u32 bid = 0;
+                u16 e = 0;
+                if (q < nbv) {
+                    const int hb = S.occb[q / nvb], pb = S.virb[q % nvb];
+                    u32 st = 0, ln = 0;
+                    if (P.bmap.find(b ^ (1ull << hb) ^ (1ull << pb), st, ln)) {
+                        f = true;
+                        bid = __ldg(&P.b_gid[st]);
+                        e = (u16)(hb | (pb << 8));
+                    }
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, f);
+                if (f) {
+                    const int at = nbs + __popc(fm & lanemask_lt());
+                    S.bs_id[at] = bid;
+                    S.bs_hp[at] = e;
+                }
+                nbs += __popc(fm);
+            }
+            __syncwarp();
+        }
+        while (pm) {
+            const int L = __ffs(pm) - 1;
+            pm &= pm - 1;
+            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
+            const u32 gn = __shfl_sync(0xffffffffu, gl, L);
+            const int ha = __shfl_sync(0xffffffffu, hh, L);
+            const int pa = __shfl_sync(0xffffffffu, pp, L);
+            const u32* row = P.pres + (i64)__ldg(&P.a_prow[__ldg(&P.a_gid[g0])]) * P.pres_words;
+            const i64 hp = tri2(ha, pa);
+            const int perm_a = occ_between(a, pa, ha);
+            tests += nbs;
+            for (int q0 = 0; q0 < nbs; q0 += 32) {
+                const int q = q0 + lane;
+                bool keep = false;
+                double h = 0.0;
+                u32 j = 0;
+                if (q < nbs) {
+                    const u32 bid = S.bs_id[q];
+                    if ((__ldg(&row[bid >> 5]) >> (bid & 31)) & 1u) {
+                        const int hb = S.bs_hp[q] & 0xff, pb = S.bs_hp[q] >> 8;
+                        const double raw = __ldg(&P.E[tri2(hp, tri2(hb, pb))]);   // (a i|b j)
+                        const int perm = perm_a + occ_between(b, pb, hb);
+                        h = (perm & 1) ? -raw : raw;
+                        keep = keep_double(cut, h);
+                        if (keep) {   // the member itself: binary search of the group
+                            const u64 y = b ^ (1ull << hb) ^ (1ull << pb);
+                            u32 lo = g0, hi = g0 + gn;
+                            while (lo < hi) {
+                                const u32 mid = (lo + hi) >> 1;
+                                if (__ldg(&P.a_other[mid]) < y) lo = mid + 1; else hi = mid;
+                            }
+                            if (lo < g0 + gn && __ldg(&P.a_other[lo]) == y)
+                                j = __ldg(&P.a_idx[lo]);
+                            else
+                                keep = false;
+                        }
+                    }
+                }
+                out.put(keep, j, h);
+            }
         }
         // large groups: binary-search every beta single of b instead
         unsigned bigm = __ballot_sync(0xffffffffu, big);
         while (bigm) {
             const int L = __ffs(bigm) - 1;
             bigm &= bigm - 1;
-            const u32 g0 = S.start[L];
+            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
             const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-            const int ha = S.h[L], pa = S.p[L];
+            const int ha = __shfl_sync(0xffffffffu, hh, L);
+            const int pa = __shfl_sync(0xffffffffu, pp, L);
             tests += nb * nvb;
             for (int q0 = 0; q0 < nb * nvb; q0 += 32) {
                 const int q = q0 + lane;
@@ -831,6 +1075,13 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
     P.cut = cut;
     P.psi = psi;
     P.big_group = kBigGroup;
+    P.c_groupwalk = g_partc_groupwalk;
+    P.a_gid = A.gid.p;
+    P.a_prow = A.prow.p;
+    P.b_gid = B.gid.p;
+    P.pres = A.pres.p;
+    P.pres_words = A.pres_words;
+    P.pres_min = A.pres.p ? A.pres_min : 0xffffffffu;
     return P;
 }
 
@@ -849,6 +1100,7 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     StrIndex A, B;
     build_str_index(A, V, n, 0, s);
     build_str_index(B, V, n, 1, s);
+    build_presence(A, B, n, s);
     DNQ_CUDA(cudaEventRecord(e1, s));
     OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
     double tg = 0, tsc = 0, tc = 0;
@@ -1271,6 +1523,7 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         build_detmap(dup, b->V[k].p, n, true, s);   // duplicates are an error
         build_str_index(b->A[k], b->V[k].p, n, 0, s);
         build_str_index(b->B[k], b->V[k].p, n, 1, s);
+        build_presence(b->A[k], b->B[k], n, s);
         const double cut = (policy == DNQ_POLICY_STATIC && use_heatbath)
                                ? hb_cutoff(ctxs[k], eps1) : full_cutoff();
         hp[k] = make_params(ctxs[k], b->V[k].p, n, n_orb[k], policy, eps1, cut, nullptr,

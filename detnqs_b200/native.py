@@ -38,6 +38,7 @@ OPT_ARENA_CAP = 3
 OPT_SPMV_LANES = 4
 OPT_SPMV_UNROLL = 5
 OPT_SPMV_PANELS = 6
+OPT_PARTC_GROUPWALK = 7
 REQ_BUILD = 0
 REQ_ELOC = 1
 

@@ -126,9 +126,15 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          not depend on it;
  *   DNQ_OPT_SPMV_PANELS n: column-panel layout of the FP32 V block (x staged
  *                          in shared memory): 0 never (default), 1 from a
- *                          handle's second FP32 H.psi, 2 from the first. */
+ *                          handle's second FP32 H.psi, 2 from the first;
+ *   DNQ_OPT_PARTC_GROUPWALK n: 1 walks the short alpha-single groups of
+ *                          the string-group matcher's opposite-spin doubles
+ *                          one group at a time, 0 packed across the groups of
+ *                          a round (default); both give identical blocks,
+ *                          entry order too. */
 enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
-       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6 };
+       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6,
+       DNQ_OPT_PARTC_GROUPWALK = 7 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */

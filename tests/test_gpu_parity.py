@@ -361,6 +361,40 @@ def test_string_groups_match_candidate_walk(core, policy, use_hb, eps):
     B.close()
 
 
+@pytest.mark.parametrize("policy", [1, 2])
+def test_partc_walks_identical(core, policy):
+    """Short alpha-single groups of the opposite-spin doubles walked packed
+    (default) and one group at a time (DNQ_OPT_PARTC_GROUPWALK) give the same
+    block with the same entries in the same row order: the FP64 H.psi over
+    the unsorted rows agrees bit for bit."""
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(24, 9, 8, 48, 29)
+    V = S.heat_bath_sample(sysm, 40000, 12)
+    psi = S.normalized_psi(len(V), 6)
+    ctx = core.IntCtx.from_arrays(24, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    kw = dict(n_orb=24, policy=policy, use_heatbath=True, eps1=1e-6, want_vp=False,
+              psi=psi if policy == 2 else None)
+    # long alpha groups (> 128 members and > the 8 x 16 beta singles of a
+    # row) take the presence rows, the rest the short-group walks
+    counts = np.unique(V[:, 0], return_counts=True)[1]
+    assert (counts > 128).sum() >= 10 and (counts <= 128).sum() >= 1000
+    A = D.build(ctx, V, **kw)
+    ya = A.spmv(psi)
+    N.check(N.lib.dnq_set_option(N.OPT_PARTC_GROUPWALK, 1))
+    try:
+        B = D.build(ctx, V, **kw)
+    finally:
+        N.check(N.lib.dnq_set_option(N.OPT_PARTC_GROUPWALK, 0))
+    yb = B.spmv(psi)
+    assert A.candidates == B.candidates
+    np.testing.assert_array_equal(ya.view(np.uint64), yb.view(np.uint64))
+    assert_coo_equal(A.to_coo(0), B.to_coo(0))
+    A.close()
+    B.close()
+
+
 @pytest.mark.parametrize("chunk,cap", [(64, 0), (512, 0), (0, 5000)])
 def test_arena_paths_match(core, chunk, cap):
     """Small warp chunks force row restarts and the long-row pass; a tiny
