@@ -68,7 +68,8 @@ struct StrIndex {
     u64 mask = 0;
     // Presence rows (alpha index only): one bit per beta group for every
     // alpha group longer than pres_min; prow[group] = its row or ~0u.
-    DBuf<u32> prow, pres;
+    DBuf<u32> prow;
+    DBuf<uint2> pres;            // {bits, set bits in the row's earlier words}
     u32 pres_words = 0;
     u32 pres_min = 0xffffffffu;
     StrMapView view() const { return StrMapView{slots.p, mask}; }
@@ -210,7 +211,7 @@ __global__ void k_prow(const u32* flag, const u32* rank, i64 ngroups, u32* prow)
 
 // One bit per member of every long alpha group: its beta string's group.
 __global__ void k_pres_fill(const u32* a_gid, const u64* a_other, const u32* prow, i64 n,
-                            StrMapView bmap, const u32* b_gid, u32 words, u32* pres) {
+                            StrMapView bmap, const u32* b_gid, u32 words, uint2* pres) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x) {
         const u32 r = prow[a_gid[t]];
@@ -218,7 +219,29 @@ __global__ void k_pres_fill(const u32* a_gid, const u64* a_other, const u32* pro
         u32 st = 0, ln = 0;
         if (!bmap.find(a_other[t], st, ln)) continue;   // every member's beta is indexed
         const u32 bid = b_gid[st];
-        atomicOr(&pres[(i64)r * words + (bid >> 5)], 1u << (bid & 31));
+        atomicOr(&pres[(i64)r * words + (bid >> 5)].x, 1u << (bid & 31));
+    }
+}
+
+// .y of every word: set bits in the earlier words of its row (one warp per row).
+__global__ void k_pres_rank(uint2* pres, i64 rows, u32 words) {
+    const int lane = threadIdx.x & 31;
+    for (i64 r = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5; r < rows;
+         r += ((i64)gridDim.x * blockDim.x) >> 5) {
+        uint2* w = pres + r * words;
+        u32 carry = 0;
+        for (u32 w0 = 0; w0 < words; w0 += 32) {
+            const u32 k = w0 + lane;
+            const u32 c = k < words ? (u32)__popc(w[k].x) : 0u;
+            u32 incl = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const u32 v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            if (k < words) w[k].y = carry + incl - c;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
     }
 }
 
@@ -237,10 +260,10 @@ void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
         DNQ_CHECK_LAUNCH();
         DNQ_CUDA(cudaMemcpyAsync(&nl, cnt.p, 8, cudaMemcpyDeviceToHost, s));
         DNQ_CUDA(cudaStreamSynchronize(s));
-        if ((i64)nl * words * 4 <= kPresBytes || (i64)thr >= n) break;
+        if ((i64)nl * words * 8 <= kPresBytes || (i64)thr >= n) break;
         thr *= 2;
     }
-    if (nl == 0 || (i64)nl * words * 4 > kPresBytes) return;
+    if (nl == 0 || (i64)nl * words * 8 > kPresBytes) return;
     DBuf<u32> flag(A.ngroups, s), rank(A.ngroups, s);
     k_long_groups<<<gsz(A.ngroups), 256, 0, s>>>(A.gstart.p, A.ngroups, n, thr, flag.p, nullptr);
     DNQ_CHECK_LAUNCH();
@@ -252,9 +275,11 @@ void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
     k_prow<<<gsz(A.ngroups), 256, 0, s>>>(flag.p, rank.p, A.ngroups, A.prow.p);
     DNQ_CHECK_LAUNCH();
     A.pres.alloc((size_t)nl * words, s);
-    DNQ_CUDA(cudaMemsetAsync(A.pres.p, 0, (size_t)nl * words * 4, s));
+    DNQ_CUDA(cudaMemsetAsync(A.pres.p, 0, (size_t)nl * words * sizeof(uint2), s));
     k_pres_fill<<<gsz(n), 256, 0, s>>>(A.gid.p, A.other.p, A.prow.p, n, B.view(), B.gid.p,
                                        words, A.pres.p);
+    DNQ_CHECK_LAUNCH();
+    k_pres_rank<<<gsz((i64)nl * 32), 256, 0, s>>>(A.pres.p, (i64)nl, words);
     DNQ_CHECK_LAUNCH();
     A.pres_words = words;
     A.pres_min = thr;
@@ -290,7 +315,7 @@ struct VVParams {
     const u32* a_gid;       // group number of every alpha-sorted position
     const u32* a_prow;      // presence row of every alpha group (~0u: none)
     const u32* b_gid;       // group number of every beta-sorted position
-    const u32* pres;
+    const uint2* pres;
     u32 pres_words;
     u32 pres_min;
 };
@@ -453,20 +478,101 @@ struct WarpShared {
     u8 occa[64], vira[64], occb[64], virb[64];
     u32 bs_id[kBS];            // beta group of each indexed beta single of the row
     u16 bs_hp[kBS];            // its excitation, hole | particle << 8
+    u32 hit_pos[64], hit_tag[64];   // ring of connected members awaiting evaluation
 };
 
-__device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, u64 all) {
-    if ((threadIdx.x & 31) == 0) {
-        int k = 0;
-        for (u64 m = a; m; m &= m - 1) S.occa[k++] = (u8)(__ffsll(m) - 1);
-        k = 0;
-        for (u64 m = ~a & all; m; m &= m - 1) S.vira[k++] = (u8)(__ffsll(m) - 1);
-        k = 0;
-        for (u64 m = b; m; m &= m - 1) S.occb[k++] = (u8)(__ffsll(m) - 1);
-        k = 0;
-        for (u64 m = ~b & all; m; m &= m - 1) S.virb[k++] = (u8)(__ffsll(m) - 1);
+// Occupied and virtual orbital lists of both strings, one lane per orbital.
+__device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, int n_orb) {
+    const int lane = threadIdx.x & 31;
+    for (int o = lane; o < n_orb; o += 32) {
+        const u64 below = (1ull << o) - 1ull;
+        if ((a >> o) & 1ull) S.occa[__popcll(a & below)] = (u8)o;
+        else S.vira[o - __popcll(a & below)] = (u8)o;
+        if ((b >> o) & 1ull) S.occb[__popcll(b & below)] = (u8)o;
+        else S.virb[o - __popcll(b & below)] = (u8)o;
     }
     __syncwarp();
+}
+
+// Members found connected to the row are queued with their kind and
+// evaluated 32 at a time, so the Slater-Condon arithmetic runs on full
+// warps; entries leave in the order they were found.
+enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2 };   // same beta / same alpha / opposite-spin
+
+struct RowCtx {
+    const VVParams& P;
+    int r;
+    u64 a, b;
+    double psr, cut;
+    WarpShared& S;
+    int n = 0, head = 0;   // queued hits (warp-uniform)
+};
+
+template <class Out>
+__device__ __forceinline__ void eval_hits(RowCtx& R, Out& out, int cnt) {
+    const int lane = threadIdx.x & 31;
+    const VVParams& P = R.P;
+    bool keep = false;
+    double h = 0.0;
+    u32 j = 0;
+    if (lane < cnt) {
+        const int k = (R.head + lane) & 63;
+        const u32 pos = R.S.hit_pos[k], tag = R.S.hit_tag[k];
+        const u32 kind = tag & 0xff;
+        if (kind == kHitC) {
+            const u64 y = __ldg(&P.a_other[pos]);
+            const u64 x = R.b ^ y;
+            const int ha = (tag >> 8) & 0xff, pa = tag >> 16;
+            const int hb = __ffsll(R.b & x) - 1, pb = __ffsll(y & x) - 1;
+            const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
+            const int perm = occ_between(R.a, pa, ha) + occ_between(R.b, pb, hb);
+            h = (perm & 1) ? -raw : raw;
+            keep = keep_double(R.cut, h);
+            if (keep) j = __ldg(&P.a_idx[pos]);
+        } else {
+            const bool alpha = kind == kHitA;   // the alpha string moves
+            const u64 y = alpha ? __ldg(&P.b_other[pos]) : __ldg(&P.a_other[pos]);
+            const u64 x = alpha ? R.a : R.b;
+            if (__popcll(x ^ y) == 2) {
+                h = str_single(P, R.a, R.b, alpha ? 0 : 1, x, y);
+                keep = keep_single(P, R.psr, h);
+            } else {
+                h = str_double_same(P, x, y);
+                keep = keep_double(R.cut, h);
+            }
+            if (keep) j = alpha ? __ldg(&P.b_idx[pos]) : __ldg(&P.a_idx[pos]);
+        }
+    }
+    out.put(keep, j, h);
+}
+
+template <class Out>
+__device__ __forceinline__ void push_hit(RowCtx& R, Out& out, bool hit, u32 pos, u32 tag) {
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (hit) {
+        const int k = (R.head + R.n + __popc(m & lanemask_lt())) & 63;
+        R.S.hit_pos[k] = pos;
+        R.S.hit_tag[k] = tag;
+    }
+    R.n += __popc(m);
+    if (R.n >= 32) {
+        __syncwarp();
+        eval_hits(R, out, 32);
+        R.head = (R.head + 32) & 63;
+        R.n -= 32;
+        __syncwarp();
+    }
+}
+
+template <class Out>
+__device__ __forceinline__ void flush_hits(RowCtx& R, Out& out) {
+    if (R.n) {
+        __syncwarp();
+        eval_hits(R, out, R.n);
+        R.head = (R.head + R.n) & 63;
+        R.n = 0;
+        __syncwarp();
+    }
 }
 
 // Part C over the short groups of one round of 32 alpha singles, packed:
@@ -474,10 +580,10 @@ __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, u64 all)
 // tests 32 consecutive members; a lane finds its member's group by a
 // five-step search of the exclusive prefix of the group lengths.
 template <class Out>
-__device__ void part_c_packed(const VVParams& P, u64 a, u64 b, double cut, WarpShared& S,
-                              Out& out, unsigned long long& tests, u32 gs, u32 sl, int hh,
-                              int pp) {
+__device__ void part_c_packed(RowCtx& R, Out& out, unsigned long long& tests, u32 gs, u32 sl,
+                              int hh, int pp) {
     const int lane = threadIdx.x & 31;
+    WarpShared& S = R.S;
     u32 incl = sl;   // inclusive prefix over lanes
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -494,28 +600,18 @@ __device__ void part_c_packed(const VVParams& P, u64 a, u64 b, double cut, WarpS
     tests += total;
     for (u32 t0 = 0; t0 < total; t0 += 32) {
         const u32 m = t0 + lane;
-        bool keep = false;
-        double h = 0.0;
-        u32 j = 0;
+        bool hit = false;
+        u32 at = 0, tag = 0;
         if (m < total) {
             int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
 #pragma unroll
             for (int bit = 16; bit; bit >>= 1)
                 if (S.pre[l + bit] <= m) l += bit;
-            const u32 at = S.start[l] + (m - S.pre[l]);
-            const u64 y = __ldg(&P.a_other[at]);
-            const u64 x = b ^ y;
-            if (__popcll(x) == 2) {
-                const int ha = S.h[l], pa = S.p[l];
-                const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
-                const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
-                const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
-                h = (perm & 1) ? -raw : raw;
-                keep = keep_double(cut, h);
-                if (keep) j = __ldg(&P.a_idx[at]);
-            }
+            at = S.start[l] + (m - S.pre[l]);
+            hit = __popcll(R.b ^ __ldg(&R.P.a_other[at])) == 2;
+            tag = kHitC | ((u32)S.h[l] << 8) | ((u32)S.p[l] << 16);
         }
-        out.put(keep, j, h);
+        push_hit(R, out, hit, at, tag);
     }
     __syncwarp();
 }
@@ -528,7 +624,8 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
     const u64 all = low_mask(P.n_orb);
     const double d = P.diag[r];
     out.put(lane == 0 && fabs(d) > kElemThresh, (u32)r, d);
-    // ---- part A: same beta string
+    RowCtx R{P, r, a, b, psr, cut, S};
+    // ---- part A: same beta string (alpha singles and doubles)
     u32 st = 0, ln = 0;
     if (lane == 0 && !P.bmap.find(b, st, ln)) ln = 0;
     st = __shfl_sync(0xffffffffu, st, 0);
@@ -536,46 +633,26 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
     tests += ln;
     for (u32 t0 = 0; t0 < ln; t0 += 32) {
         const u32 t = t0 + lane;
-        bool keep = false;
-        double h = 0.0;
-        u32 j = 0;
+        bool hit = false;
         if (t < ln) {
-            const u64 y = __ldg(&P.b_other[st + t]);
-            const int dd = __popcll(a ^ y);
-            if (dd == 2) {
-                h = str_single(P, a, b, 0, a, y);
-                keep = keep_single(P, psr, h);
-            } else if (dd == 4) {
-                h = str_double_same(P, a, y);
-                keep = keep_double(cut, h);
-            }
-            if (keep) j = __ldg(&P.b_idx[st + t]);
+            const int dd = __popcll(a ^ __ldg(&P.b_other[st + t]));
+            hit = dd == 2 || dd == 4;
         }
-        out.put(keep, j, h);
+        push_hit(R, out, hit, st + t, kHitA);
     }
-    // ---- part B: same alpha string
+    // ---- part B: same alpha string (beta singles and doubles)
     if (lane == 0 && !P.amap.find(a, st, ln)) ln = 0;
     st = __shfl_sync(0xffffffffu, st, 0);
     ln = __shfl_sync(0xffffffffu, ln, 0);
     tests += ln;
     for (u32 t0 = 0; t0 < ln; t0 += 32) {
         const u32 t = t0 + lane;
-        bool keep = false;
-        double h = 0.0;
-        u32 j = 0;
+        bool hit = false;
         if (t < ln) {
-            const u64 y = __ldg(&P.a_other[st + t]);
-            const int dd = __popcll(b ^ y);
-            if (dd == 2) {
-                h = str_single(P, a, b, 1, b, y);
-                keep = keep_single(P, psr, h);
-            } else if (dd == 4) {
-                h = str_double_same(P, b, y);
-                keep = keep_double(cut, h);
-            }
-            if (keep) j = __ldg(&P.a_idx[st + t]);
+            const int dd = __popcll(b ^ __ldg(&P.a_other[st + t]));
+            hit = dd == 2 || dd == 4;
         }
-        out.put(keep, j, h);
+        push_hit(R, out, hit, st + t, kHitB);
     }
     // ---- part C: alpha single x beta single, via the groups of the a'
     const int na = __popcll(a), nva = __popcll(~a & all);
@@ -599,7 +676,7 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
         const bool big = !pbig && gl > P.big_group;
         const bool small = gl != 0 && !pbig && !big;
         if (!P.c_groupwalk) {
-            part_c_packed(P, a, b, cut, S, out, tests, gs, small ? gl : 0u, hh, pp);
+            part_c_packed(R, out, tests, gs, small ? gl : 0u, hh, pp);
         } else {
             // one group at a time: start, length and the alpha excitation are
             // warp-uniform, members in order 32 per step
@@ -609,29 +686,13 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
                 m &= m - 1;
                 const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
                 const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-                const int ha = __shfl_sync(0xffffffffu, hh, L);
-                const int pa = __shfl_sync(0xffffffffu, pp, L);
-                const i64 hp = tri2(ha, pa);
-                const int perm_a = occ_between(a, pa, ha);
+                const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                                ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
                 tests += gn;
                 for (u32 t0 = 0; t0 < gn; t0 += 32) {
                     const u32 t = t0 + lane;
-                    bool keep = false;
-                    double h = 0.0;
-                    u32 j = 0;
-                    if (t < gn) {
-                        const u64 y = __ldg(&P.a_other[g0 + t]);
-                        const u64 x = b ^ y;
-                        if (__popcll(x) == 2) {
-                            const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
-                            const double raw = __ldg(&P.E[tri2(hp, tri2(hb, pb))]);   // (a i|b j)
-                            const int perm = perm_a + occ_between(b, pb, hb);
-                            h = (perm & 1) ? -raw : raw;
-                            keep = keep_double(cut, h);
-                            if (keep) j = __ldg(&P.a_idx[g0 + t]);
-                        }
-                    }
-                    out.put(keep, j, h);
+                    const bool hit = t < gn && __popcll(b ^ __ldg(&P.a_other[g0 + t])) == 2;
+                    push_hit(R, out, hit, g0 + t, tag);
                 }
             }
         }
@@ -645,10 +706,10 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
                 u16 e = 0;
                 if (q < nbv) {
                     const int hb = S.occb[q / nvb], pb = S.virb[q % nvb];
-                    u32 st = 0, ln = 0;
-                    if (P.bmap.find(b ^ (1ull << hb) ^ (1ull << pb), st, ln)) {
+                    u32 bst = 0, bln = 0;
+                    if (P.bmap.find(b ^ (1ull << hb) ^ (1ull << pb), bst, bln)) {
                         f = true;
-                        bid = __ldg(&P.b_gid[st]);
+                        bid = __ldg(&P.b_gid[bst]);
                         e = (u16)(hb | (pb << 8));
                     }
                 }
@@ -663,83 +724,62 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
             __syncwarp();
         }
         while (pm) {
+            // members of a long group are sorted by beta group: the member
+            // with beta group bid sits at the number of set bits before bid
             const int L = __ffs(pm) - 1;
             pm &= pm - 1;
             const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
-            const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-            const int ha = __shfl_sync(0xffffffffu, hh, L);
-            const int pa = __shfl_sync(0xffffffffu, pp, L);
-            const u32* row = P.pres + (i64)__ldg(&P.a_prow[__ldg(&P.a_gid[g0])]) * P.pres_words;
-            const i64 hp = tri2(ha, pa);
-            const int perm_a = occ_between(a, pa, ha);
+            const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
+            const uint2* row =
+                P.pres + (i64)__ldg(&P.a_prow[__ldg(&P.a_gid[g0])]) * P.pres_words;
             tests += nbs;
             for (int q0 = 0; q0 < nbs; q0 += 32) {
                 const int q = q0 + lane;
-                bool keep = false;
-                double h = 0.0;
-                u32 j = 0;
+                bool hit = false;
+                u32 at = 0;
                 if (q < nbs) {
                     const u32 bid = S.bs_id[q];
-                    if ((__ldg(&row[bid >> 5]) >> (bid & 31)) & 1u) {
-                        const int hb = S.bs_hp[q] & 0xff, pb = S.bs_hp[q] >> 8;
-                        const double raw = __ldg(&P.E[tri2(hp, tri2(hb, pb))]);   // (a i|b j)
-                        const int perm = perm_a + occ_between(b, pb, hb);
-                        h = (perm & 1) ? -raw : raw;
-                        keep = keep_double(cut, h);
-                        if (keep) {   // the member itself: binary search of the group
-                            const u64 y = b ^ (1ull << hb) ^ (1ull << pb);
-                            u32 lo = g0, hi = g0 + gn;
-                            while (lo < hi) {
-                                const u32 mid = (lo + hi) >> 1;
-                                if (__ldg(&P.a_other[mid]) < y) lo = mid + 1; else hi = mid;
-                            }
-                            if (lo < g0 + gn && __ldg(&P.a_other[lo]) == y)
-                                j = __ldg(&P.a_idx[lo]);
-                            else
-                                keep = false;
-                        }
-                    }
+                    const uint2 w = __ldg(&row[bid >> 5]);
+                    const u32 below = w.x & ((1u << (bid & 31)) - 1u);
+                    hit = (w.x >> (bid & 31)) & 1u;
+                    at = g0 + w.y + __popc(below);
                 }
-                out.put(keep, j, h);
+                push_hit(R, out, hit, at, tag);
             }
         }
-        // large groups: binary-search every beta single of b instead
+        // other large groups: binary-search every beta single of b
         unsigned bigm = __ballot_sync(0xffffffffu, big);
         while (bigm) {
             const int L = __ffs(bigm) - 1;
             bigm &= bigm - 1;
             const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
             const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-            const int ha = __shfl_sync(0xffffffffu, hh, L);
-            const int pa = __shfl_sync(0xffffffffu, pp, L);
-            tests += nb * nvb;
-            for (int q0 = 0; q0 < nb * nvb; q0 += 32) {
+            const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
+            tests += nbv;
+            for (int q0 = 0; q0 < nbv; q0 += 32) {
                 const int q = q0 + lane;
-                bool keep = false;
-                double h = 0.0;
-                u32 j = 0;
-                if (q < nb * nvb) {
+                bool hit = false;
+                u32 lo = 0;
+                if (q < nbv) {
                     const int hb = S.occb[q / nvb];
                     const int pb = S.virb[q % nvb];
                     const u64 y = b ^ (1ull << hb) ^ (1ull << pb);
-                    u32 lo = g0, hi = g0 + gn;
+                    lo = g0;
+                    u32 hi = g0 + gn;
                     while (lo < hi) {
                         const u32 mid = (lo + hi) >> 1;
                         if (__ldg(&P.a_other[mid]) < y) lo = mid + 1; else hi = mid;
                     }
-                    if (lo < g0 + gn && __ldg(&P.a_other[lo]) == y) {
-                        const double raw = eri(P.E, ha, pa, hb, pb);
-                        const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
-                        h = (perm & 1) ? -raw : raw;
-                        keep = keep_double(cut, h);
-                        if (keep) j = __ldg(&P.a_idx[lo]);
-                    }
+                    hit = lo < g0 + gn && __ldg(&P.a_other[lo]) == y;
                 }
-                out.put(keep, j, h);
+                push_hit(R, out, hit, lo, tag);
             }
         }
         __syncwarp();
     }
+    flush_hits(R, out);
 }
 
 __device__ __forceinline__ void row_setup(const VVParams& P, int r, u64& a, u64& b, double& psr,
@@ -788,7 +828,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, low_mask(P.n_orb));
+        load_lists(S, a, b, P.n_orb);
         for (int attempt = 0; attempt < 2; ++attempt) {
             ChunkOut out{A.acol, A.aval, cpos, cend, cb};
             unsigned long long tt = 0;
@@ -857,7 +897,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, low_mask(P.n_orb));
+        load_lists(S, a, b, P.n_orb);
         ExactOut out{A.acol, A.aval, (i64)base, cb};
         unsigned long long tt = 0;
         vv_row(P, r, a, b, psr, cut, S, out, tt);
@@ -902,7 +942,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_twopass(Loc L, Arena A) {
         u64 a, b;
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
-        load_lists(S, a, b, low_mask(P.n_orb));
+        load_lists(S, a, b, P.n_orb);
         unsigned long long tt = 0;
         if (!FILL) {
             CountOut out;
