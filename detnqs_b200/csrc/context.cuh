@@ -73,7 +73,7 @@ struct dnq_ctx_s {
     dnq::PairTable tab;
     bool has_hb = false;
     double hb_thr = 0.0;
-    std::atomic<long long> vv_nnz_hint{0};   // largest H_VV built here (arena sizing)
+    std::atomic<long long> vv_nnz_hint{0};   // largest H_VV (entries or members) built here
 
     dnq::CtxView view() const {
         dnq::CtxView c;

@@ -337,6 +337,7 @@ struct Arena {
     int* n_big;
     int* next_row;
     unsigned long long* n_test;
+    unsigned long long* n_hit;        // members recorded by k_vv_arena (optional)
     u32* cnt;                         // two-pass fallback
     const i64* off;
     u32* col;
@@ -404,33 +405,6 @@ struct ExactOut {
     }
 };
 
-// Writes into [w, end) of a chunk; past the end it only counts.
-struct ChunkOut {
-    u32* col;
-    double* val;
-    i64 w, end;
-    u32 base;
-    u32 c = 0;
-    bool over = false;
-    __device__ __forceinline__ void put(bool keep, u32 j, double h) {
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        const int k = __popc(m);
-        if (!over) {
-            if (w + k > end) {
-                over = true;
-            } else {
-                if (keep) {
-                    const i64 at = w + __popc(m & lanemask_lt());
-                    col[at] = j + base;
-                    val[at] = h;
-                }
-                w += k;
-            }
-        }
-        c += k;
-    }
-};
-
 // Single within one spin: bra string x -> ket string y (differ in 2 bits).
 __device__ __forceinline__ double str_single(const VVParams& P, u64 a, u64 b, int spin, u64 x,
                                              u64 y) {
@@ -472,13 +446,19 @@ __device__ __forceinline__ bool keep_single(const VVParams& P, double psr, doubl
 // Per-warp shared state.
 constexpr int kBS = 512;   // beta singles of one row kept for the presence rows
 
+// Loads of a scan are issued kScanU steps ahead of their tests (every step
+// is a dependent global load); the sink sees the kScanU steps' hits, then
+// one sync, so a queue holds at most 31 + 32 kScanU members.
+constexpr int kScanU = 4;
+constexpr int kRing = 32 + 32 * kScanU;
+
 struct WarpShared {
     u32 start[32], pre[32];    // part C: group starts, exclusive prefix of lengths
     u8 h[32], p[32];
     u8 occa[64], vira[64], occb[64], virb[64];
     u32 bs_id[kBS];            // beta group of each indexed beta single of the row
     u16 bs_hp[kBS];            // its excitation, hole | particle << 8
-    u32 hit_pos[64], hit_tag[64];   // ring of connected members awaiting evaluation
+    u32 hit_pos[kRing], hit_tag[kRing];   // members awaiting evaluation (fallback walks)
 };
 
 // Occupied and virtual orbital lists of both strings, one lane per orbital.
@@ -494,96 +474,63 @@ __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, int n_or
     __syncwarp();
 }
 
-// Members found connected to the row are queued with their kind and
-// evaluated 32 at a time, so the Slater-Condon arithmetic runs on full
-// warps; entries leave in the order they were found.
-enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2 };   // same beta / same alpha / opposite-spin
+// A connected member of a row is a (sorted position, tag) pair: the tag's
+// low byte is its kind, and for opposite-spin doubles bits 8-15 / 16-23
+// hold the alpha hole and particle.  The diagonal is a member of its own
+// kind whose position is the row.  Members are found by walk_row and
+// turned into elements by eval_hit, in the order found.
+// kinds: same beta string, same alpha string, opposite-spin double, diagonal
+enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2, kHitD = 3 };
 
-struct RowCtx {
-    const VVParams& P;
-    int r;
-    u64 a, b;
-    double psr, cut;
-    WarpShared& S;
-    int n = 0, head = 0;   // queued hits (warp-uniform)
+struct Hit {
+    double h;
+    u32 j;
+    bool keep;
 };
 
-template <class Out>
-__device__ __forceinline__ void eval_hits(RowCtx& R, Out& out, int cnt) {
-    const int lane = threadIdx.x & 31;
-    const VVParams& P = R.P;
-    bool keep = false;
-    double h = 0.0;
-    u32 j = 0;
-    if (lane < cnt) {
-        const int k = (R.head + lane) & 63;
-        const u32 pos = R.S.hit_pos[k], tag = R.S.hit_tag[k];
-        const u32 kind = tag & 0xff;
-        if (kind == kHitC) {
-            const u64 y = __ldg(&P.a_other[pos]);
-            const u64 x = R.b ^ y;
-            const int ha = (tag >> 8) & 0xff, pa = tag >> 16;
-            const int hb = __ffsll(R.b & x) - 1, pb = __ffsll(y & x) - 1;
-            const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
-            const int perm = occ_between(R.a, pa, ha) + occ_between(R.b, pb, hb);
-            h = (perm & 1) ? -raw : raw;
-            keep = keep_double(R.cut, h);
-            if (keep) j = __ldg(&P.a_idx[pos]);
+__device__ __forceinline__ Hit eval_hit(const VVParams& P, int r, u64 a, u64 b, double psr,
+                                        double cut, u32 pos, u32 tag) {
+    Hit e{0.0, 0u, false};
+    const u32 kind = tag & 0xff;
+    if (kind == kHitC) {
+        const u64 y = __ldg(&P.a_other[pos]);
+        const u64 x = b ^ y;
+        const int ha = (tag >> 8) & 0xff, pa = tag >> 16;
+        const int hb = __ffsll(b & x) - 1, pb = __ffsll(y & x) - 1;
+        const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
+        const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
+        e.h = (perm & 1) ? -raw : raw;
+        e.keep = keep_double(cut, e.h);
+        if (e.keep) e.j = __ldg(&P.a_idx[pos]);
+    } else if (kind == kHitD) {
+        e.h = P.diag[r];
+        e.keep = fabs(e.h) > kElemThresh;
+        e.j = (u32)r;
+    } else {
+        const bool alpha = kind == kHitA;   // the alpha string moves
+        const u64 y = alpha ? __ldg(&P.b_other[pos]) : __ldg(&P.a_other[pos]);
+        const u64 x = alpha ? a : b;
+        if (__popcll(x ^ y) == 2) {
+            e.h = str_single(P, a, b, alpha ? 0 : 1, x, y);
+            e.keep = keep_single(P, psr, e.h);
         } else {
-            const bool alpha = kind == kHitA;   // the alpha string moves
-            const u64 y = alpha ? __ldg(&P.b_other[pos]) : __ldg(&P.a_other[pos]);
-            const u64 x = alpha ? R.a : R.b;
-            if (__popcll(x ^ y) == 2) {
-                h = str_single(P, R.a, R.b, alpha ? 0 : 1, x, y);
-                keep = keep_single(P, R.psr, h);
-            } else {
-                h = str_double_same(P, x, y);
-                keep = keep_double(R.cut, h);
-            }
-            if (keep) j = alpha ? __ldg(&P.b_idx[pos]) : __ldg(&P.a_idx[pos]);
+            e.h = str_double_same(P, x, y);
+            e.keep = keep_double(cut, e.h);
         }
+        if (e.keep) e.j = alpha ? __ldg(&P.b_idx[pos]) : __ldg(&P.a_idx[pos]);
     }
-    out.put(keep, j, h);
-}
-
-template <class Out>
-__device__ __forceinline__ void push_hit(RowCtx& R, Out& out, bool hit, u32 pos, u32 tag) {
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    if (hit) {
-        const int k = (R.head + R.n + __popc(m & lanemask_lt())) & 63;
-        R.S.hit_pos[k] = pos;
-        R.S.hit_tag[k] = tag;
-    }
-    R.n += __popc(m);
-    if (R.n >= 32) {
-        __syncwarp();
-        eval_hits(R, out, 32);
-        R.head = (R.head + 32) & 63;
-        R.n -= 32;
-        __syncwarp();
-    }
-}
-
-template <class Out>
-__device__ __forceinline__ void flush_hits(RowCtx& R, Out& out) {
-    if (R.n) {
-        __syncwarp();
-        eval_hits(R, out, R.n);
-        R.head = (R.head + R.n) & 63;
-        R.n = 0;
-        __syncwarp();
-    }
+    return e;
 }
 
 // Part C over the short groups of one round of 32 alpha singles, packed:
 // the members of all of them are numbered in group order and each step
 // tests 32 consecutive members; a lane finds its member's group by a
 // five-step search of the exclusive prefix of the group lengths.
-template <class Out>
-__device__ void part_c_packed(RowCtx& R, Out& out, unsigned long long& tests, u32 gs, u32 sl,
-                              int hh, int pp) {
+template <class Q>
+__device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const u64* a_other, u64 b,
+                                              unsigned long long& tests, u32 gs, u32 sl, int hh,
+                                              int pp) {
     const int lane = threadIdx.x & 31;
-    WarpShared& S = R.S;
     u32 incl = sl;   // inclusive prefix over lanes
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -598,62 +545,80 @@ __device__ void part_c_packed(RowCtx& R, Out& out, unsigned long long& tests, u3
     S.p[lane] = (u8)pp;
     __syncwarp();
     tests += total;
-    for (u32 t0 = 0; t0 < total; t0 += 32) {
-        const u32 m = t0 + lane;
-        bool hit = false;
-        u32 at = 0, tag = 0;
-        if (m < total) {
-            int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
+    for (u32 t0 = 0; t0 < total; t0 += 32 * kScanU) {
+        u32 at[kScanU], tag[kScanU];
+        u64 y[kScanU];
 #pragma unroll
-            for (int bit = 16; bit; bit >>= 1)
-                if (S.pre[l + bit] <= m) l += bit;
-            at = S.start[l] + (m - S.pre[l]);
-            hit = __popcll(R.b ^ __ldg(&R.P.a_other[at])) == 2;
-            tag = kHitC | ((u32)S.h[l] << 8) | ((u32)S.p[l] << 16);
+        for (int u = 0; u < kScanU; ++u) {
+            const u32 m = t0 + 32 * u + lane;
+            at[u] = 0;
+            tag[u] = 0;
+            y[u] = b;   // no hit
+            if (m < total) {
+                int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
+#pragma unroll
+                for (int bit = 16; bit; bit >>= 1)
+                    if (S.pre[l + bit] <= m) l += bit;
+                at[u] = S.start[l] + (m - S.pre[l]);
+                tag[u] = kHitC | ((u32)S.h[l] << 8) | ((u32)S.p[l] << 16);
+                y[u] = __ldg(&a_other[at[u]]);
+            }
         }
-        push_hit(R, out, hit, at, tag);
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u) {
+            if (t0 + 32 * u >= total) break;
+            q.push(__popcll(b ^ y[u]) == 2, at[u], tag[u]);
+        }
+        q.sync();
     }
     __syncwarp();
 }
 
-// All entries of row r: the diagonal first, then parts A, B and C.
-template <class Out>
-__device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, double cut,
-                       WarpShared& S, Out& out, unsigned long long& tests) {
+// Parts A and B: the members of one group [st, st + ln) whose string differs
+// from x in 2 or 4 orbitals.
+template <class Q>
+__device__ __forceinline__ void scan_same(Q& q, const u64* other, u64 x, u32 st, u32 ln,
+                                          u32 kind) {
+    const int lane = threadIdx.x & 31;
+    for (u32 t0 = 0; t0 < ln; t0 += 32 * kScanU) {
+        u64 y[kScanU];
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u) {
+            const u32 t = t0 + 32 * u + lane;
+            y[u] = t < ln ? __ldg(&other[st + t]) : x;
+        }
+#pragma unroll
+        for (int u = 0; u < kScanU; ++u) {
+            if (t0 + 32 * u >= ln) break;
+            const int dd = __popcll(x ^ y[u]);
+            q.push(dd == 2 || dd == 4, st + t0 + 32 * u + lane, kind);
+        }
+        q.sync();
+    }
+}
+
+// The members of row r = (a, b) in their fixed order: the diagonal, then
+// parts A, B and C.  q.push(hit, position, tag) is warp-collective, once
+// per step of 32; q.sync() follows every group of at most kScanU steps.
+template <class Q>
+__device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b, WarpShared& S,
+                                         Q& q, unsigned long long& tests) {
     const int lane = threadIdx.x & 31;
     const u64 all = low_mask(P.n_orb);
-    const double d = P.diag[r];
-    out.put(lane == 0 && fabs(d) > kElemThresh, (u32)r, d);
-    RowCtx R{P, r, a, b, psr, cut, S};
+    q.push(lane == 0, (u32)r, kHitD);
     // ---- part A: same beta string (alpha singles and doubles)
     u32 st = 0, ln = 0;
     if (lane == 0 && !P.bmap.find(b, st, ln)) ln = 0;
     st = __shfl_sync(0xffffffffu, st, 0);
     ln = __shfl_sync(0xffffffffu, ln, 0);
     tests += ln;
-    for (u32 t0 = 0; t0 < ln; t0 += 32) {
-        const u32 t = t0 + lane;
-        bool hit = false;
-        if (t < ln) {
-            const int dd = __popcll(a ^ __ldg(&P.b_other[st + t]));
-            hit = dd == 2 || dd == 4;
-        }
-        push_hit(R, out, hit, st + t, kHitA);
-    }
+    scan_same(q, P.b_other, a, st, ln, kHitA);
     // ---- part B: same alpha string (beta singles and doubles)
     if (lane == 0 && !P.amap.find(a, st, ln)) ln = 0;
     st = __shfl_sync(0xffffffffu, st, 0);
     ln = __shfl_sync(0xffffffffu, ln, 0);
     tests += ln;
-    for (u32 t0 = 0; t0 < ln; t0 += 32) {
-        const u32 t = t0 + lane;
-        bool hit = false;
-        if (t < ln) {
-            const int dd = __popcll(b ^ __ldg(&P.a_other[st + t]));
-            hit = dd == 2 || dd == 4;
-        }
-        push_hit(R, out, hit, st + t, kHitB);
-    }
+    scan_same(q, P.a_other, b, st, ln, kHitB);
     // ---- part C: alpha single x beta single, via the groups of the a'
     const int na = __popcll(a), nva = __popcll(~a & all);
     const int nsa = na * nva;
@@ -676,7 +641,7 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
         const bool big = !pbig && gl > P.big_group;
         const bool small = gl != 0 && !pbig && !big;
         if (!P.c_groupwalk) {
-            part_c_packed(R, out, tests, gs, small ? gl : 0u, hh, pp);
+            part_c_packed(q, S, P.a_other, b, tests, gs, small ? gl : 0u, hh, pp);
         } else {
             // one group at a time: start, length and the alpha excitation are
             // warp-uniform, members in order 32 per step
@@ -689,10 +654,19 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
                 const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
                                 ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
                 tests += gn;
-                for (u32 t0 = 0; t0 < gn; t0 += 32) {
-                    const u32 t = t0 + lane;
-                    const bool hit = t < gn && __popcll(b ^ __ldg(&P.a_other[g0 + t])) == 2;
-                    push_hit(R, out, hit, g0 + t, tag);
+                for (u32 t0 = 0; t0 < gn; t0 += 32 * kScanU) {
+                    u64 y[kScanU];
+#pragma unroll
+                    for (int u = 0; u < kScanU; ++u) {
+                        const u32 t = t0 + 32 * u + lane;
+                        y[u] = t < gn ? __ldg(&P.a_other[g0 + t]) : b;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kScanU; ++u) {
+                        if (t0 + 32 * u >= gn) break;
+                        q.push(__popcll(b ^ y[u]) == 2, g0 + t0 + 32 * u + lane, tag);
+                    }
+                    q.sync();
                 }
             }
         }
@@ -700,12 +674,12 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
         if (pm && nbs < 0) {   // the row's indexed beta singles, once per row, in order
             nbs = 0;
             for (int q0 = 0; q0 < nbv; q0 += 32) {
-                const int q = q0 + lane;
+                const int qi = q0 + lane;
                 bool f = false;
                 u32 bid = 0;
                 u16 e = 0;
-                if (q < nbv) {
-                    const int hb = S.occb[q / nvb], pb = S.virb[q % nvb];
+                if (qi < nbv) {
+                    const int hb = S.occb[qi / nvb], pb = S.virb[qi % nvb];
                     u32 bst = 0, bln = 0;
                     if (P.bmap.find(b ^ (1ull << hb) ^ (1ull << pb), bst, bln)) {
                         f = true;
@@ -734,18 +708,28 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
             const uint2* row =
                 P.pres + (i64)__ldg(&P.a_prow[__ldg(&P.a_gid[g0])]) * P.pres_words;
             tests += nbs;
-            for (int q0 = 0; q0 < nbs; q0 += 32) {
-                const int q = q0 + lane;
-                bool hit = false;
-                u32 at = 0;
-                if (q < nbs) {
-                    const u32 bid = S.bs_id[q];
-                    const uint2 w = __ldg(&row[bid >> 5]);
-                    const u32 below = w.x & ((1u << (bid & 31)) - 1u);
-                    hit = (w.x >> (bid & 31)) & 1u;
-                    at = g0 + w.y + __popc(below);
+            for (int q0 = 0; q0 < nbs; q0 += 32 * kScanU) {
+                uint2 w[kScanU];
+                u32 bit[kScanU];
+#pragma unroll
+                for (int u = 0; u < kScanU; ++u) {
+                    const int qi = q0 + 32 * u + lane;
+                    w[u] = make_uint2(0u, 0u);
+                    bit[u] = 0;
+                    if (qi < nbs) {
+                        const u32 bid = S.bs_id[qi];
+                        bit[u] = bid & 31;
+                        w[u] = __ldg(&row[bid >> 5]);
+                    }
                 }
-                push_hit(R, out, hit, at, tag);
+#pragma unroll
+                for (int u = 0; u < kScanU; ++u) {
+                    if (q0 + 32 * u >= nbs) break;
+                    const bool hit = (w[u].x >> bit[u]) & 1u;
+                    const u32 at = g0 + w[u].y + __popc(w[u].x & ((1u << bit[u]) - 1u));
+                    q.push(hit, at, tag);
+                }
+                q.sync();
             }
         }
         // other large groups: binary-search every beta single of b
@@ -759,12 +743,12 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
                             ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
             tests += nbv;
             for (int q0 = 0; q0 < nbv; q0 += 32) {
-                const int q = q0 + lane;
+                const int qi = q0 + lane;
                 bool hit = false;
                 u32 lo = 0;
-                if (q < nbv) {
-                    const int hb = S.occb[q / nvb];
-                    const int pb = S.virb[q % nvb];
+                if (qi < nbv) {
+                    const int hb = S.occb[qi / nvb];
+                    const int pb = S.virb[qi % nvb];
                     const u64 y = b ^ (1ull << hb) ^ (1ull << pb);
                     lo = g0;
                     u32 hi = g0 + gn;
@@ -774,12 +758,103 @@ __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, doubl
                     }
                     hit = lo < g0 + gn && __ldg(&P.a_other[lo]) == y;
                 }
-                push_hit(R, out, hit, lo, tag);
+                q.push(hit, lo, tag);
+                q.sync();
             }
         }
         __syncwarp();
     }
-    flush_hits(R, out);
+}
+
+// Sink of walk_row that records the members only: (position, tag) pairs
+// appended to [w, end) of an arena chunk (col holds the position, the low
+// word of the value slot the tag); past the end it only counts.
+struct HitOut {
+    u32* col;
+    u32* tag;   // the arena's value array as u32 pairs
+    i64 w, end;
+    u32 c = 0;
+    bool over = false;
+    __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        const int k = __popc(m);
+        if (!over) {
+            if (w + k > end) {
+                over = true;
+            } else {
+                if (hit) {
+                    const i64 at = w + __popc(m & lanemask_lt());
+                    col[at] = pos;
+                    tag[2 * at] = t;
+                }
+                w += k;
+            }
+        }
+        c += k;
+    }
+    __device__ __forceinline__ void sync() {}
+};
+
+// Sink of walk_row that evaluates as it goes (the long-row and two-pass
+// walks): members queue in shared memory and are evaluated 32 at a time.
+template <class Out>
+struct QueueEval {
+    const VVParams& P;
+    int r;
+    u64 a, b;
+    double psr, cut;
+    WarpShared& S;
+    Out& out;
+    int n = 0, head = 0;   // queued members (warp-uniform)
+    __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            int k = head + n + __popc(m & lanemask_lt());
+            if (k >= kRing) k -= kRing;
+            S.hit_pos[k] = pos;
+            S.hit_tag[k] = t;
+        }
+        n += __popc(m);
+    }
+    __device__ __forceinline__ void eval(int cnt) {
+        const int lane = threadIdx.x & 31;
+        Hit e{0.0, 0u, false};
+        if (lane < cnt) {
+            int k = head + lane;
+            if (k >= kRing) k -= kRing;
+            e = eval_hit(P, r, a, b, psr, cut, S.hit_pos[k], S.hit_tag[k]);
+        }
+        out.put(e.keep, e.j, e.h);
+        head += cnt;
+        if (head >= kRing) head -= kRing;
+        n -= cnt;
+    }
+    __device__ __forceinline__ void sync() {
+        if (n >= 32) {
+            __syncwarp();
+            do {
+                eval(32);
+            } while (n >= 32);
+            __syncwarp();
+        }
+    }
+    __device__ __forceinline__ void flush() {
+        sync();
+        if (n) {
+            __syncwarp();
+            eval(n);
+            __syncwarp();
+        }
+    }
+};
+
+// All entries of row r, evaluated in the walk.
+template <class Out>
+__device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, double cut,
+                       WarpShared& S, Out& out, unsigned long long& tests) {
+    QueueEval<Out> q{P, r, a, b, psr, cut, S, out};
+    walk_row(P, r, a, b, S, q, tests);
+    q.flush();
 }
 
 __device__ __forceinline__ void row_setup(const VVParams& P, int r, u64& a, u64& b, double& psr,
@@ -800,9 +875,10 @@ __device__ __forceinline__ int next_row(int* ctr) {
     return __shfl_sync(0xffffffffu, r, 0);
 }
 
-// Single pass: each warp appends its rows to private chunks of the arena.
+// Single pass, first half: each warp appends the members of its rows to
+// private chunks of the arena (k_vv_eval turns them into entries in place).
 template <class Loc>
-__global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
+__global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -817,7 +893,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
             cend = cpos + A.chunk;
         }
     }
-    unsigned long long tests = 0;
+    unsigned long long tests = 0, hits = 0;
     for (;;) {
         const int g = next_row(A.next_row);
         if (g >= nrows) break;
@@ -830,10 +906,13 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
         for (int attempt = 0; attempt < 2; ++attempt) {
-            ChunkOut out{A.acol, A.aval, cpos, cend, cb};
+            HitOut out{A.acol, reinterpret_cast<u32*>(A.aval), cpos, cend};
             unsigned long long tt = 0;
-            vv_row(P, r, a, b, psr, cut, S, out, tt);
-            if (attempt == 0) tests += tt;
+            walk_row(P, r, a, b, S, out, tt);
+            if (attempt == 0) {
+                tests += tt;
+                hits += out.c;
+            }
             if (!out.over) {
                 if (lane == 0) {
                     A.row_pos[g] = cpos;
@@ -850,6 +929,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
             // fall back to the exact two-pass build if the arena runs out.
             if ((i64)out.c > A.restart || attempt == 1) {
                 if (lane == 0) {
+                    A.row_pos[g] = -1;   // k_vv_big places it
                     A.row_len[g] = out.c;
                     A.big[atomicAdd(A.n_big, 1)] = (u32)g;
                 }
@@ -867,11 +947,54 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_arena(Loc L, Arena A) {
         }
         __syncwarp();
     }
-    if (lane == 0) atomicAdd(A.n_test, tests);
+    if (lane == 0) {
+        atomicAdd(A.n_test, tests);
+        if (A.n_hit) atomicAdd(A.n_hit, hits);
+    }
 }
 
-// Rows longer than a chunk: exact contiguous space, second walk.  The count
-// of such rows is read on the device so the launch can sit in a graph.
+// Single pass, second half: the members of every arena row become its
+// entries, in place and in order (entry k is written after member k has
+// been read, at a position <= k).  One warp per row, all lanes evaluating.
+template <class Loc>
+__global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    const i64 nrows = L.rows();
+    if (*(volatile int*)A.overflow) return;
+    const u32* tags = reinterpret_cast<const u32*>(A.aval);
+    for (i64 g = gw; g < nrows; g += nw) {
+        const i64 pos = A.row_pos[g];
+        if (pos < 0) continue;   // a long row
+        const u32 len = A.row_len[g];
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
+        u64 a, b;
+        double psr, cut;
+        row_setup(P, r, a, b, psr, cut);
+        i64 w = pos;
+        for (u32 k0 = 0; k0 < len; k0 += 32) {
+            const u32 k = k0 + lane;
+            Hit e{0.0, 0u, false};
+            if (k < len) e = eval_hit(P, r, a, b, psr, cut, A.acol[pos + k], tags[2 * (pos + k)]);
+            const unsigned m = __ballot_sync(0xffffffffu, e.keep);
+            if (e.keep) {
+                const i64 at = w + __popc(m & lanemask_lt());
+                A.acol[at] = e.j + cb;
+                A.aval[at] = e.h;
+            }
+            w += __popc(m);
+        }
+        if (lane == 0) A.row_len[g] = (u32)(w - pos);
+        __syncwarp();
+    }
+}
+
+// Rows longer than a chunk: contiguous space for their members, second
+// walk evaluating as it goes.  The count of such rows is read on the device
+// so the launch can sit in a graph.
 template <class Loc>
 __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
@@ -901,7 +1024,10 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         ExactOut out{A.acol, A.aval, (i64)base, cb};
         unsigned long long tt = 0;
         vv_row(P, r, a, b, psr, cut, S, out, tt);
-        if (lane == 0) A.row_pos[g] = (i64)base;
+        if (lane == 0) {
+            A.row_pos[g] = (i64)base;
+            A.row_len[g] = out.c;   // members counted, entries kept
+        }
         __syncwarp();
     }
 }
@@ -978,7 +1104,7 @@ i64 g_arena_cap = 0;
 
 namespace {
 
-// Arena entries that always suffice for a matrix of nnz entries built by
+// Arena slots that always suffice for rows of `nnz` members in all built by
 // `grid` blocks (see the restart rule of k_vv_arena).
 i64 arena_bound(i64 nnz, int grid, i64 chunk) {
     return nnz + nnz / 3 + 1 + ((i64)grid * kWS + 1) * chunk;
@@ -996,7 +1122,7 @@ int vv_grid(int device) {
 // the arena is too small.  Returns the number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
-           double* t_gen, double* t_scan, double* t_compact) {
+           double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
@@ -1010,7 +1136,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
     if (g_arena_cap > 0) cap = g_arena_cap;
     DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
-    DBuf<unsigned long long> nt(1, s), cursor(1, s);
+    DBuf<unsigned long long> nt(1, s), cursor(1, s), nh(1, s);
     DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s);
     DBuf<double> aval(cap, s);
     DBuf<i64> rpos(nrows, s);
@@ -1028,7 +1154,9 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.n_big = nbig.p;
     A.next_row = next.p;
     A.n_test = nt.p;
+    A.n_hit = nh.p;
     DNQ_CUDA(cudaMemsetAsync(nt.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(nh.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(ovf.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(nbig.p, 0, 4, s));
@@ -1037,6 +1165,8 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaMemsetAsync(rlen.p + nrows, 0, 4, s));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
     k_vv_arena<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     k_vv_big<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1079,9 +1209,11 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
         DNQ_CHECK_LAUNCH();
     }
     DNQ_CUDA(cudaEventRecord(ev[3], s));
-    unsigned long long tests = 0;
+    unsigned long long tests = 0, hits = 0;
     DNQ_CUDA(cudaMemcpyAsync(&tests, nt.p, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaMemcpyAsync(&hits, nh.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaEventSynchronize(ev[3]));
+    if (hits_out) *hits_out = hov ? std::max<i64>(M.nnz, 2 * cap) : (i64)hits;
     M.sorted = false;
     float ms;
     DNQ_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
@@ -1144,10 +1276,14 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     DNQ_CUDA(cudaEventRecord(e1, s));
     OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
     double tg = 0, tsc = 0, tc = 0;
-    H->candidates = run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc);
+    i64 hits = 0;
+    H->candidates =
+        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits);
     H->vv.nc = n;
+    // the arena holds members before they become entries: size by the larger
+    const long long want = std::max<long long>(H->vv.nnz, hits);
     long long prev = ctx->vv_nnz_hint.load();   // shared by builds on other threads
-    while (prev < H->vv.nnz && !ctx->vv_nnz_hint.compare_exchange_weak(prev, H->vv.nnz)) {
+    while (prev < want && !ctx->vv_nnz_hint.compare_exchange_weak(prev, want)) {
     }
     float ms = 0;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -1291,6 +1427,7 @@ struct dnq_batch_s {
     dnq::DBuf<unsigned long long> nt, cursor;
     dnq::DBuf<dnq::u8> scan_tmp;
     dnq::i64 cap = 0;
+    dnq::i64 hits = 0;   // members of the sizing build (the arena holds members)
     bool planned = false;
     // tunables
     dnq::i64 chunk = dnq::kChunk;
@@ -1346,11 +1483,11 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     // the sizing build fills the batch's CSR itself, so the blocks are
     // valid right after creation
-    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr);
+    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits);
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
-    b->cap = arena_bound(nnz, grid, b->chunk);
+    b->cap = arena_bound(std::max(nnz, b->hits), grid, b->chunk);
     b->acol.alloc(b->cap, s);
     b->aval.alloc(b->cap, s);
     b->rlen.alloc(n + 1, s);
@@ -1393,8 +1530,9 @@ void enqueue_apply(dnq_batch_s* b, int precision, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
 }
 
-// The step on planned buffers: diag, single-pass build, long rows, scan,
-// compaction, FP32 split, H.x, energies.  No allocation, no host sync.
+// The step on planned buffers: diag, single-pass build (members, then their
+// entries), long rows, scan, compaction, FP32 split, H.x, energies.  No
+// allocation, no host sync.
 void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev = nullptr) {
     auto mark = [&](int k) {
         if (ev) DNQ_CUDA(cudaEventRecord(ev[k], s));
@@ -1428,6 +1566,8 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CUDA(cudaMemsetAsync(b->bad.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
     k_vv_arena<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     k_vv_big<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1617,7 +1757,7 @@ int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg4) {
     upload_params(b, nullptr);
     if (resize) {   // larger chunks need a larger arena
         const int grid = vv_grid<ManySys>(b->device);
-        b->cap = arena_bound(b->M.nnz, grid, b->chunk);
+        b->cap = arena_bound(std::max(b->M.nnz, b->hits), grid, b->chunk);
         b->acol.alloc(b->cap, nullptr);
         b->aval.alloc(b->cap, nullptr);
         DNQ_CUDA(cudaStreamSynchronize(nullptr));
