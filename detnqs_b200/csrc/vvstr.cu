@@ -458,7 +458,11 @@ struct WarpShared {
     u8 occa[64], vira[64], occb[64], virb[64];
     u32 bs_id[kBS];            // beta group of each indexed beta single of the row
     u16 bs_hp[kBS];            // its excitation, hole | particle << 8
-    u32 hit_pos[kRing], hit_tag[kRing];   // members awaiting evaluation (fallback walks)
+};
+
+// Members awaiting evaluation in the walks that evaluate as they go.
+struct HitRing {
+    u32 pos[kRing], tag[kRing];
 };
 
 // Occupied and virtual orbital lists of both strings, one lane per orbital.
@@ -803,7 +807,7 @@ struct QueueEval {
     int r;
     u64 a, b;
     double psr, cut;
-    WarpShared& S;
+    HitRing& Q;
     Out& out;
     int n = 0, head = 0;   // queued members (warp-uniform)
     __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
@@ -811,8 +815,8 @@ struct QueueEval {
         if (hit) {
             int k = head + n + __popc(m & lanemask_lt());
             if (k >= kRing) k -= kRing;
-            S.hit_pos[k] = pos;
-            S.hit_tag[k] = t;
+            Q.pos[k] = pos;
+            Q.tag[k] = t;
         }
         n += __popc(m);
     }
@@ -822,7 +826,7 @@ struct QueueEval {
         if (lane < cnt) {
             int k = head + lane;
             if (k >= kRing) k -= kRing;
-            e = eval_hit(P, r, a, b, psr, cut, S.hit_pos[k], S.hit_tag[k]);
+            e = eval_hit(P, r, a, b, psr, cut, Q.pos[k], Q.tag[k]);
         }
         out.put(e.keep, e.j, e.h);
         head += cnt;
@@ -851,8 +855,8 @@ struct QueueEval {
 // All entries of row r, evaluated in the walk.
 template <class Out>
 __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, double cut,
-                       WarpShared& S, Out& out, unsigned long long& tests) {
-    QueueEval<Out> q{P, r, a, b, psr, cut, S, out};
+                       WarpShared& S, HitRing& ring, Out& out, unsigned long long& tests) {
+    QueueEval<Out> q{P, r, a, b, psr, cut, ring, out};
     walk_row(P, r, a, b, S, q, tests);
     q.flush();
 }
@@ -954,8 +958,9 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
 }
 
 // Single pass, second half: the members of every arena row become its
-// entries, in place and in order (entry k is written after member k has
-// been read, at a position <= k).  One warp per row, all lanes evaluating.
+// entries, in place and in order (a step reads its 64 members before it
+// writes, and writes only at positions below the next step's).  One warp
+// per row, all lanes evaluating.
 template <class Loc>
 __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
     const int lane = threadIdx.x & 31;
@@ -975,15 +980,32 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
         i64 w = pos;
-        for (u32 k0 = 0; k0 < len; k0 += 32) {
-            const u32 k = k0 + lane;
-            Hit e{0.0, 0u, false};
-            if (k < len) e = eval_hit(P, r, a, b, psr, cut, A.acol[pos + k], tags[2 * (pos + k)]);
-            const unsigned m = __ballot_sync(0xffffffffu, e.keep);
-            if (e.keep) {
+        for (u32 k0 = 0; k0 < len; k0 += 64) {   // two members per lane in flight
+            const u32 k1 = k0 + lane, k2 = k1 + 32;
+            u32 p1 = 0, t1 = 0, p2 = 0, t2 = 0;
+            if (k1 < len) {
+                p1 = A.acol[pos + k1];
+                t1 = tags[2 * (pos + k1)];
+            }
+            if (k2 < len) {
+                p2 = A.acol[pos + k2];
+                t2 = tags[2 * (pos + k2)];
+            }
+            Hit e1{0.0, 0u, false}, e2{0.0, 0u, false};
+            if (k1 < len) e1 = eval_hit(P, r, a, b, psr, cut, p1, t1);
+            if (k2 < len) e2 = eval_hit(P, r, a, b, psr, cut, p2, t2);
+            unsigned m = __ballot_sync(0xffffffffu, e1.keep);
+            if (e1.keep) {
                 const i64 at = w + __popc(m & lanemask_lt());
-                A.acol[at] = e.j + cb;
-                A.aval[at] = e.h;
+                A.acol[at] = e1.j + cb;
+                A.aval[at] = e1.h;
+            }
+            w += __popc(m);
+            m = __ballot_sync(0xffffffffu, e2.keep);
+            if (e2.keep) {
+                const i64 at = w + __popc(m & lanemask_lt());
+                A.acol[at] = e2.j + cb;
+                A.aval[at] = e2.h;
             }
             w += __popc(m);
         }
@@ -998,7 +1020,9 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
 template <class Loc>
 __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
+    __shared__ HitRing rings[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
+    HitRing& R = rings[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -1023,7 +1047,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         load_lists(S, a, b, P.n_orb);
         ExactOut out{A.acol, A.aval, (i64)base, cb};
         unsigned long long tt = 0;
-        vv_row(P, r, a, b, psr, cut, S, out, tt);
+        vv_row(P, r, a, b, psr, cut, S, R, out, tt);
         if (lane == 0) {
             A.row_pos[g] = (i64)base;
             A.row_len[g] = out.c;   // members counted, entries kept
@@ -1045,9 +1069,25 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
     }
     for (i64 r = gw; r < n; r += nw) {
         const i64 src = row_pos[r], dst = rowptr[r], len = rowptr[r + 1] - dst;
-        for (i64 t = lane; t < len; t += 32) {
-            col[dst + t] = acol[src + t];
-            val[dst + t] = aval[src + t];
+        for (i64 t0 = 0; t0 < len; t0 += 128) {   // four loads per lane before the stores
+            u32 c[4];
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const i64 t = t0 + 32 * u + lane;
+                if (t < len) {
+                    c[u] = acol[src + t];
+                    v[u] = aval[src + t];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const i64 t = t0 + 32 * u + lane;
+                if (t < len) {
+                    col[dst + t] = c[u];
+                    val[dst + t] = v[u];
+                }
+            }
         }
     }
 }
@@ -1056,7 +1096,9 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
 template <class Loc, bool FILL>
 __global__ void __launch_bounds__(kWS * 32) k_vv_twopass(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
+    __shared__ HitRing rings[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
+    HitRing& R = rings[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const i64 nrows = L.rows();
     for (;;) {
@@ -1072,11 +1114,11 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_twopass(Loc L, Arena A) {
         unsigned long long tt = 0;
         if (!FILL) {
             CountOut out;
-            vv_row(P, r, a, b, psr, cut, S, out, tt);
+            vv_row(P, r, a, b, psr, cut, S, R, out, tt);
             if (lane == 0) A.cnt[g] = out.c;
         } else {
             ExactOut out{A.col, A.val, A.off[g], cb};
-            vv_row(P, r, a, b, psr, cut, S, out, tt);
+            vv_row(P, r, a, b, psr, cut, S, R, out, tt);
         }
         __syncwarp();
     }
