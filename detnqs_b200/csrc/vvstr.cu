@@ -60,6 +60,7 @@ struct StrMapView {
 
 struct StrIndex {
     DBuf<u64> other;     // sorted companion string (alpha for beta groups, ...)
+    DBuf<u32> other32;   // the same in 32 bits (indices of systems with n_orb <= 32)
     DBuf<u32> idx;       // original position in V
     DBuf<u32> gid;       // group number of every sorted position
     DBuf<u32> gstart;    // first sorted position of every group
@@ -187,6 +188,20 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s
     DNQ_CHECK_LAUNCH();
 }
 
+__global__ void k_narrow(const u64* x, i64 n, u32* y) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        y[t] = (u32)x[t];
+}
+
+// 32-bit companion strings for scans (every string below orbital 32).
+void narrow_index(StrIndex& X, i64 n, cudaStream_t s) {
+    if (n == 0) return;
+    X.other32.alloc(n, s);
+    k_narrow<<<gsz(n), 256, 0, s>>>(X.other.p, n, X.other32.p);
+    DNQ_CHECK_LAUNCH();
+}
+
 constexpr u32 kPresMin = 128;                    // presence rows for alpha groups longer than this
 constexpr i64 kPresBytes = 256ll << 20;          // cap on the presence rows of one index
 
@@ -303,6 +318,8 @@ struct VVParams {
     const u32* a_idx;
     const u64* b_other;     // alpha of the beta-sorted entries
     const u32* b_idx;
+    const u32* a_other32;   // the same as u32 when n_orb <= 32 (else null)
+    const u32* b_other32;
     const double* diag;
     int policy;
     double eps1;
@@ -526,12 +543,31 @@ __device__ __forceinline__ Hit eval_hit(const VVParams& P, int r, u64 a, u64 b, 
     return e;
 }
 
+// Scans read the companion strings as W: u32 when every string fits in 32
+// orbitals (half the bytes, one xor and popcount per test), else u64.
+__device__ __forceinline__ int popc_w(u32 x) { return __popc(x); }
+__device__ __forceinline__ int popc_w(u64 x) { return __popcll(x); }
+template <class W> __device__ __forceinline__ const W* a_others(const VVParams& P);
+template <class W> __device__ __forceinline__ const W* b_others(const VVParams& P);
+template <> __device__ __forceinline__ const u64* a_others<u64>(const VVParams& P) {
+    return P.a_other;
+}
+template <> __device__ __forceinline__ const u64* b_others<u64>(const VVParams& P) {
+    return P.b_other;
+}
+template <> __device__ __forceinline__ const u32* a_others<u32>(const VVParams& P) {
+    return P.a_other32;
+}
+template <> __device__ __forceinline__ const u32* b_others<u32>(const VVParams& P) {
+    return P.b_other32;
+}
+
 // Part C over the short groups of one round of 32 alpha singles, packed:
 // the members of all of them are numbered in group order and each step
 // tests 32 consecutive members; a lane finds its member's group by a
 // five-step search of the exclusive prefix of the group lengths.
-template <class Q>
-__device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const u64* a_other, u64 b,
+template <class W, class Q>
+__device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_other, W b,
                                               unsigned long long& tests, u32 gs, u32 sl, int hh,
                                               int pp) {
     const int lane = threadIdx.x & 31;
@@ -551,7 +587,7 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const u64* a_
     tests += total;
     for (u32 t0 = 0; t0 < total; t0 += 32 * kScanU) {
         u32 at[kScanU], tag[kScanU];
-        u64 y[kScanU];
+        W y[kScanU];
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             const u32 m = t0 + 32 * u + lane;
@@ -571,7 +607,7 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const u64* a_
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             if (t0 + 32 * u >= total) break;
-            q.push(__popcll(b ^ y[u]) == 2, at[u], tag[u]);
+            q.push(popc_w(b ^ y[u]) == 2, at[u], tag[u]);
         }
         q.sync();
     }
@@ -580,12 +616,11 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const u64* a_
 
 // Parts A and B: the members of one group [st, st + ln) whose string differs
 // from x in 2 or 4 orbitals.
-template <class Q>
-__device__ __forceinline__ void scan_same(Q& q, const u64* other, u64 x, u32 st, u32 ln,
-                                          u32 kind) {
+template <class W, class Q>
+__device__ __forceinline__ void scan_same(Q& q, const W* other, W x, u32 st, u32 ln, u32 kind) {
     const int lane = threadIdx.x & 31;
     for (u32 t0 = 0; t0 < ln; t0 += 32 * kScanU) {
-        u64 y[kScanU];
+        W y[kScanU];
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             const u32 t = t0 + 32 * u + lane;
@@ -594,7 +629,7 @@ __device__ __forceinline__ void scan_same(Q& q, const u64* other, u64 x, u32 st,
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             if (t0 + 32 * u >= ln) break;
-            const int dd = __popcll(x ^ y[u]);
+            const int dd = popc_w(x ^ y[u]);
             q.push(dd == 2 || dd == 4, st + t0 + 32 * u + lane, kind);
         }
         q.sync();
@@ -604,10 +639,12 @@ __device__ __forceinline__ void scan_same(Q& q, const u64* other, u64 x, u32 st,
 // The members of row r = (a, b) in their fixed order: the diagonal, then
 // parts A, B and C.  q.push(hit, position, tag) is warp-collective, once
 // per step of 32; q.sync() follows every group of at most kScanU steps.
-template <class Q>
+template <class W, class Q>
 __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b, WarpShared& S,
                                          Q& q, unsigned long long& tests) {
     const int lane = threadIdx.x & 31;
+    const W* ao = a_others<W>(P);
+    const W aw = (W)a, bw = (W)b;
     const u64 all = low_mask(P.n_orb);
     q.push(lane == 0, (u32)r, kHitD);
     // ---- part A: same beta string (alpha singles and doubles)
@@ -616,13 +653,13 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     st = __shfl_sync(0xffffffffu, st, 0);
     ln = __shfl_sync(0xffffffffu, ln, 0);
     tests += ln;
-    scan_same(q, P.b_other, a, st, ln, kHitA);
+    scan_same(q, b_others<W>(P), aw, st, ln, kHitA);
     // ---- part B: same alpha string (beta singles and doubles)
     if (lane == 0 && !P.amap.find(a, st, ln)) ln = 0;
     st = __shfl_sync(0xffffffffu, st, 0);
     ln = __shfl_sync(0xffffffffu, ln, 0);
     tests += ln;
-    scan_same(q, P.a_other, b, st, ln, kHitB);
+    scan_same(q, ao, bw, st, ln, kHitB);
     // ---- part C: alpha single x beta single, via the groups of the a'
     const int na = __popcll(a), nva = __popcll(~a & all);
     const int nsa = na * nva;
@@ -645,7 +682,7 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
         const bool big = !pbig && gl > P.big_group;
         const bool small = gl != 0 && !pbig && !big;
         if (!P.c_groupwalk) {
-            part_c_packed(q, S, P.a_other, b, tests, gs, small ? gl : 0u, hh, pp);
+            part_c_packed(q, S, ao, bw, tests, gs, small ? gl : 0u, hh, pp);
         } else {
             // one group at a time: start, length and the alpha excitation are
             // warp-uniform, members in order 32 per step
@@ -659,16 +696,16 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
                                 ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
                 tests += gn;
                 for (u32 t0 = 0; t0 < gn; t0 += 32 * kScanU) {
-                    u64 y[kScanU];
+                    W y[kScanU];
 #pragma unroll
                     for (int u = 0; u < kScanU; ++u) {
                         const u32 t = t0 + 32 * u + lane;
-                        y[u] = t < gn ? __ldg(&P.a_other[g0 + t]) : b;
+                        y[u] = t < gn ? __ldg(&ao[g0 + t]) : bw;
                     }
 #pragma unroll
                     for (int u = 0; u < kScanU; ++u) {
                         if (t0 + 32 * u >= gn) break;
-                        q.push(__popcll(b ^ y[u]) == 2, g0 + t0 + 32 * u + lane, tag);
+                        q.push(popc_w(bw ^ y[u]) == 2, g0 + t0 + 32 * u + lane, tag);
                     }
                     q.sync();
                 }
@@ -781,6 +818,7 @@ struct HitOut {
     bool over = false;
     __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
         const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (m == 0) return;   // most steps find nothing
         const int k = __popc(m);
         if (!over) {
             if (w + k > end) {
@@ -857,7 +895,7 @@ template <class Out>
 __device__ void vv_row(const VVParams& P, int r, u64 a, u64 b, double psr, double cut,
                        WarpShared& S, HitRing& ring, Out& out, unsigned long long& tests) {
     QueueEval<Out> q{P, r, a, b, psr, cut, ring, out};
-    walk_row(P, r, a, b, S, q, tests);
+    walk_row<u64>(P, r, a, b, S, q, tests);
     q.flush();
 }
 
@@ -881,7 +919,7 @@ __device__ __forceinline__ int next_row(int* ctr) {
 
 // Single pass, first half: each warp appends the members of its rows to
 // private chunks of the arena (k_vv_eval turns them into entries in place).
-template <class Loc>
+template <class Loc, class W>
 __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
@@ -912,7 +950,7 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         for (int attempt = 0; attempt < 2; ++attempt) {
             HitOut out{A.acol, reinterpret_cast<u32*>(A.aval), cpos, cend};
             unsigned long long tt = 0;
-            walk_row(P, r, a, b, S, out, tt);
+            walk_row<W>(P, r, a, b, S, out, tt);
             if (attempt == 0) {
                 tests += tt;
                 hits += out.c;
@@ -1155,7 +1193,8 @@ i64 arena_bound(i64 nnz, int grid, i64 chunk) {
 template <class Loc>
 int vv_grid(int device) {
     int per_sm = 0;
-    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vv_arena<Loc>, kWS * 32, 0));
+    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vv_arena<Loc, u64>,
+                                                           kWS * 32, 0));
     return std::max(1, per_sm) * sm_count(device);
 }
 
@@ -1164,7 +1203,8 @@ int vv_grid(int device) {
 // the arena is too small.  Returns the number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
-           double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr) {
+           double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr,
+           bool narrow = false) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
@@ -1172,7 +1212,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     size_t freeb = 0, totb = 0;
     DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
     const i64 chunk = g_arena_chunk > 0 ? g_arena_chunk : kChunk;
-    i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 256 * nrows;
+    i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 512 * nrows;
     want += warps * chunk;
     const i64 maxfit = (i64)(freeb / 2 / 12);
     i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
@@ -1206,7 +1246,8 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaMemsetAsync(cursor.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(rlen.p + nrows, 0, 4, s));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
-    k_vv_arena<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    if (narrow) k_vv_arena<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_arena<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1282,6 +1323,8 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
     P.a_other = A.other.p;
     P.a_idx = A.idx.p;
     P.b_other = B.other.p;
+    P.a_other32 = A.other32.p;
+    P.b_other32 = B.other32.p;
     P.b_idx = B.idx.p;
     P.diag = diag;
     P.policy = policy;
@@ -1315,12 +1358,17 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     build_str_index(A, V, n, 0, s);
     build_str_index(B, V, n, 1, s);
     build_presence(A, B, n, s);
+    const bool narrow = n_orb <= 32;
+    if (narrow) {
+        narrow_index(A, n, s);
+        narrow_index(B, n, s);
+    }
     DNQ_CUDA(cudaEventRecord(e1, s));
     OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
     double tg = 0, tsc = 0, tc = 0;
     i64 hits = 0;
     H->candidates =
-        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits);
+        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits, narrow);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);
@@ -1470,6 +1518,7 @@ struct dnq_batch_s {
     dnq::DBuf<dnq::u8> scan_tmp;
     dnq::i64 cap = 0;
     dnq::i64 hits = 0;   // members of the sizing build (the arena holds members)
+    bool narrow = false;   // every system has n_orb <= 32 (32-bit scans)
     bool planned = false;
     // tunables
     dnq::i64 chunk = dnq::kChunk;
@@ -1525,7 +1574,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     // the sizing build fills the batch's CSR itself, so the blocks are
     // valid right after creation
-    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits);
+    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits, b->narrow);
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
@@ -1607,7 +1656,8 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CUDA(cudaMemsetAsync(b->cursor.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(b->bad.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
-    k_vv_arena<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    if (b->narrow) k_vv_arena<ManySys, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_arena<ManySys, u64><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1736,6 +1786,7 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
     b->V.resize(n_sys);
     b->A.resize(n_sys);
     b->B.resize(n_sys);
+    b->narrow = std::all_of(n_orb, n_orb + n_sys, [](int o) { return o <= 32; });
     for (int k = 0; k < n_sys; ++k) {
         const i64 n = n_dets[k];
         b->V[k].alloc(2 * n, s);
@@ -1746,6 +1797,10 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         build_str_index(b->A[k], b->V[k].p, n, 0, s);
         build_str_index(b->B[k], b->V[k].p, n, 1, s);
         build_presence(b->A[k], b->B[k], n, s);
+        if (b->narrow) {
+            narrow_index(b->A[k], n, s);
+            narrow_index(b->B[k], n, s);
+        }
         const double cut = (policy == DNQ_POLICY_STATIC && use_heatbath)
                                ? hb_cutoff(ctxs[k], eps1) : full_cutoff();
         hp[k] = make_params(ctxs[k], b->V[k].p, n, n_orb[k], policy, eps1, cut, nullptr,

@@ -338,17 +338,23 @@ def test_edge_cases(core, gctx, golden_small):
 
 @pytest.mark.parametrize("policy,use_hb,eps", [(0, False, 0.0), (1, True, 1e-6), (1, True, 1e-3),
                                                (1, False, 1e-6), (2, True, 1e-6)])
-def test_string_groups_match_candidate_walk(core, policy, use_hb, eps):
-    """V->V-only builds take the string-group matcher; the candidate walk
-    (forced by DNQ_OPT_FORCE_WALK) must give the identical block."""
+@pytest.mark.parametrize("n_orb", [20, 40])
+def test_string_groups_match_candidate_walk(core, policy, use_hb, eps, n_orb):
+    """V->V-only builds take the string-group matcher (32-bit scans at 20
+    orbitals, 64-bit at 40); the candidate walk (forced by
+    DNQ_OPT_FORCE_WALK) must give the identical block."""
     from detnqs_b200 import device as D
     from detnqs_b200 import native as N
-    sysm = S.make_system(20, 7, 6, 40, 17)
-    V = S.heat_bath_sample(sysm, 30000, 9)
+    if n_orb == 20:
+        sysm = S.make_system(20, 7, 6, 40, 17)
+        V = S.heat_bath_sample(sysm, 30000, 9)
+    else:
+        sysm = S.make_system(40, 8, 8, 80, 19)
+        V = S.heat_bath_sample(sysm, 15000, 11)
     psi = S.normalized_psi(len(V), 4)
-    ctx = core.IntCtx.from_arrays(20, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx = core.IntCtx.from_arrays(n_orb, sysm.h1e, sysm.eri, sysm.e_core)
     ctx.hb_prepare(1e-15)
-    kw = dict(n_orb=20, policy=policy, use_heatbath=use_hb, eps1=eps, want_vp=False,
+    kw = dict(n_orb=n_orb, policy=policy, use_heatbath=use_hb, eps1=eps, want_vp=False,
               psi=psi if policy == 2 else None)
     A = D.build(ctx, V, **kw)
     N.check(N.lib.dnq_set_option(1, 1))
