@@ -807,12 +807,11 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     }
 }
 
-// Sink of walk_row that records the members only: (position, tag) pairs
-// appended to [w, end) of an arena chunk (col holds the position, the low
-// word of the value slot the tag); past the end it only counts.
+// Sink of walk_row that records the members only: position | tag << 32 in
+// the value slots [w, end) of an arena chunk (whole 8-byte words, so no
+// partial-sector writes); past the end it only counts.
 struct HitOut {
-    u32* col;
-    u32* tag;   // the arena's value array as u32 pairs
+    u64* mem;   // the arena's value array as u64
     i64 w, end;
     u32 c = 0;
     bool over = false;
@@ -826,8 +825,7 @@ struct HitOut {
             } else {
                 if (hit) {
                     const i64 at = w + __popc(m & lanemask_lt());
-                    col[at] = pos;
-                    tag[2 * at] = t;
+                    mem[at] = (u64)pos | ((u64)t << 32);
                 }
                 w += k;
             }
@@ -948,7 +946,7 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
         for (int attempt = 0; attempt < 2; ++attempt) {
-            HitOut out{A.acol, reinterpret_cast<u32*>(A.aval), cpos, cend};
+            HitOut out{reinterpret_cast<u64*>(A.aval), cpos, cend};
             unsigned long long tt = 0;
             walk_row<W>(P, r, a, b, S, out, tt);
             if (attempt == 0) {
@@ -1006,7 +1004,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
     const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
     const i64 nrows = L.rows();
     if (*(volatile int*)A.overflow) return;
-    const u32* tags = reinterpret_cast<const u32*>(A.aval);
+    const u64* mem = reinterpret_cast<const u64*>(A.aval);
     for (i64 g = gw; g < nrows; g += nw) {
         const i64 pos = A.row_pos[g];
         if (pos < 0) continue;   // a long row
@@ -1020,15 +1018,9 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
         i64 w = pos;
         for (u32 k0 = 0; k0 < len; k0 += 64) {   // two members per lane in flight
             const u32 k1 = k0 + lane, k2 = k1 + 32;
-            u32 p1 = 0, t1 = 0, p2 = 0, t2 = 0;
-            if (k1 < len) {
-                p1 = A.acol[pos + k1];
-                t1 = tags[2 * (pos + k1)];
-            }
-            if (k2 < len) {
-                p2 = A.acol[pos + k2];
-                t2 = tags[2 * (pos + k2)];
-            }
+            const u64 m1 = k1 < len ? mem[pos + k1] : 0ull;
+            const u64 m2 = k2 < len ? mem[pos + k2] : 0ull;
+            const u32 p1 = (u32)m1, t1 = (u32)(m1 >> 32), p2 = (u32)m2, t2 = (u32)(m2 >> 32);
             Hit e1{0.0, 0u, false}, e2{0.0, 0u, false};
             if (k1 < len) e1 = eval_hit(P, r, a, b, psr, cut, p1, t1);
             if (k2 < len) e2 = eval_hit(P, r, a, b, psr, cut, p2, t2);
