@@ -351,6 +351,7 @@ struct Arena {
     i64* row_pos;
     u32* row_len;
     u32* big;                         // rows longer than one chunk
+    u32* big_len;                     // their member counts
     int* n_big;
     int* next_row;
     unsigned long long* n_test;
@@ -394,6 +395,10 @@ struct ManySys {
 };
 
 constexpr i64 kChunk = 8192;   // default arena entries per warp chunk
+// row_pos of a long row carries this bit: its slots hold entries and holes
+// (column kHole) until k_vv_compact_long gathers them.
+constexpr i64 kLongRow = 1ll << 62;
+constexpr u32 kHole = 0xffffffffu;
 
 // Warp-collective sinks of one row's entries (columns offset by `base`).
 struct CountOut {
@@ -1044,15 +1049,14 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
     }
 }
 
-// Rows longer than a chunk: contiguous space for their members, second
-// walk evaluating as it goes.  The count of such rows is read on the device
-// so the launch can sit in a graph.
-template <class Loc>
+// Rows longer than a chunk: exact contiguous space and a second walk that
+// records their members there (one warp per row; the walk is cheap next to
+// the evaluation, which k_vv_eval_long spreads over the whole grid).  The
+// count of such rows is read on the device so the launch can sit in a graph.
+template <class Loc, class W>
 __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
-    __shared__ HitRing rings[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
-    HitRing& R = rings[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -1075,14 +1079,101 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
-        ExactOut out{A.acol, A.aval, (i64)base, cb};
+        HitOut out{reinterpret_cast<u64*>(A.aval), (i64)base, (i64)base + len};
         unsigned long long tt = 0;
-        vv_row(P, r, a, b, psr, cut, S, R, out, tt);
+        walk_row<W>(P, r, a, b, S, out, tt);
         if (lane == 0) {
-            A.row_pos[g] = (i64)base;
-            A.row_len[g] = out.c;   // members counted, entries kept
+            A.row_pos[g] = (i64)base | kLongRow;
+            A.big_len[i] = len;
+            A.row_len[g] = 0;   // entries kept, summed by k_vv_eval_long
         }
         __syncwarp();
+    }
+}
+
+// The members of the long rows become entries in place, 64 per warp step
+// over the whole grid; a dropped member leaves a hole.  The 64-member units
+// of all long rows are dealt round-robin to the warps as one sequence (unit
+// u of row i goes to warp (units before row i + u) mod warps).  Kept counts
+// are summed into row_len.
+template <class Loc>
+__global__ void __launch_bounds__(kWS * 32) k_vv_eval_long(Loc L, Arena A) {
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    const int nbig = *A.n_big;
+    if (*(volatile int*)A.overflow) return;
+    const u64* mem = reinterpret_cast<const u64*>(A.aval);
+    i64 off = 0;   // units of the rows before row i, mod nw
+    for (int i = 0; i < nbig; ++i) {
+        const int g = (int)A.big[i];
+        const i64 len = A.big_len[i];
+        const i64 units = (len + 63) / 64;
+        const i64 u0 = (gw - off + nw) % nw;   // this warp's first unit of row i
+        off = (off + units) % nw;
+        if (u0 >= units) continue;
+        const i64 pos = A.row_pos[g] & ~kLongRow;
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(g, r, cb);
+        u64 a, b;
+        double psr, cut;
+        row_setup(P, r, a, b, psr, cut);
+        u32 kept = 0;
+        for (i64 k0 = u0 * 64; k0 < len; k0 += nw * 64) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const i64 k = k0 + 32 * h + lane;
+                bool keep = false;
+                if (k < len) {
+                    const u64 m = mem[pos + k];
+                    const Hit e = eval_hit(P, r, a, b, psr, cut, (u32)m, (u32)(m >> 32));
+                    keep = e.keep;
+                    A.acol[pos + k] = e.keep ? e.j + cb : kHole;
+                    A.aval[pos + k] = e.h;
+                }
+                kept += __popc(__ballot_sync(0xffffffffu, keep));
+            }
+        }
+        if (lane == 0 && kept) atomicAdd(&A.row_len[g], kept);
+    }
+}
+
+// Ordered gather of the long rows (block per row): holes dropped.
+__global__ void __launch_bounds__(256) k_vv_compact_long(const u32* big, const u32* big_len,
+                                                         const int* n_big, const i64* row_pos,
+                                                         const i64* rowptr, i64 n,
+                                                         const u32* acol, const double* aval,
+                                                         u32* col, double* val, i64 cap) {
+    __shared__ u32 wsum[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (rowptr[n] > cap) return;   // a stale plan (k_vv_compact raises the flag)
+    const int nbig = *n_big;
+    for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
+        const u32 g = big[i];
+        const i64 src = row_pos[g] & ~kLongRow, dst = rowptr[g];
+        const i64 len = big_len[i];
+        i64 carry = 0;
+        for (i64 t0 = 0; t0 < len; t0 += 256) {
+            const i64 t = t0 + threadIdx.x;
+            const u32 c = t < len ? acol[src + t] : kHole;
+            const bool keep = c != kHole;
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) wsum[wid] = __popc(m);
+            __syncthreads();
+            u32 before = 0, total = 0;
+            for (int w = 0; w < 8; ++w) {
+                if (w < wid) before += wsum[w];
+                total += wsum[w];
+            }
+            if (keep) {
+                const i64 at = dst + carry + before + __popc(m & lanemask_lt());
+                col[at] = c;
+                val[at] = aval[src + t];
+            }
+            carry += total;
+            __syncthreads();
+        }
     }
 }
 
@@ -1099,6 +1190,7 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
     }
     for (i64 r = gw; r < n; r += nw) {
         const i64 src = row_pos[r], dst = rowptr[r], len = rowptr[r + 1] - dst;
+        if (src & kLongRow) continue;   // k_vv_compact_long
         for (i64 t0 = 0; t0 < len; t0 += 128) {   // four loads per lane before the stores
             u32 c[4];
             double v[4];
@@ -1211,7 +1303,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     if (g_arena_cap > 0) cap = g_arena_cap;
     DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
     DBuf<unsigned long long> nt(1, s), cursor(1, s), nh(1, s);
-    DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s);
+    DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s), blen(nrows, s);
     DBuf<double> aval(cap, s);
     DBuf<i64> rpos(nrows, s);
     Arena A{};
@@ -1225,6 +1317,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.row_pos = rpos.p;
     A.row_len = rlen.p;
     A.big = big.p;
+    A.big_len = blen.p;
     A.n_big = nbig.p;
     A.next_row = next.p;
     A.n_test = nt.p;
@@ -1243,7 +1336,10 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CHECK_LAUNCH();
     k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    k_vv_big<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    if (narrow) k_vv_big<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_big<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_eval_long<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     int hov = 0;
     DNQ_CUDA(cudaMemcpyAsync(&hov, ovf.p, 4, cudaMemcpyDeviceToHost, s));
@@ -1260,6 +1356,9 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
         DNQ_CUDA(cudaEventRecord(ev[2], s));
         k_vv_compact<<<grid, kWS * 32, 0, s>>>(rpos.p, M.rowptr.p, nrows, acol.p, aval.p, M.col.p,
                                                M.val.p, M.nnz, bad.p);
+        DNQ_CHECK_LAUNCH();
+        k_vv_compact_long<<<grid, 256, 0, s>>>(big.p, blen.p, nbig.p, rpos.p, M.rowptr.p, nrows,
+                                               acol.p, aval.p, M.col.p, M.val.p, M.nnz);
         DNQ_CHECK_LAUNCH();
     } else {
         acol.release();
@@ -1502,7 +1601,7 @@ struct dnq_batch_s {
     dnq::DBuf<double> diag_op;
     dnq::Csr M;
     // planned arena (fixed sizes for graph replays)
-    dnq::DBuf<dnq::u32> acol, rlen, big;
+    dnq::DBuf<dnq::u32> acol, rlen, big, blen;
     dnq::DBuf<double> aval;
     dnq::DBuf<dnq::i64> rpos;
     dnq::DBuf<int> next, ovf, nbig, bad;
@@ -1575,6 +1674,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->aval.alloc(b->cap, s);
     b->rlen.alloc(n + 1, s);
     b->big.alloc(n, s);
+    b->blen.alloc(n, s);
     b->rpos.alloc(n, s);
     b->next.alloc(1, s);
     b->ovf.alloc(1, s);
@@ -1635,6 +1735,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     A.row_pos = b->rpos.p;
     A.row_len = b->rlen.p;
     A.big = b->big.p;
+    A.big_len = b->blen.p;
     A.n_big = b->nbig.p;
     A.next_row = b->next.p;
     A.n_test = b->nt.p;
@@ -1653,7 +1754,10 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CHECK_LAUNCH();
     k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    k_vv_big<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    if (b->narrow) k_vv_big<ManySys, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_big<ManySys, u64><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+    k_vv_eval_long<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     mark(2);
     size_t bytes = b->scan_tmp.n;
@@ -1663,6 +1767,10 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CHECK_LAUNCH();
     k_vv_compact<<<grid, kWS * 32, 0, s>>>(b->rpos.p, b->M.rowptr.p, n, b->acol.p, b->aval.p,
                                            b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p);
+    DNQ_CHECK_LAUNCH();
+    k_vv_compact_long<<<grid, 256, 0, s>>>(b->big.p, b->blen.p, b->nbig.p, b->rpos.p,
+                                           b->M.rowptr.p, n, b->acol.p, b->aval.p, b->M.col.p,
+                                           b->M.val.p, b->M.nnz);
     DNQ_CHECK_LAUNCH();
     if (precision == DNQ_F32) launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
     mark(3);
