@@ -761,7 +761,12 @@ def run_serving(args, rank: int, world: int):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    # warm-up: one small system through both paths (kernels, pools, threads)
+    # warm-up: every system built once (its context then sizes later builds
+    # as the plain path's will be), and one small system through both paths
+    for k, (sysm, d) in enumerate(systems):
+        H = device.build(ctxs[k], d, n_orb=sysm.n_orb, policy=native.POLICY_STATIC,
+                         use_heatbath=True, eps1=1e-7, want_vp=False)
+        H.close()
     small = int(np.argmin([len(d) for _, d in systems]))
     for _ in range(max(1, args.warmup)):
         with V.Server(device=local, budget_bytes=SERVE_BUDGET, build_slots=4) as srv:
@@ -1183,7 +1188,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--df-dets", type=int, default=DF_S,
                     help="size of S for --workload downfold (a smaller S for profiling)")
-    ap.add_argument("--serve-slots", type=int, default=4,
+    ap.add_argument("--serve-slots", type=int, default=2,
                     help="build worker streams of the served path")
     ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold"],
                     default="single",

@@ -236,11 +236,17 @@ void upload_tables(dnq_ctx_s* c) {
 // Keep memory freed by cudaFreeAsync in the device's default pool instead
 // of returning it to the driver at every synchronisation: repeated builds
 // then reuse the same pages (process-local runtime setting).
+// The device's stream-ordered pool keeps what it has mapped (no release at
+// synchronisation), and an allocation never waits on another stream's work
+// to reuse memory that stream freed: builds and local-energy groups run on
+// separate streams, and such hidden waits chained them into each other.
 void keep_pool(int device) {
     cudaMemPool_t pool;
     DNQ_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t thr = ~0ull;
     DNQ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    int no = 0;
+    DNQ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
 }
 
 namespace {

@@ -121,22 +121,26 @@ __global__ void k_group_energy(const EnergyDesc* d, double* out2) {
     }
 }
 
-// Pinned host buffer that only grows.
+// Pinned host buffer that only grows, at least doubling each time.  A
+// replaced buffer is kept until the server closes: cudaFreeHost waits for
+// the whole device, which would stall every build in flight.
 template <class T>
 struct Pinned {
     T* p = nullptr;
     size_t n = 0;
+    std::vector<T*> retired;
     void need(size_t count) {
         if (count <= n) return;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        n = 0;
-        DNQ_CUDA(cudaHostAlloc((void**)&p, std::max<size_t>(count, 1) * sizeof(T),
-                               cudaHostAllocDefault));
-        n = count;
+        const size_t want = std::max<size_t>(std::max<size_t>(count, 2 * n), 1);
+        T* q = nullptr;
+        DNQ_CUDA(cudaHostAlloc((void**)&q, want * sizeof(T), cudaHostAllocDefault));
+        if (p) retired.push_back(p);
+        p = q;
+        n = want;
     }
     ~Pinned() {
         if (p) cudaFreeHost(p);
+        for (T* q : retired) cudaFreeHost(q);
     }
 };
 

@@ -37,7 +37,7 @@ class Ticket:
 
 
 class Server:
-    def __init__(self, *, device: int = 0, budget_bytes: float = 150e9, build_slots: int = 4,
+    def __init__(self, *, device: int = 0, budget_bytes: float = 150e9, build_slots: int = 2,
                  max_group: int = 64):
         h = C.c_void_p()
         N.check(N.lib.dnq_server_create(int(device), int(budget_bytes), int(build_slots),
