@@ -1144,7 +1144,9 @@ __global__ void __launch_bounds__(256) k_vv_compact_long(const u32* big, const u
                                                          const int* n_big, const i64* row_pos,
                                                          const i64* rowptr, i64 n,
                                                          const u32* acol, const double* aval,
-                                                         u32* col, double* val, i64 cap) {
+                                                         u32* col, double* val, i64 cap,
+                                                         float* val32 = nullptr,
+                                                         double* dg = nullptr) {
     __shared__ u32 wsum[8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (rowptr[n] > cap) return;   // a stale plan (k_vv_compact raises the flag)
@@ -1153,6 +1155,8 @@ __global__ void __launch_bounds__(256) k_vv_compact_long(const u32* big, const u
         const u32 g = big[i];
         const i64 src = row_pos[g] & ~kLongRow, dst = rowptr[g];
         const i64 len = big_len[i];
+        if (val32 && threadIdx.x == 0) dg[g] = 0.0;   // set below when the row keeps it
+        __syncthreads();
         i64 carry = 0;
         for (i64 t0 = 0; t0 < len; t0 += 256) {
             const i64 t = t0 + threadIdx.x;
@@ -1167,9 +1171,15 @@ __global__ void __launch_bounds__(256) k_vv_compact_long(const u32* big, const u
                 total += wsum[w];
             }
             if (keep) {
-                const i64 at = dst + carry + before + __popc(m & lanemask_lt());
-                col[at] = c;
-                val[at] = aval[src + t];
+                const i64 o = carry + before + __popc(m & lanemask_lt());
+                const double v = aval[src + t];
+                col[dst + o] = c;
+                val[dst + o] = v;
+                if (val32) {
+                    const bool diag = o == 0 && c == g;
+                    val32[dst + o] = diag ? 0.0f : (float)v;
+                    if (diag) dg[g] = v;
+                }
             }
             carry += total;
             __syncthreads();
@@ -1179,8 +1189,12 @@ __global__ void __launch_bounds__(256) k_vv_compact_long(const u32* big, const u
 
 // Gather the rows from the arena into a standard CSR; rows past `cap`
 // entries (a stale plan) are not written and raise `*bad`.
+// With val32, also the FP32 operator copy: FP32 values with the diagonal
+// entry (a row's first entry when kept: the walk records it first) moved to
+// dg in FP64, 0 where a row has none.
 __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const u32* acol,
-                             const double* aval, u32* col, double* val, i64 cap, int* bad) {
+                             const double* aval, u32* col, double* val, i64 cap, int* bad,
+                             float* val32 = nullptr, double* dg = nullptr) {
     const int lane = threadIdx.x & 31;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
@@ -1191,6 +1205,7 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
     for (i64 r = gw; r < n; r += nw) {
         const i64 src = row_pos[r], dst = rowptr[r], len = rowptr[r + 1] - dst;
         if (src & kLongRow) continue;   // k_vv_compact_long
+        if (val32 && lane == 0) dg[r] = (len > 0 && acol[src] == (u32)r) ? aval[src] : 0.0;
         for (i64 t0 = 0; t0 < len; t0 += 128) {   // four loads per lane before the stores
             u32 c[4];
             double v[4];
@@ -1208,6 +1223,7 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
                 if (t < len) {
                     col[dst + t] = c[u];
                     val[dst + t] = v[u];
+                    if (val32) val32[dst + t] = (t == 0 && c[u] == (u32)r) ? 0.0f : (float)v[u];
                 }
             }
         }
@@ -1765,14 +1781,16 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
                                            n + 1, s));
     k_sanitize<<<1, 1024, 0, s>>>(b->M.rowptr.p, n, b->M.nnz, b->ovf.p, b->bad.p);
     DNQ_CHECK_LAUNCH();
+    // FP32 steps write the FP32 operator copy in the same pass
+    float* v32 = precision == DNQ_F32 ? b->val32.p : nullptr;
+    double* dg = precision == DNQ_F32 ? b->diag_op.p : nullptr;
     k_vv_compact<<<grid, kWS * 32, 0, s>>>(b->rpos.p, b->M.rowptr.p, n, b->acol.p, b->aval.p,
-                                           b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p);
+                                           b->M.col.p, b->M.val.p, b->M.nnz, b->bad.p, v32, dg);
     DNQ_CHECK_LAUNCH();
     k_vv_compact_long<<<grid, 256, 0, s>>>(b->big.p, b->blen.p, b->nbig.p, b->rpos.p,
                                            b->M.rowptr.p, n, b->acol.p, b->aval.p, b->M.col.p,
-                                           b->M.val.p, b->M.nnz);
+                                           b->M.val.p, b->M.nnz, v32, dg);
     DNQ_CHECK_LAUNCH();
-    if (precision == DNQ_F32) launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
     mark(3);
     enqueue_apply(b, precision, s);
     mark(4);
