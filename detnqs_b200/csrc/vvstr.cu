@@ -476,7 +476,7 @@ constexpr int kRing = 32 + 32 * kScanU;
 
 struct WarpShared {
     u32 start[32], pre[32];    // part C: group starts, exclusive prefix of lengths
-    u8 h[32], p[32];
+    u32 tg[32];                // part C: member tag of each group (alpha hole, particle)
     u8 occa[64], vira[64], occb[64], virb[64];
     u32 bs_id[kBS];            // beta group of each indexed beta single of the row
     u16 bs_hp[kBS];            // its excitation, hole | particle << 8
@@ -586,18 +586,18 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_ot
     if (total == 0) return;
     S.start[lane] = gs;
     S.pre[lane] = incl - sl;
-    S.h[lane] = (u8)hh;
-    S.p[lane] = (u8)pp;
+    S.tg[lane] = kHitC | ((u32)hh << 8) | ((u32)pp << 16);
     __syncwarp();
     tests += total;
     for (u32 t0 = 0; t0 < total; t0 += 32 * kScanU) {
-        u32 at[kScanU], tag[kScanU];
+        u32 at[kScanU];
+        int gl[kScanU];
         W y[kScanU];
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             const u32 m = t0 + 32 * u + lane;
             at[u] = 0;
-            tag[u] = 0;
+            gl[u] = 0;
             y[u] = b;   // no hit
             if (m < total) {
                 int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
@@ -605,14 +605,15 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_ot
                 for (int bit = 16; bit; bit >>= 1)
                     if (S.pre[l + bit] <= m) l += bit;
                 at[u] = S.start[l] + (m - S.pre[l]);
-                tag[u] = kHitC | ((u32)S.h[l] << 8) | ((u32)S.p[l] << 16);
+                gl[u] = l;
                 y[u] = __ldg(&a_other[at[u]]);
             }
         }
 #pragma unroll
         for (int u = 0; u < kScanU; ++u) {
             if (t0 + 32 * u >= total) break;
-            q.push(popc_w(b ^ y[u]) == 2, at[u], tag[u]);
+            const int l = gl[u];
+            q.push(popc_w(b ^ y[u]) == 2, at[u], [&] { return S.tg[l]; });   // tag read on a hit
         }
         q.sync();
     }
@@ -812,6 +813,13 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     }
 }
 
+// A member's tag, given as a value or as a function read only on a hit.
+__device__ __forceinline__ u32 tag_value(u32 t) { return t; }
+template <class F>
+__device__ __forceinline__ auto tag_value(const F& f) -> decltype(f()) {
+    return f();
+}
+
 // Sink of walk_row that records the members only: position | tag << 32 in
 // the value slots [w, end) of an arena chunk (whole 8-byte words, so no
 // partial-sector writes); past the end it only counts.
@@ -820,7 +828,8 @@ struct HitOut {
     i64 w, end;
     u32 c = 0;
     bool over = false;
-    __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
+    template <class T>
+    __device__ __forceinline__ void push(bool hit, u32 pos, const T& t) {
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (m == 0) return;   // most steps find nothing
         const int k = __popc(m);
@@ -830,7 +839,7 @@ struct HitOut {
             } else {
                 if (hit) {
                     const i64 at = w + __popc(m & lanemask_lt());
-                    mem[at] = (u64)pos | ((u64)t << 32);
+                    mem[at] = (u64)pos | ((u64)tag_value(t) << 32);
                 }
                 w += k;
             }
@@ -851,13 +860,14 @@ struct QueueEval {
     HitRing& Q;
     Out& out;
     int n = 0, head = 0;   // queued members (warp-uniform)
-    __device__ __forceinline__ void push(bool hit, u32 pos, u32 t) {
+    template <class T>
+    __device__ __forceinline__ void push(bool hit, u32 pos, const T& t) {
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
             int k = head + n + __popc(m & lanemask_lt());
             if (k >= kRing) k -= kRing;
             Q.pos[k] = pos;
-            Q.tag[k] = t;
+            Q.tag[k] = tag_value(t);
         }
         n += __popc(m);
     }
