@@ -111,14 +111,44 @@ __global__ void k_group_starts(const unsigned* head, u32* gid, i64 n, u32* gstar
     }
 }
 
+// Strings of at most 32 orbitals: one 64-bit key (group string << 32 | companion).
+__global__ void k_keys_by64(const u64* V, i64 n, int major, u64* k, u32* id) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u64 a = V[2 * t], b = V[2 * t + 1];
+        k[t] = major == 0 ? (a << 32) | b : (b << 32) | a;
+        id[t] = (u32)t;
+    }
+}
+
+__global__ void k_split_sorted64(const u64* k, i64 n, u64* other, u32* other32, unsigned* head) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        other[t] = k[t] & 0xffffffffull;
+        other32[t] = (u32)k[t];
+        head[t] = (t == 0 || (k[t] >> 32) != (k[t - 1] >> 32)) ? 1u : 0u;
+    }
+}
+
+// Group string of sorted position t, for either key layout.
+struct Key128 {
+    const ulonglong2* k;
+    __device__ __forceinline__ u64 operator()(i64 t) const { return k[t].x; }
+};
+struct Key64 {
+    const u64* k;
+    __device__ __forceinline__ u64 operator()(i64 t) const { return k[t] >> 32; }
+};
+
 // Insert one slot per group: (string, start << 32 | len).
-__global__ void k_group_insert(const ulonglong2* k, const u32* gstart, i64 ngroups, i64 n,
-                               ulonglong2* slots, u64 mask) {
+template <class K>
+__global__ void k_group_insert(K k, const u32* gstart, i64 ngroups, i64 n, ulonglong2* slots,
+                               u64 mask) {
     for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < ngroups;
          g += (i64)gridDim.x * blockDim.x) {
         const i64 t = gstart[g];
         const i64 e = g + 1 < ngroups ? (i64)gstart[g + 1] : n;
-        const u64 key = k[t].x;
+        const u64 key = k(t);
         const u64 val = ((u64)t << 32) | (u64)(e - t);
         u64 h = det_hash(key, 0x5bd1e995ull) & mask;
         for (u64 probe = 0; probe <= mask; ++probe) {
@@ -138,8 +168,10 @@ int gsz(i64 n) {
     return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
 }
 
-// major 0: groups by alpha (companion beta); major 1: groups by beta.
-void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s) {
+// major 0: groups by alpha (companion beta); major 1: groups by beta.  With
+// n_orb <= 32 the sort runs on 64-bit keys over 32 + n_orb bits, and the
+// 32-bit companion strings of the scans come out of the same pass.
+void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cudaStream_t s) {
     if (n == 0) {   // no groups: an empty table
         X.ngroups = 0;
         X.mask = 1023;
@@ -147,21 +179,41 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s
         DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, 1024 * sizeof(ulonglong2), s));
         return;
     }
-    DBuf<ulonglong2> k(n, s), ks(n, s);
+    const bool narrow = n_orb <= 32;
+    DBuf<ulonglong2> k, ks;
+    DBuf<u64> k64, ks64;
     DBuf<u32> id(n, s);
     X.idx.alloc(n, s);
     X.other.alloc(n, s);
-    k_keys_by<<<gsz(n), 256, 0, s>>>(V, n, major, k.p, id.p);
-    DNQ_CHECK_LAUNCH();
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k.p, ks.p, id.p, X.idx.p, n,
-                                             SwapKey{}, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k.p, ks.p, id.p, X.idx.p, n,
-                                             SwapKey{}, s));
     DBuf<unsigned> head(n, s);
-    k_split_sorted<<<gsz(n), 256, 0, s>>>(ks.p, n, X.other.p, head.p);
-    DNQ_CHECK_LAUNCH();
+    if (narrow) {
+        k64.alloc(n, s);
+        ks64.alloc(n, s);
+        X.other32.alloc(n, s);
+        k_keys_by64<<<gsz(n), 256, 0, s>>>(V, n, major, k64.p, id.p);
+        DNQ_CHECK_LAUNCH();
+        size_t tmp = 0;
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k64.p, ks64.p, id.p, X.idx.p, n,
+                                                 0, 32 + n_orb, s));
+        DBuf<u8> tb(tmp, s);
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k64.p, ks64.p, id.p, X.idx.p, n, 0,
+                                                 32 + n_orb, s));
+        k_split_sorted64<<<gsz(n), 256, 0, s>>>(ks64.p, n, X.other.p, X.other32.p, head.p);
+        DNQ_CHECK_LAUNCH();
+    } else {
+        k.alloc(n, s);
+        ks.alloc(n, s);
+        k_keys_by<<<gsz(n), 256, 0, s>>>(V, n, major, k.p, id.p);
+        DNQ_CHECK_LAUNCH();
+        size_t tmp = 0;
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k.p, ks.p, id.p, X.idx.p, n,
+                                                 SwapKey{}, s));
+        DBuf<u8> tb(tmp, s);
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k.p, ks.p, id.p, X.idx.p, n,
+                                                 SwapKey{}, s));
+        k_split_sorted<<<gsz(n), 256, 0, s>>>(ks.p, n, X.other.p, head.p);
+        DNQ_CHECK_LAUNCH();
+    }
     X.gid.alloc(n, s);
     X.gstart.alloc(n, s);
     DBuf<u32>& gid = X.gid;
@@ -184,7 +236,12 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, cudaStream_t s
     X.mask = cap - 1;
     X.slots.alloc(cap, s);
     DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, cap * sizeof(ulonglong2), s));
-    k_group_insert<<<gsz(ngroups), 256, 0, s>>>(ks.p, gstart.p, ngroups, n, X.slots.p, X.mask);
+    if (narrow)
+        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key64{ks64.p}, gstart.p, ngroups, n,
+                                                    X.slots.p, X.mask);
+    else
+        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key128{ks.p}, gstart.p, ngroups, n,
+                                                    X.slots.p, X.mask);
     DNQ_CHECK_LAUNCH();
 }
 
@@ -196,7 +253,7 @@ __global__ void k_narrow(const u64* x, i64 n, u32* y) {
 
 // 32-bit companion strings for scans (every string below orbital 32).
 void narrow_index(StrIndex& X, i64 n, cudaStream_t s) {
-    if (n == 0) return;
+    if (n == 0 || X.other32.n == (size_t)n) return;
     X.other32.alloc(n, s);
     k_narrow<<<gsz(n), 256, 0, s>>>(X.other.p, n, X.other32.p);
     DNQ_CHECK_LAUNCH();
@@ -1472,8 +1529,8 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     DNQ_CUDA(cudaEventCreate(&e1));
     DNQ_CUDA(cudaEventRecord(e0, s));
     StrIndex A, B;
-    build_str_index(A, V, n, 0, s);
-    build_str_index(B, V, n, 1, s);
+    build_str_index(A, V, n, 0, n_orb, s);
+    build_str_index(B, V, n, 1, n_orb, s);
     build_presence(A, B, n, s);
     const bool narrow = n_orb <= 32;
     if (narrow) {
@@ -1922,8 +1979,8 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         check_orbitals(b->V[k].p, n, n_orb[k], s);
         DetMap dup;
         build_detmap(dup, b->V[k].p, n, true, s);   // duplicates are an error
-        build_str_index(b->A[k], b->V[k].p, n, 0, s);
-        build_str_index(b->B[k], b->V[k].p, n, 1, s);
+        build_str_index(b->A[k], b->V[k].p, n, 0, n_orb[k], s);
+        build_str_index(b->B[k], b->V[k].p, n, 1, n_orb[k], s);
         build_presence(b->A[k], b->B[k], n, s);
         if (b->narrow) {
             narrow_index(b->A[k], n, s);
