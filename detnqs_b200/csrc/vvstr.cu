@@ -21,6 +21,7 @@
 #include <cuda/std/tuple>
 
 #include <algorithm>
+#include <type_traits>
 #include <memory>
 #include <vector>
 
@@ -987,6 +988,20 @@ __device__ __forceinline__ int next_row(int* ctr) {
     return __shfl_sync(0xffffffffu, r, 0);
 }
 
+// Word type of the scans: u32 / u64 for every row, or PerRowW to pick per
+// row (batches mixing systems of at most and of more than 32 orbitals).
+struct PerRowW {};
+template <class W, class Q>
+__device__ __forceinline__ void walk_any(const VVParams& P, int r, u64 a, u64 b, WarpShared& S,
+                                         Q& q, unsigned long long& tests) {
+    if constexpr (std::is_same<W, PerRowW>::value) {
+        if (P.a_other32) walk_row<u32>(P, r, a, b, S, q, tests);
+        else walk_row<u64>(P, r, a, b, S, q, tests);
+    } else {
+        walk_row<W>(P, r, a, b, S, q, tests);
+    }
+}
+
 // Single pass, first half: each warp appends the members of its rows to
 // private chunks of the arena (k_vv_eval turns them into entries in place).
 template <class Loc, class W>
@@ -1020,7 +1035,7 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         for (int attempt = 0; attempt < 2; ++attempt) {
             HitOut out{reinterpret_cast<u64*>(A.aval), cpos, cend};
             unsigned long long tt = 0;
-            walk_row<W>(P, r, a, b, S, out, tt);
+            walk_any<W>(P, r, a, b, S, out, tt);
             if (attempt == 0) {
                 tests += tt;
                 hits += out.c;
@@ -1148,7 +1163,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         load_lists(S, a, b, P.n_orb);
         HitOut out{reinterpret_cast<u64*>(A.aval), (i64)base, (i64)base + len};
         unsigned long long tt = 0;
-        walk_row<W>(P, r, a, b, S, out, tt);
+        walk_any<W>(P, r, a, b, S, out, tt);
         if (lane == 0) {
             A.row_pos[g] = (i64)base | kLongRow;
             A.big_len[i] = len;
@@ -1365,13 +1380,30 @@ int vv_grid(int device) {
     return std::max(1, per_sm) * sm_count(device);
 }
 
+// scan: 0 = 64-bit strings, 1 = 32-bit, 2 = chosen per row.
+template <class Loc>
+void launch_walk(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s) {
+    if (scan == 1) k_vv_arena<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else if (scan == 2) k_vv_arena<Loc, PerRowW><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_arena<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+}
+
+template <class Loc>
+void launch_big(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s) {
+    if (scan == 1) k_vv_big<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
+    else if (scan == 2) k_vv_big<Loc, PerRowW><<<grid, kWS * 32, 0, s>>>(L, A);
+    else k_vv_big<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
+}
+
 // Single-pass build of nrows rows of L into M (allocated here).  cap_hint:
 // expected nnz (0 = unknown).  Falls back to the exact two-pass walk when
 // the arena is too small.  Returns the number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
            double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr,
-           bool narrow = false) {
+           int scan = 0) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
@@ -1414,13 +1446,10 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaMemsetAsync(cursor.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(rlen.p + nrows, 0, 4, s));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
-    if (narrow) k_vv_arena<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
-    else k_vv_arena<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
-    DNQ_CHECK_LAUNCH();
+    launch_walk<Loc>(scan, grid, L, A, s);
     k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    if (narrow) k_vv_big<Loc, u32><<<grid, kWS * 32, 0, s>>>(L, A);
-    else k_vv_big<Loc, u64><<<grid, kWS * 32, 0, s>>>(L, A);
+    launch_big<Loc>(scan, grid, L, A, s);
     DNQ_CHECK_LAUNCH();
     k_vv_eval_long<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
@@ -1542,7 +1571,8 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     double tg = 0, tsc = 0, tc = 0;
     i64 hits = 0;
     H->candidates =
-        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits, narrow);
+        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits,
+               narrow ? 1 : 0);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);
@@ -1692,7 +1722,7 @@ struct dnq_batch_s {
     dnq::DBuf<dnq::u8> scan_tmp;
     dnq::i64 cap = 0;
     dnq::i64 hits = 0;   // members of the sizing build (the arena holds members)
-    bool narrow = false;   // every system has n_orb <= 32 (32-bit scans)
+    int scan = 0;   // string words of the scans: 0 u64, 1 u32 (all n_orb <= 32), 2 per system
     bool planned = false;
     // tunables
     dnq::i64 chunk = dnq::kChunk;
@@ -1748,7 +1778,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     // the sizing build fills the batch's CSR itself, so the blocks are
     // valid right after creation
-    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits, b->narrow);
+    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits, b->scan);
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
@@ -1832,14 +1862,10 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CUDA(cudaMemsetAsync(b->cursor.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(b->bad.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
-    if (b->narrow) k_vv_arena<ManySys, u32><<<grid, kWS * 32, 0, s>>>(L, A);
-    else k_vv_arena<ManySys, u64><<<grid, kWS * 32, 0, s>>>(L, A);
-    DNQ_CHECK_LAUNCH();
+    launch_walk<ManySys>(b->scan, grid, L, A, s);
     k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    if (b->narrow) k_vv_big<ManySys, u32><<<grid, kWS * 32, 0, s>>>(L, A);
-    else k_vv_big<ManySys, u64><<<grid, kWS * 32, 0, s>>>(L, A);
-    DNQ_CHECK_LAUNCH();
+    launch_big<ManySys>(b->scan, grid, L, A, s);
     k_vv_eval_long<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     mark(2);
@@ -1971,7 +1997,8 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
     b->V.resize(n_sys);
     b->A.resize(n_sys);
     b->B.resize(n_sys);
-    b->narrow = std::all_of(n_orb, n_orb + n_sys, [](int o) { return o <= 32; });
+    const int n_narrow = (int)std::count_if(n_orb, n_orb + n_sys, [](int o) { return o <= 32; });
+    b->scan = n_narrow == n_sys ? 1 : (n_narrow > 0 ? 2 : 0);
     for (int k = 0; k < n_sys; ++k) {
         const i64 n = n_dets[k];
         b->V[k].alloc(2 * n, s);
@@ -1982,7 +2009,7 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         build_str_index(b->A[k], b->V[k].p, n, 0, n_orb[k], s);
         build_str_index(b->B[k], b->V[k].p, n, 1, n_orb[k], s);
         build_presence(b->A[k], b->B[k], n, s);
-        if (b->narrow) {
+        if (n_orb[k] <= 32) {
             narrow_index(b->A[k], n, s);
             narrow_index(b->B[k], n, s);
         }
