@@ -398,6 +398,12 @@ struct VVParams {
 // Where rows are written.  Single pass: rows appended to warp-private
 // chunks of an arena; long rows get exact space in a second walk; the
 // two-pass fallback counts, then fills at known offsets.
+struct SingleOut {
+    double h;
+    u32 j;
+    u32 keep;
+};
+
 struct Arena {
     u32* acol;
     double* aval;
@@ -414,6 +420,14 @@ struct Arena {
     int* next_row;
     unsigned long long* n_test;
     unsigned long long* n_hit;        // members recorded by k_vv_arena (optional)
+    // single excitations recorded by k_vv_arena in warp-private slices of
+    // sgl_slice entries, evaluated by k_vv_singles one per thread; past its
+    // slice a warp leaves them ordinary members
+    uint4* sgl;                       // (row, sorted position, kind, 0)
+    SingleOut* sres;
+    u32* sgl_n;                       // entries used in each warp's slice
+    u32 sgl_slice;
+    i64 sgl_cap;                      // warps * sgl_slice
     u32* cnt;                         // two-pass fallback
     const i64* off;
     u32* col;
@@ -563,8 +577,11 @@ __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, int n_or
 // hold the alpha hole and particle.  The diagonal is a member of its own
 // kind whose position is the row.  Members are found by walk_row and
 // turned into elements by eval_hit, in the order found.
-// kinds: same beta string, same alpha string, opposite-spin double, diagonal
-enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2, kHitD = 3 };
+// kinds: same beta string, same alpha string, opposite-spin double, diagonal,
+// a single evaluated ahead (its position field is its index in the singles
+// list).  kSingleBit marks a single of kind A or B as the walk finds it.
+enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2, kHitD = 3, kHitS = 4 };
+constexpr u32 kSingleBit = 0x80;
 
 struct Hit {
     double h;
@@ -573,10 +590,16 @@ struct Hit {
 };
 
 __device__ __forceinline__ Hit eval_hit(const VVParams& P, int r, u64 a, u64 b, double psr,
-                                        double cut, u32 pos, u32 tag) {
+                                        double cut, u32 pos, u32 tag,
+                                        const SingleOut* sres = nullptr) {
     Hit e{0.0, 0u, false};
-    const u32 kind = tag & 0xff;
-    if (kind == kHitC) {
+    const u32 kind = tag & 0x7f;
+    if (kind == kHitS) {
+        const SingleOut o = sres[pos];
+        e.h = o.h;
+        e.j = o.j;
+        e.keep = o.keep != 0;
+    } else if (kind == kHitC) {
         const u64 y = __ldg(&P.a_other[pos]);
         const u64 x = b ^ y;
         const int ha = (tag >> 8) & 0xff, pa = tag >> 16;
@@ -694,7 +717,8 @@ __device__ __forceinline__ void scan_same(Q& q, const W* other, W x, u32 st, u32
         for (int u = 0; u < kScanU; ++u) {
             if (t0 + 32 * u >= ln) break;
             const int dd = popc_w(x ^ y[u]);
-            q.push(dd == 2 || dd == 4, st + t0 + 32 * u + lane, kind);
+            q.push_ab(dd == 2 || dd == 4, st + t0 + 32 * u + lane,
+                      kind | (dd == 2 ? kSingleBit : 0u));
         }
         q.sync();
     }
@@ -884,6 +908,11 @@ __device__ __forceinline__ auto tag_value(const F& f) -> decltype(f()) {
 struct HitOut {
     u64* mem;   // the arena's value array as u64
     i64 w, end;
+    uint4* sgl = nullptr;   // this warp's singles slice (null: singles stay members)
+    u32* sgn = nullptr;     // its entries used
+    u32 sslice = 0;         // its size
+    u32 sbase = 0;          // index of its first entry in the list
+    u32 row = 0;            // global row, recorded with its singles
     u32 c = 0;
     bool over = false;
     template <class T>
@@ -898,6 +927,36 @@ struct HitOut {
                 if (hit) {
                     const i64 at = w + __popc(m & lanemask_lt());
                     mem[at] = (u64)pos | ((u64)tag_value(t) << 32);
+                }
+                w += k;
+            }
+        }
+        c += k;
+    }
+    // Parts A and B: a single (tag with kSingleBit) goes to the singles list
+    // when there is one and it has room.
+    __device__ __forceinline__ void push_ab(bool hit, u32 pos, u32 tg) {
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (m == 0) return;
+        const int k = __popc(m);
+        if (!over) {
+            if (w + k > end) {
+                over = true;
+            } else {
+                u64 rec = (u64)pos | ((u64)(tg & ~kSingleBit) << 32);
+                const bool sg = hit && (tg & kSingleBit) && sgl;
+                const unsigned sm = __ballot_sync(0xffffffffu, sg);
+                if (sm) {
+                    const u32 idx = *sgn + __popc(sm & lanemask_lt());
+                    if (sg && idx < sslice) {
+                        sgl[idx] = make_uint4(row, pos, tg & ~kSingleBit, 0u);
+                        rec = (u64)(sbase + idx) | ((u64)kHitS << 32);
+                    }
+                    *sgn += __popc(sm);
+                }
+                if (hit) {
+                    const i64 at = w + __popc(m & lanemask_lt());
+                    mem[at] = rec;
                 }
                 w += k;
             }
@@ -925,10 +984,11 @@ struct QueueEval {
             int k = head + n + __popc(m & lanemask_lt());
             if (k >= kRing) k -= kRing;
             Q.pos[k] = pos;
-            Q.tag[k] = tag_value(t);
+            Q.tag[k] = tag_value(t) & ~kSingleBit;
         }
         n += __popc(m);
     }
+    __device__ __forceinline__ void push_ab(bool hit, u32 pos, u32 t) { push(hit, pos, t); }
     __device__ __forceinline__ void eval(int cnt) {
         const int lane = threadIdx.x & 31;
         Hit e{0.0, 0u, false};
@@ -1021,6 +1081,9 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         }
     }
     unsigned long long tests = 0, hits = 0;
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint4* slice = A.sgl ? A.sgl + (i64)wid * A.sgl_slice : nullptr;
+    u32 sgn = 0;
     for (;;) {
         const int g = next_row(A.next_row);
         if (g >= nrows) break;
@@ -1032,8 +1095,11 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
+        const u32 sgn0 = sgn;   // a row that is walked again drops its singles
         for (int attempt = 0; attempt < 2; ++attempt) {
-            HitOut out{reinterpret_cast<u64*>(A.aval), cpos, cend};
+            sgn = sgn0;
+            HitOut out{reinterpret_cast<u64*>(A.aval), cpos, cend, slice, &sgn, A.sgl_slice,
+                       (u32)wid * A.sgl_slice, (u32)g};
             unsigned long long tt = 0;
             walk_any<W>(P, r, a, b, S, out, tt);
             if (attempt == 0) {
@@ -1060,6 +1126,7 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
                     A.row_len[g] = out.c;
                     A.big[atomicAdd(A.n_big, 1)] = (u32)g;
                 }
+                sgn = sgn0;
                 break;
             }
             unsigned long long base = 0;
@@ -1077,6 +1144,33 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
     if (lane == 0) {
         atomicAdd(A.n_test, tests);
         if (A.n_hit) atomicAdd(A.n_hit, hits);
+        if (A.sgl) A.sgl_n[wid] = sgn < A.sgl_slice ? sgn : A.sgl_slice;
+    }
+}
+
+// Single excitations recorded by the walk, one per thread: their elements
+// are chains of dependent additions, which a warp per row would wait on.
+template <class Loc>
+__global__ void __launch_bounds__(256) k_vv_singles(Loc L, Arena A) {
+    if (*(volatile int*)A.overflow) return;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < A.sgl_cap;
+         i += (i64)gridDim.x * blockDim.x) {
+        if ((u32)(i % A.sgl_slice) >= A.sgl_n[i / A.sgl_slice]) continue;
+        const uint4 e = A.sgl[i];
+        int r;
+        u32 cb;
+        const VVParams& P = L.at(e.x, r, cb);
+        u64 a, b;
+        double psr, cut;
+        row_setup(P, r, a, b, psr, cut);
+        const bool alpha = e.z == kHitA;   // the alpha string moves
+        const u64 y = alpha ? __ldg(&P.b_other[e.y]) : __ldg(&P.a_other[e.y]);
+        const double h = str_single(P, a, b, alpha ? 0 : 1, alpha ? a : b, y);
+        SingleOut o;
+        o.h = h;
+        o.keep = keep_single(P, psr, h) ? 1u : 0u;
+        o.j = alpha ? __ldg(&P.b_idx[e.y]) : __ldg(&P.a_idx[e.y]);
+        A.sres[i] = o;
     }
 }
 
@@ -1109,8 +1203,8 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
             const u64 m2 = k2 < len ? mem[pos + k2] : 0ull;
             const u32 p1 = (u32)m1, t1 = (u32)(m1 >> 32), p2 = (u32)m2, t2 = (u32)(m2 >> 32);
             Hit e1{0.0, 0u, false}, e2{0.0, 0u, false};
-            if (k1 < len) e1 = eval_hit(P, r, a, b, psr, cut, p1, t1);
-            if (k2 < len) e2 = eval_hit(P, r, a, b, psr, cut, p2, t2);
+            if (k1 < len) e1 = eval_hit(P, r, a, b, psr, cut, p1, t1, A.sres);
+            if (k2 < len) e2 = eval_hit(P, r, a, b, psr, cut, p2, t2, A.sres);
             unsigned m = __ballot_sync(0xffffffffu, e1.keep);
             if (e1.keep) {
                 const i64 at = w + __popc(m & lanemask_lt());
@@ -1418,6 +1512,14 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     if (g_arena_cap > 0) cap = g_arena_cap;
     DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
     DBuf<unsigned long long> nt(1, s), cursor(1, s), nh(1, s);
+    // singles list: ~5 per row on heat-bath spaces, in one slice per warp;
+    // past its slice a warp evaluates them with their row
+    const u32 slice = (u32)std::max<i64>(
+        64, std::min<i64>(std::max<i64>(8 * nrows, 1024), i64(64) << 20) / warps);
+    const i64 scap = (i64)slice * warps;
+    DBuf<uint4> sgl(scap, s);
+    DBuf<SingleOut> sres(scap, s);
+    DBuf<u32> sgn(warps, s);
     DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s), blen(nrows, s);
     DBuf<double> aval(cap, s);
     DBuf<i64> rpos(nrows, s);
@@ -1437,6 +1539,11 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.next_row = next.p;
     A.n_test = nt.p;
     A.n_hit = nh.p;
+    A.sgl = sgl.p;
+    A.sres = sres.p;
+    A.sgl_n = sgn.p;
+    A.sgl_slice = slice;
+    A.sgl_cap = scap;
     DNQ_CUDA(cudaMemsetAsync(nt.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(nh.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
@@ -1447,6 +1554,8 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaMemsetAsync(rlen.p + nrows, 0, 4, s));
     DNQ_CUDA(cudaEventRecord(ev[0], s));
     launch_walk<Loc>(scan, grid, L, A, s);
+    k_vv_singles<Loc><<<grid, 256, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
     k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     launch_big<Loc>(scan, grid, L, A, s);
@@ -1715,6 +1824,10 @@ struct dnq_batch_s {
     dnq::Csr M;
     // planned arena (fixed sizes for graph replays)
     dnq::DBuf<dnq::u32> acol, rlen, big, blen;
+    dnq::DBuf<uint4> sgl;
+    dnq::DBuf<dnq::SingleOut> sres;
+    dnq::DBuf<dnq::u32> sgn;
+    dnq::u32 sgl_slice = 0;
     dnq::DBuf<double> aval;
     dnq::DBuf<dnq::i64> rpos;
     dnq::DBuf<int> next, ovf, nbig, bad;
@@ -1788,6 +1901,14 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->rlen.alloc(n + 1, s);
     b->big.alloc(n, s);
     b->blen.alloc(n, s);
+    {
+        const i64 warps = (i64)grid * kWS;
+        b->sgl_slice = (u32)std::max<i64>(
+            64, std::min<i64>(std::max<i64>(8 * n, 1024), i64(64) << 20) / warps);
+        b->sgl.alloc((i64)b->sgl_slice * warps, s);
+        b->sres.alloc((i64)b->sgl_slice * warps, s);
+        b->sgn.alloc(warps, s);
+    }
     b->rpos.alloc(n, s);
     b->next.alloc(1, s);
     b->ovf.alloc(1, s);
@@ -1849,6 +1970,11 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     A.row_len = b->rlen.p;
     A.big = b->big.p;
     A.big_len = b->blen.p;
+    A.sgl = b->sgl.p;
+    A.sres = b->sres.p;
+    A.sgl_n = b->sgn.p;
+    A.sgl_slice = b->sgl_slice;
+    A.sgl_cap = (i64)b->sgl.n;
     A.n_big = b->nbig.p;
     A.next_row = b->next.p;
     A.n_test = b->nt.p;
@@ -1863,6 +1989,8 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     DNQ_CUDA(cudaMemsetAsync(b->bad.p, 0, 4, s));
     DNQ_CUDA(cudaMemsetAsync(b->rlen.p + n, 0, 4, s));
     launch_walk<ManySys>(b->scan, grid, L, A, s);
+    k_vv_singles<ManySys><<<grid, 256, 0, s>>>(L, A);
+    DNQ_CHECK_LAUNCH();
     k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     launch_big<ManySys>(b->scan, grid, L, A, s);
