@@ -425,6 +425,7 @@ def run_ours(args, rank: int, world: int):
         "candidates_per_s": cand / (float(np.mean(t_build)) * 1e-3),
         "dE_fp32_vs_fp64_Ha": dE,
         "build_phase_ms": {k: float(v) for k, v in last.timings().items()},
+        "ms_steps": [round(x, 3) for x in t_steps],
         "roofline": {"bound": "hbm",
                      "kernel": "k_vv_arena + k_vv_eval (V->V build: members, then entries)",
                      "achieved": alg_fill / (fill_ms * 1e-3) / 1e9, "peak": peak,
@@ -444,7 +445,8 @@ def run_ours(args, rank: int, world: int):
                               "frac": (nnz * 8 + n_dets * 36) / (ss["f32"] * 1e-3) / 1e9 / peak,
                               "traffic": ncu_traffic("k_spmv_f32c"), "peak_kind": peak_kind},
         "e2e": {"value": world * nnz / (e2e_ms * 1e-3), "unit": "elements/s",
-                "ms_per_step": e2e_ms, "h2d_bytes_per_step": n_dets * 16 + 2 * n_dets * 8,
+                "ms_per_step": e2e_ms, "ms_steps": [round(x, 3) for x in e2e],
+                "h2d_bytes_per_step": n_dets * 16 + 2 * n_dets * 8,
                 "d2h_bytes_per_step": 2 * n_dets * 8 + 32},
         "gpu_launches": int(launches),
         "clocks": clocks,
