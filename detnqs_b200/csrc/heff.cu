@@ -427,28 +427,46 @@ __global__ void __launch_bounds__(1024) k_long_sum64(const double* term, i64 n, 
     if (threadIdx.x == 0) *out = acc;
 }
 
-// FP32: float-float sums per lane (terms strided by 32), merged in lane
-// order: deterministic, accurate to a few FP32 ulps squared.
-__global__ void k_long_sum32(const float2* term, i64 n, float2* out) {
-    const int lane = threadIdx.x & 31;
+// FP32: float-float sums over a fixed tree: kSum32Blocks x 256 threads each
+// sum a strided share of the terms, the block merges its threads in order,
+// and k_long_merge32 merges the blocks in order.  The tree does not depend
+// on the GPU, so the result is deterministic; accurate to a few FP32 ulps
+// squared.
+constexpr int kSum32Blocks = 256;
+
+struct FF {
     float hi = 0.0f, lo = 0.0f;
-    auto add = [&](float p, float pe) {
+    __device__ __forceinline__ void add(float p, float pe) {
         float s2, e;
         f_two_sum(hi, p, s2, e);
         const float c = __fadd_rn(lo, __fadd_rn(e, pe));
         hi = __fadd_rn(s2, c);
         lo = __fsub_rn(c, __fsub_rn(hi, s2));
-    };
-    for (i64 t = lane; t < n; t += 32) add(term[t].x, term[t].y);
-    __shared__ float sh[2][32];
-    sh[0][lane] = hi;
-    sh[1][lane] = lo;
-    __syncwarp();
-    if (lane == 0) {
-        hi = 0.0f;
-        lo = 0.0f;
-        for (int q = 0; q < 32; ++q) add(sh[0][q], sh[1][q]);
-        *out = make_float2(hi, lo);
+    }
+};
+
+__global__ void __launch_bounds__(256) k_long_part32(const float2* term, i64 n, float2* part) {
+    __shared__ float2 sh[256];
+    FF acc;
+    const i64 stride = (i64)kSum32Blocks * 256;
+    for (i64 t = blockIdx.x * 256ll + threadIdx.x; t < n; t += stride) {
+        const float2 v = term[t];
+        acc.add(v.x, v.y);
+    }
+    sh[threadIdx.x] = make_float2(acc.hi, acc.lo);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        FF b;
+        for (int q = 0; q < 256; ++q) b.add(sh[q].x, sh[q].y);
+        part[blockIdx.x] = make_float2(b.hi, b.lo);
+    }
+}
+
+__global__ void k_long_merge32(const float2* part, float2* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        FF b;
+        for (int q = 0; q < kSum32Blocks; ++q) b.add(part[q].x, part[q].y);
+        *out = make_float2(b.hi, b.lo);
     }
 }
 
@@ -727,8 +745,14 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
                                                skip.p, t0, t1, precision == DNQ_F32, term.p,
                                                term2.p, multi.p, ltouch.p + q);
             DNQ_CHECK_LAUNCH();
-            if (precision == DNQ_F32) k_long_sum32<<<1, 32, 0, s>>>(term2.p, m, ldiag2.p + q);
-            else k_long_sum64<<<1, 1024, 0, s>>>(term.p, m, ldiag.p + q);
+            if (precision == DNQ_F32) {
+                DBuf<float2> part(kSum32Blocks, s);
+                k_long_part32<<<kSum32Blocks, 256, 0, s>>>(term2.p, m, part.p);
+                DNQ_CHECK_LAUNCH();
+                k_long_merge32<<<1, 32, 0, s>>>(part.p, ldiag2.p + q);
+            } else {
+                k_long_sum64<<<1, 1024, 0, s>>>(term.p, m, ldiag.p + q);
+            }
             DNQ_CHECK_LAUNCH();
             // kept k's whose column holds other rows, in order
             DBuf<u32> idx(m, s), sel(m, s);
