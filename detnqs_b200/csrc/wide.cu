@@ -123,6 +123,28 @@ __device__ double diag2(const CtxView& C, const M2& a, const M2& b) {
 
 // Single h -> p in spin s (ham_eval.cpp:88-115): h1 first, then the other
 // occupied orbitals, alpha ascending then beta ascending.
+// e + arr[occ[t]] for t = 0..cnt-1 except occ[t] == skip, added in t order;
+// the loads are issued eight at a time ahead of their additions.
+__device__ __forceinline__ double add_occ(double e, const double* arr, const u8* occ, int cnt,
+                                          int skip) {
+    int t = 0;
+    for (; t + 8 <= cnt; t += 8) {
+        double v[8];
+        int o[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            o[q] = occ[t + q];
+            v[q] = __ldg(&arr[o[q]]);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (o[q] != skip) e += v[q];
+    }
+    for (; t < cnt; ++t)
+        if (occ[t] != skip) e += arr[occ[t]];
+    return e;
+}
+
 __device__ __forceinline__ double single2(const CtxView& C, const WRow& R, int s, int h, int p) {
     const int n = C.n;
     double e = C.h1[h * n + p];
@@ -130,13 +152,11 @@ __device__ __forceinline__ double single2(const CtxView& C, const WRow& R, int s
     const double* ss = C.sss + base;
     const double* os = C.sos + base;
     if (s == 0) {
-        for (int t = 0; t < R.na; ++t)
-            if (R.occa[t] != h) e += ss[R.occa[t]];
-        for (int t = 0; t < R.nb; ++t) e += os[R.occb[t]];
+        e = add_occ(e, ss, R.occa, R.na, h);
+        e = add_occ(e, os, R.occb, R.nb, -1);
     } else {
-        for (int t = 0; t < R.na; ++t) e += os[R.occa[t]];
-        for (int t = 0; t < R.nb; ++t)
-            if (R.occb[t] != h) e += ss[R.occb[t]];
+        e = add_occ(e, os, R.occa, R.na, -1);
+        e = add_occ(e, ss, R.occb, R.nb, h);
     }
     const int perm = between2(s ? R.b : R.a, h, p);
     return (perm & 1) ? -e : e;
