@@ -58,6 +58,7 @@ sys.path.insert(0, ROOT)
 N_ORB, N_ALPHA, N_BETA, N_CHOL = 30, 12, 12, 60
 N_DETS = 1_000_000
 EPS1 = 1e-6
+SMS = 148          # B200 streaming multiprocessors
 INT_SEED, DET_SEED, PSI_SEED = 1001, 2002, 3003
 CACHE = os.path.join(tempfile.gettempdir(), "detnqs_b200_bench")
 
@@ -444,6 +445,22 @@ def run_ours(args, rank: int, world: int):
                               "peak": peak, "unit": "GB/s",
                               "frac": (nnz * 8 + n_dets * 36) / (ss["f32"] * 1e-3) / 1e9 / peak,
                               "traffic": ncu_traffic("k_spmv_f32c"), "peak_kind": peak_kind},
+        # every x gather of H.psi is its own 32-byte L1 sector; an SM's L1
+        # returns about one sector per clock, which bounds both precisions
+        "gather_bound_spmv": {
+            "unit": "sectors/s",
+            "sectors_per_launch": {"f64": nnz + (nnz * 12 + n_dets * 24) / 32,
+                                   "f32": nnz + (nnz * 8 + n_dets * 36) / 32},
+            "peak": SMS * (clocks.get("sm_mhz") or 1965.0) * 1e6,
+            "achieved": {k: sec / (ss[k] * 1e-3) for k, sec in
+                         (("f64", nnz + (nnz * 12 + n_dets * 24) / 32),
+                          ("f32", nnz + (nnz * 8 + n_dets * 36) / 32))},
+            "frac": {k: sec / (ss[k] * 1e-3) / (SMS * (clocks.get("sm_mhz") or 1965.0) * 1e6)
+                     for k, sec in (("f64", nnz + (nnz * 12 + n_dets * 24) / 32),
+                                    ("f32", nnz + (nnz * 8 + n_dets * 36) / 32))},
+            "note": "one L1 sector per gathered x value plus the streamed CSR sectors; peak = 1 "
+                    "sector per SM clock, the rate ncu measured for the FP32 kernel on the 200k "
+                    "case (profiles/spmv_200k_full.md)"},
         "e2e": {"value": world * nnz / (e2e_ms * 1e-3), "unit": "elements/s",
                 "ms_per_step": e2e_ms, "ms_steps": [round(x, 3) for x in e2e],
                 "h2d_bytes_per_step": n_dets * 16 + 2 * n_dets * 8,
