@@ -12,11 +12,21 @@
 //   B  same alpha string a: beta single or beta-beta double of b;
 //   C  alpha string a' = single of a, beta string a single of b:
 //      the group of every single a' of a, filtered by popc(b ^ b') == 2.
+// Long alpha groups in C are not scanned: each keeps a presence row (one
+// bit per beta group) tested against the row's indexed beta singles.
 // Each match gets its element exactly as HamEval::compute_elem does
 // (ham_eval.cpp:88-147: same integrals, same order of operations) and is
 // kept under the policy's rules; for a double |H| equals the heat-bath
 // weight |<ij||ab>| bit for bit, so the table cut w >= cut is applied to
 // the element.  Results are identical to the candidate walk in gen.cuh.
+//
+// The single-pass build runs in stages: k_vv_arena walks the rows and
+// records their members in warp-private arena chunks (single excitations
+// also in a per-warp list), k_vv_singles evaluates the singles one per
+// thread, k_vv_eval turns each row's members into entries in place,
+// k_vv_big / k_vv_eval_long / k_vv_compact_long handle rows longer than a
+// chunk, and k_vv_compact gathers the CSR.  k_vv_twopass is the exact
+// fallback when the arena runs out.
 #include <cub/cub.cuh>
 #include <cuda/std/tuple>
 
