@@ -24,20 +24,20 @@ struct Csr {
 
 // Column-panel layout of a square FP32 operator block (panel.cu).
 struct Panels {
-    i64 nr = 0, nc = 0, nnz = 0, nblocks = 0, npanels = 0, nseg = 0;
-    int group = 1;             // lanes per row
+    i64 nr = 0, nc = 0, nnz = 0, npanels = 0, nslices = 0, nent = 0, nchunks = 0;
+    int grid = 0;              // CTAs the slice split was made for
     bool ready = false;
-    DBuf<i64> blk_seg;         // per row block: its segments
-    DBuf<u32> seg_panel;       // per segment: panel
-    DBuf<i64> seg_base;        // per segment: first entry
-    DBuf<u16> seg_len;         // per segment: length of each row of the block
-    DBuf<u16> col;             // per entry: column offset in the panel
-    DBuf<float> val;           // per entry: FP32 value
-    DBuf<float> part;          // per panel group and row: Dot2 partial (2 floats)
-    DBuf<u8> flag;             // per (row block, panel group): partial written
+    DBuf<u16> col;             // per slot: column offset in the panel (k-major in a slice)
+    DBuf<float> val;           // per slot: FP32 value (0 in padding slots)
+    DBuf<i64> soff;            // per slice: first slot
+    DBuf<u32> swidth;          // per slice: entries of its longest chunk
+    DBuf<u32> schunk;          // per slice and lane: its chunk's place in row order (~0u: none)
+    DBuf<u32> split;           // per panel: slice range of each CTA (grid + 1 bounds)
+    DBuf<i64> rptr;            // per row: first of its chunks in row order
+    DBuf<float> part;          // per chunk, in row order: Dot2 partial (2 floats)
     size_t bytes() const {
-        return blk_seg.bytes() + seg_panel.bytes() + seg_base.bytes() + seg_len.bytes() +
-               col.bytes() + val.bytes() + part.bytes() + flag.bytes();
+        return col.bytes() + val.bytes() + soff.bytes() + swidth.bytes() + schunk.bytes() +
+               split.bytes() + rptr.bytes() + part.bytes();
     }
 };
 

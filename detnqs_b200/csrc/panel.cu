@@ -1,30 +1,35 @@
 // panel.cu -- column-panel layout of the FP32 operator for H.psi.
 //
-// The CSR H.psi gathers x[col] from L2 for every element: one 32-byte
-// sector per 4-byte value, which on B200 costs more than streaming the CSR
-// itself (measured: 0.90 ms with gathers, 0.35 ms without, on the
-// 1e6-determinant space).  This layout moves the gathers to shared memory:
+// The CSR H.psi gathers x[col] through L1 for every element: one 32-byte
+// sector per 4-byte value, and an SM's L1 returns about one sector per
+// clock, which bounds the CSR kernel (ncu: 1.0 sector per SM clock).  This
+// layout moves the gathers to shared memory:
 //
-//   rows in blocks of kRB, columns in panels of kPW;
-//   entries of a block reordered panel by panel, rows ascending inside a
-//   panel, the row's own order kept inside (row, panel);
-//   per entry: column offset in its panel (u16) + FP32 value (6 bytes);
-//   per non-empty (block, panel) "segment": panel, first entry, and the
-//   kRB row lengths (u16).
+//   columns in panels of kPW (192 KB of FP32 x: one panel fills a CTA's
+//   shared memory); a row's entries in a panel are cut into chunks of at
+//   most kChunkLen, in CSR order; the chunks of a panel, ordered by length
+//   (longest first), form slices of 32 chunks; a slice stores its entries
+//   k-major (slot k * 32 + lane holds entry k of the slice's chunk `lane`),
+//   padded to the slice's longest chunk with zero values: column offset in
+//   the panel (u16) + FP32 value, 6 bytes per slot.  The chunk length bounds
+//   the serial work of a lane, so rows of thousands of entries in one panel
+//   do not hold a warp.
 //
-// One CTA per row block: for each of its segments the CTA loads the x
-// panel into shared memory, scans the row lengths, and its lane groups
-// accumulate Dot2 (TwoProduct + TwoSum) pairs per row in shared memory,
-// panel after panel; y = (s + c) + diag * x in FP64.  The result is the
-// compensated FP32 operator of spmv.cu with another order of
-// accumulation (same accuracy class); it is deterministic and depends on
-// the matrix only.
+// One CTA per SM, persistent: panel after panel it loads x's panel into
+// shared memory and its warps run their share of the panel's slices (split
+// by slots), a lane summing its chunk's entries as a Dot2 (TwoProduct +
+// TwoSum) pair.  The pair of each chunk is stored; a finishing kernel
+// merges a row's chunk pairs in (panel, chunk) order and adds diag * x in
+// FP64.  The result is the compensated FP32 operator with another order of
+// accumulation (same accuracy class), and deterministic: a chunk's sum is
+// one lane's, in CSR order, whichever CTA runs it.
 //
-// Measured on the 1e6-determinant heat-bath space it is slower than the CSR
-// kernel (5.7 ms against 1.0 ms): each row contributes ~3.5 entries to each
-// 64 KB panel, and the rows of a block, some with thousands of entries,
-// share the block's barriers, so every segment waits for its longest row.
-// It is therefore off by default (DNQ_OPT_SPMV_PANELS).
+// Measured on the 1e6-determinant heat-bath space it is still slower than
+// the CSR kernel (1.37 ms against 1.0 ms): a row keeps ~13 entries per panel,
+// so a lane's chunk is short and each warp step waits a full memory latency
+// for four of them; loading sixteen ahead wasted more than it hid (2.5 ms).
+// It is therefore off by default (DNQ_OPT_SPMV_PANELS).  The first layout
+// (row blocks x 16k-column panels, one CTA per block) took 5.7 ms.
 #include <cub/cub.cuh>
 
 #include <vector>
@@ -34,11 +39,10 @@
 namespace dnq {
 namespace {
 
-constexpr int kPShift = 14;
-constexpr int kPW = 1 << kPShift;   // columns per panel: 64 KB of FP32 x
-constexpr int kRB = 2048;           // rows per block
-constexpr int kPT = 512;            // threads per CTA
-constexpr int kItems = kRB / kPT;   // row lengths scanned per thread
+constexpr i64 kPW = 49152;          // columns per panel (192 KB of FP32 x)
+constexpr u32 kChunkLen = 64;       // entries of a row in a panel per chunk
+constexpr int kPT = 1024;           // threads per CTA
+constexpr u32 kNoRow = 0xffffffffu;
 
 __device__ __forceinline__ void ts(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
@@ -64,12 +68,15 @@ struct Pair32 {
     }
 };
 
+int pg(i64 n) {
+    const i64 b = (n + 255) / 256;
+    return (int)std::max<i64>(1, std::min<i64>(b, 65535));
+}
+
 // ---- layout construction -------------------------------------------------
 
-// key = ((block * npanels + panel) << rbits) | row in block; row of each
-// entry by binary search of the row pointers.
-__global__ void k_pkeys(const i64* rowptr, i64 nr, const u32* col, i64 nnz, i64 npanels,
-                        int rbits, u64* key, u32* idx) {
+// key = panel << 32 | row of every entry (row by binary search of rowptr).
+__global__ void k_pkeys(const i64* rowptr, i64 nr, const u32* col, i64 nnz, u64* key, u32* idx) {
     for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < nnz;
          k += (i64)gridDim.x * blockDim.x) {
         i64 lo = 0, hi = nr;
@@ -77,348 +84,396 @@ __global__ void k_pkeys(const i64* rowptr, i64 nr, const u32* col, i64 nnz, i64 
             const i64 mid = (lo + hi) >> 1;
             if (rowptr[mid] <= k) lo = mid; else hi = mid;
         }
-        const u64 blk = (u64)(lo / kRB), local = (u64)(lo % kRB);
-        const u64 pan = col[k] >> kPShift;
-        key[k] = ((blk * (u64)npanels + pan) << rbits) | local;
+        key[k] = ((u64)(col[k] / (u32)kPW) << 32) | (u64)lo;
         idx[k] = (u32)k;
     }
 }
 
-__global__ void k_pgather(const u64* skey, const u32* perm, const u32* col, const float* val32,
-                          i64 nnz, u16* ocol, float* oval, u32* seg_head, u32* row_head,
-                          int rbits) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nnz;
-         t += (i64)gridDim.x * blockDim.x) {
-        const u32 k = perm[t];
-        ocol[t] = (u16)(col[k] & (kPW - 1));
-        oval[t] = val32[k];
-        const u64 kk = skey[t];
-        seg_head[t] = (t == 0 || (skey[t - 1] >> rbits) != (kk >> rbits)) ? 1u : 0u;
-        row_head[t] = (t == 0 || skey[t - 1] != kk) ? 1u : 0u;
-    }
+__global__ void k_heads(const u64* skey, i64 n, u32* head) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        head[t] = (t == 0 || skey[t - 1] != skey[t]) ? 1u : 0u;
 }
 
-// At every segment head: its panel, block and first entry.
-__global__ void k_pseg(const u64* skey, const u32* seg_head, const u32* seg_id, i64 nnz,
-                       i64 npanels, int rbits, u32* seg_panel, u32* seg_block, i64* seg_base) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < nnz;
-         t += (i64)gridDim.x * blockDim.x) {
-        if (!seg_head[t]) continue;
-        const u32 s = seg_id[t] - 1;
-        const u64 bp = skey[t] >> rbits;
-        seg_panel[s] = (u32)(bp % (u64)npanels);
-        seg_block[s] = (u32)(bp / (u64)npanels);
-        seg_base[s] = t;
-    }
-}
-
-// Row lengths: for each row run (head positions listed), its length goes to
-// seg_len[segment * kRB + row in block].
-__global__ void k_plen(const u64* skey, const u32* rpos, i64 nruns, i64 nnz, const u32* seg_id,
-                       u16* seg_len) {
-    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nruns;
-         r += (i64)gridDim.x * blockDim.x) {
-        const i64 b = rpos[r], e = r + 1 < nruns ? (i64)rpos[r + 1] : nnz;
-        const u64 local = skey[b] & (u64)(kRB - 1);
-        seg_len[(i64)(seg_id[b] - 1) * kRB + (i64)local] = (u16)(e - b);
-    }
-}
-
-// First segment of every block (segments are sorted by block).
-__global__ void k_pblk(const u32* seg_block, i64 nseg, i64 nblocks, i64* blk_seg) {
-    for (i64 b = blockIdx.x * (i64)blockDim.x + threadIdx.x; b <= nblocks;
-         b += (i64)gridDim.x * blockDim.x) {
-        i64 lo = 0, hi = nseg;
-        while (lo < hi) {
-            const i64 mid = (lo + hi) >> 1;
-            if ((i64)seg_block[mid] < b) lo = mid + 1; else hi = mid;
-        }
-        blk_seg[b] = lo;
-    }
-}
-
-__global__ void k_piota(u32* p, i64 n) {
+__global__ void k_iota(u32* p, i64 n) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x)
         p[t] = (u32)t;
 }
 
-int pg(i64 n) {
-    const i64 b = (n + 255) / 256;
-    return (int)std::max<i64>(1, std::min<i64>(b, 65535));
+// Per (panel, row) pair: its entry count and chunk count.
+__global__ void k_pairs(const u32* pstart, i64 np, i64 n, u32* pcount, u32* pnch) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < np;
+         i += (i64)gridDim.x * blockDim.x) {
+        const i64 b = pstart[i], e = i + 1 < np ? (i64)pstart[i + 1] : n;
+        const u32 c = (u32)(e - b);
+        pcount[i] = c;
+        pnch[i] = (c + kChunkLen - 1) / kChunkLen;
+    }
+}
+
+// Chunks of every pair, in (panel, row, chunk) order: their pair, length,
+// the slicing key panel << 32 | (2^32 - 1 - length) (longest first) and the
+// gathering key row << 32 | panel << 16 | chunk.
+__global__ void k_chunks(const u64* skey, const u32* pstart, const u32* pcount, const i64* cpre,
+                         i64 np, u32* cpair, u32* clen, u64* skey_c, u64* rkey_c) {
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < np;
+         i += (i64)gridDim.x * blockDim.x) {
+        const u64 k = skey[pstart[i]];
+        const u64 panel = k >> 32, row = k & 0xffffffffull;
+        const u32 cnt = pcount[i];
+        for (u32 q = 0; q * kChunkLen < cnt; ++q) {
+            const i64 c = cpre[i] + q;
+            const u32 len = min(kChunkLen, cnt - q * kChunkLen);
+            cpair[c] = (u32)i;
+            clen[c] = len;
+            skey_c[c] = (panel << 32) | (u64)(0xffffffffu - len);
+            rkey_c[c] = (row << 32) | (panel << 16) | (u64)q;
+        }
+    }
+}
+
+// First sorted chunk of every panel.
+__global__ void k_panel_first(const u64* skey_s, i64 m, i64 npanels, u32* first) {
+    for (i64 p = blockIdx.x * (i64)blockDim.x + threadIdx.x; p <= npanels;
+         p += (i64)gridDim.x * blockDim.x) {
+        i64 lo = 0, hi = m;
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if ((i64)(skey_s[mid] >> 32) < p) lo = mid + 1; else hi = mid;
+        }
+        first[p] = (u32)lo;
+    }
+}
+
+// Sorted chunk j -> slice and lane; slice widths from their first chunk.
+__global__ void k_inverse(const u32* order, i64 m, u32* inv) {
+    for (i64 j = blockIdx.x * (i64)blockDim.x + threadIdx.x; j < m;
+         j += (i64)gridDim.x * blockDim.x)
+        inv[order[j]] = (u32)j;
+}
+
+// schunk holds the chunk's place in the row-ordered list: its partial is
+// written there, so a row's partials are contiguous for the merge.
+__global__ void k_slices(const u32* order, const u64* skey_s, const u32* pfirst, const i64* sfirst,
+                         const u32* clen, const u32* rpos, i64 m, u32* cslot, u32* swidth,
+                         u32* schunk) {
+    for (i64 j = blockIdx.x * (i64)blockDim.x + threadIdx.x; j < m;
+         j += (i64)gridDim.x * blockDim.x) {
+        const u32 p = (u32)(skey_s[j] >> 32);
+        const i64 rank = j - (i64)pfirst[p];
+        const i64 s = sfirst[p] + rank / 32;
+        const u32 lane = (u32)(rank % 32);
+        const u32 c = order[j];
+        cslot[c] = (u32)(s * 32 + lane);
+        if (lane == 0) swidth[s] = clen[c];
+        schunk[s * 32 + lane] = rpos[c];
+    }
+}
+
+__global__ void k_slots(const u32* swidth, i64 ns, i64* slots) {
+    for (i64 s = blockIdx.x * (i64)blockDim.x + threadIdx.x; s < ns;
+         s += (i64)gridDim.x * blockDim.x)
+        slots[s] = (i64)swidth[s] * 32;
+}
+
+// Entry t of the (panel, row)-sorted order -> its slot.
+__global__ void k_scatter(const u64* skey, const u32* perm, const u32* pair_id, const u32* pstart,
+                          const i64* cpre, const u32* cslot, const i64* soff, const u32* col,
+                          const float* val32, i64 n, u16* ocol, float* oval) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        const u32 i = pair_id[t] - 1;
+        const i64 k = t - (i64)pstart[i];
+        const u32 sl = cslot[cpre[i] + k / kChunkLen];
+        const i64 dst = soff[sl / 32] + (k % kChunkLen) * 32 + (sl % 32);
+        const u32 e = perm[t];
+        ocol[dst] = (u16)(col[e] - (u32)((skey[t] >> 32) * (u64)kPW));
+        oval[dst] = val32[e];
+    }
+}
+
+// First chunk of every row in the row-sorted chunk keys.
+__global__ void k_row_first(const u64* rkey_s, i64 m, i64 nr, i64* rptr) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r <= nr;
+         r += (i64)gridDim.x * blockDim.x) {
+        i64 lo = 0, hi = m;
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if ((i64)(rkey_s[mid] >> 32) < r) lo = mid + 1; else hi = mid;
+        }
+        rptr[r] = lo;
+    }
+}
+
+// Slice bounds of every CTA in every panel, by slots.
+__global__ void k_split(const i64* sfirst, const i64* soff, i64 npanels, int grid, u32* split) {
+    for (i64 q = blockIdx.x * (i64)blockDim.x + threadIdx.x; q < npanels * (grid + 1);
+         q += (i64)gridDim.x * blockDim.x) {
+        const i64 p = q / (grid + 1), c = q % (grid + 1);
+        const i64 s0 = sfirst[p], s1 = sfirst[p + 1];
+        if (c == grid) {
+            split[q] = (u32)s1;
+            continue;
+        }
+        const i64 target = soff[s0] + (soff[s1] - soff[s0]) * c / grid;
+        i64 lo = s0, hi = s1;   // first slice starting at or after target
+        while (lo < hi) {
+            const i64 mid = (lo + hi) >> 1;
+            if (soff[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        split[q] = (u32)lo;
+    }
 }
 
 // ---- H.psi -----------------------------------------------------------------
 
-struct PanelView {
-    i64 nr, nc, nblocks;
-    const i64* blk_seg;
-    const u32* seg_panel;
-    const i64* seg_base;
-    const u16* seg_len;
+struct SliceView {
+    i64 nr, nc, npanels;
     const u16* col;
     const float* val;
+    const i64* soff;
+    const u32* swidth;
+    const u32* schunk;
+    const u32* split;
 };
 
-constexpr int kPGS = 8;   // panels per task: a CTA sums one group of panels of one row block
-
-// One CTA per (row block, group of kPGS panels): the group's segments of the
-// block are summed into per-row Dot2 pairs, written as the group's partial
-// (flag[task] says whether the group had any segment).
-template <int G, int D, int RR>
-__global__ void __launch_bounds__(kPT, 2) k_spmv_panel(PanelView P, i64 ngroups_p,
-                                                    const float* __restrict__ x32,
-                                                    float2* __restrict__ part,
-                                                    u8* __restrict__ flag) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    float* xs = reinterpret_cast<float*>(smem);                         // kPW
-    float2* acc = reinterpret_cast<float2*>(smem + kPW * 4);            // kRB
-    u32* offs = reinterpret_cast<u32*>(smem + kPW * 4 + kRB * 8);       // kRB + 1
-    using Scan = cub::BlockScan<u32, kPT>;
-    __shared__ typename Scan::TempStorage scan_tmp;
-    __shared__ i64 seg_lo, seg_hi;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int sub = lane & (G - 1);
-    const int group = tid / G, ngroups = kPT / G;
-    const i64 ntasks = P.nblocks * ngroups_p;
-    for (i64 task = blockIdx.x; task < ntasks; task += gridDim.x) {
-        const i64 b = task / ngroups_p, pg = task % ngroups_p;
-        const i64 row0 = b * kRB;
-        const int nrow = (int)min((i64)kRB, P.nr - row0);
-        if (tid == 0) {   // segments of block b with panel in [pg*kPGS, (pg+1)*kPGS)
-            const i64 s0 = P.blk_seg[b], s1 = P.blk_seg[b + 1];
-            i64 lo = s0, hi = s1;
-            while (lo < hi) {
-                const i64 mid = (lo + hi) >> 1;
-                if ((i64)P.seg_panel[mid] < pg * kPGS) lo = mid + 1; else hi = mid;
-            }
-            seg_lo = lo;
-            hi = s1;
-            while (lo < hi) {
-                const i64 mid = (lo + hi) >> 1;
-                if ((i64)P.seg_panel[mid] < (pg + 1) * kPGS) lo = mid + 1; else hi = mid;
-            }
-            seg_hi = lo;
-        }
-        for (int r = tid; r < kRB; r += kPT) acc[r] = make_float2(0.0f, 0.0f);
+// Persistent: one CTA per SM, panel after panel.
+__global__ void __launch_bounds__(kPT, 1) k_spmv_slices(SliceView V, const float* __restrict__ x32,
+                                                        float2* __restrict__ part) {
+    extern __shared__ __align__(16) float xs[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (i64 p = 0; p < V.npanels; ++p) {
+        const i64 c0 = p * kPW;
+        const int ncol = (int)min(kPW, V.nc - c0);
+        const float* xp = x32 + c0;   // c0 is a multiple of 4 floats (16 bytes)
+        for (int t = tid; t < (ncol >> 2); t += kPT)
+            reinterpret_cast<float4*>(xs)[t] = __ldg(reinterpret_cast<const float4*>(xp) + t);
+        for (int t = (ncol & ~3) + tid; t < ncol; t += kPT) xs[t] = __ldg(xp + t);
         __syncthreads();
-        const i64 g0 = seg_lo, g1 = seg_hi;
-        if (tid == 0) flag[task] = g1 > g0 ? 1 : 0;
-        for (i64 sg = g0; sg < g1; ++sg) {
-            const i64 c0 = (i64)P.seg_panel[sg] << kPShift;
-            const int ncol = (int)min((i64)kPW, P.nc - c0);
-            const float* xp = x32 + c0;
-            if ((ncol & 3) == 0) {
-                for (int t = tid; t < (ncol >> 2); t += kPT)
-                    reinterpret_cast<float4*>(xs)[t] = __ldg(reinterpret_cast<const float4*>(xp) + t);
-            } else {
-                for (int t = tid; t < ncol; t += kPT) xs[t] = __ldg(xp + t);
-            }
-            u32 len[kItems];
-            const u16* lp = P.seg_len + sg * kRB + tid * kItems;
-#pragma unroll
-            for (int q = 0; q < kItems; ++q) len[q] = lp[q];
-            u32 ex[kItems];
-            Scan(scan_tmp).ExclusiveSum(len, ex);
-#pragma unroll
-            for (int q = 0; q < kItems; ++q) offs[tid * kItems + q] = ex[q];
-            if (tid == kPT - 1) offs[kRB] = ex[kItems - 1] + len[kItems - 1];
-            __syncthreads();
-            const u16* cp = P.col + P.seg_base[sg];
-            const float* vp = P.val + P.seg_base[sg];
-            // rows handed out in rounds of ngroups (every lane of a warp runs
-            // the same rounds: the group shuffles need all lanes).  RR rounds
-            // at a time, D slots per lane each, are loaded before any is
-            // used, so one memory latency covers RR*D entries per lane.
-            for (int r0 = 0; r0 < nrow; r0 += ngroups * RR) {
-                u32 bb[RR], ee[RR];
-#pragma unroll
-                for (int q = 0; q < RR; ++q) {
-                    const int r = r0 + q * ngroups + group;
-                    const bool on = r < nrow;
-                    bb[q] = on ? offs[r] : 0u;
-                    ee[q] = on ? offs[r + 1] : 0u;
-                }
-                Pair32 a[RR];
-                u32 kb[RR];
-#pragma unroll
-                for (int q = 0; q < RR; ++q) kb[q] = bb[q] + sub;
-                bool more = true;
-                while (more) {
-                    float v[RR][D];
-                    u32 c[RR][D];
-#pragma unroll
-                    for (int q = 0; q < RR; ++q)
-#pragma unroll
-                        for (int d = 0; d < D; ++d) {
-                            const u32 k = kb[q] + (u32)(d * G);
-                            const bool ok = k < ee[q];
-                            v[q][d] = ok ? __ldcs(vp + k) : 0.0f;
-                            c[q][d] = ok ? (u32)__ldcs(cp + k) : 0u;
-                        }
-                    more = false;
-#pragma unroll
-                    for (int q = 0; q < RR; ++q) {
-#pragma unroll
-                        for (int d = 0; d < D; ++d)
-                            if (kb[q] + (u32)(d * G) < ee[q]) a[q].add_prod(v[q][d], xs[c[q][d]]);
-                        kb[q] += (u32)(D * G);
-                        more = more || kb[q] < ee[q];
-                    }
-                    more = __any_sync(0xffffffffu, more);
-                }
-#pragma unroll
-                for (int q = 0; q < RR; ++q) {
-                    Pair32 t = a[q];
-#pragma unroll
-                    for (int o = G / 2; o; o >>= 1)
-                        t.merge(__shfl_xor_sync(0xffffffffu, t.s, o, G),
-                                __shfl_xor_sync(0xffffffffu, t.c, o, G));
-                    const int r = r0 + q * ngroups + group;
-                    if (sub == 0 && r < nrow && ee[q] > bb[q]) {
-                        Pair32 u;
-                        u.s = acc[r].x;
-                        u.c = acc[r].y;
-                        u.merge(t.s, t.c);
-                        acc[r] = make_float2(u.s, u.c);
-                    }
-                }
-            }
-            __syncthreads();   // xs / offs free for the next segment
+        const u32* sp = V.split + p * (gridDim.x + 1);
+        const u32 s0 = sp[blockIdx.x], s1 = sp[blockIdx.x + 1];
+        // the next slice's offset, width and chunk are loaded while the
+        // current one is summed
+        u32 s = s0 + warp;
+        i64 nbase = 0;
+        u32 nw = 0, nchunk = kNoRow;
+        if (s < s1) {
+            nbase = V.soff[s];
+            nw = V.swidth[s];
+            nchunk = V.schunk[(i64)s * 32 + lane];
         }
-        if (g1 > g0)
-            for (int r = tid; r < nrow; r += kPT) part[pg * P.nr + row0 + r] = acc[r];
-        __syncthreads();
+        for (; s < s1; s += kPT / 32) {
+            const i64 base = nbase + lane;
+            const u32 w = nw, chunk = nchunk;
+            const u32 sn = s + kPT / 32;
+            if (sn < s1) {
+                nbase = V.soff[sn];
+                nw = V.swidth[sn];
+                nchunk = V.schunk[(i64)sn * 32 + lane];
+            }
+            Pair32 a;
+            u32 k = 0;
+            for (; k + 4 <= w; k += 4) {
+                float v[4];
+                u32 c[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    v[q] = __ldcs(V.val + base + (i64)(k + q) * 32);
+                    c[q] = __ldcs(V.col + base + (i64)(k + q) * 32);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) a.add_prod(v[q], xs[c[q]]);
+            }
+            for (; k < w; ++k)
+                a.add_prod(__ldcs(V.val + base + (i64)k * 32), xs[__ldcs(V.col + base + (i64)k * 32)]);
+            if (chunk != kNoRow) part[chunk] = make_float2(a.s, a.c);
+        }
+        __syncthreads();   // xs free for the next panel
     }
 }
 
-// y = merge of the groups' partials in group order + diag * x (FP64).
-__global__ void k_panel_finish(const float2* part, const u8* flag, i64 nr, i64 ngroups_p,
-                               const double* diag, const double* x, double* y) {
+// y = merge of a row's chunk pairs in (panel, chunk) order (contiguous in
+// part) + diag * x (FP64).
+__global__ void k_slices_finish(const float2* part, const i64* rptr, i64 nr, const double* diag,
+                                const double* x, double* y) {
     for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
          r += (i64)gridDim.x * blockDim.x) {
-        const i64 b = r / kRB;
         Pair32 a;
-        for (i64 pg = 0; pg < ngroups_p; ++pg)
-            if (flag[b * ngroups_p + pg]) {
-                const float2 p = part[pg * nr + r];
-                a.merge(p.x, p.y);
-            }
+        for (i64 j = rptr[r]; j < rptr[r + 1]; ++j) {
+            const float2 q = part[j];
+            a.merge(q.x, q.y);
+        }
         double v = (double)a.s + (double)a.c;
         if (diag) v += diag[r] * x[r];
         y[r] = v;
     }
 }
 
-size_t panel_smem() { return (size_t)kPW * 4 + (size_t)kRB * 8 + (size_t)(kRB + 1) * 4; }
-
-template <int G, int D, int RR>
-void launch_panel(const PanelView& v, i64 ngroups_p, const float* x32, float2* part, u8* flag,
-                  int device, cudaStream_t s) {
-    auto kern = k_spmv_panel<G, D, RR>;
-    const size_t sm = panel_smem();
-    DNQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    int per_sm = 0;
-    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPT, sm));
-    const i64 ntasks = v.nblocks * ngroups_p;
-    const i64 grid = std::min<i64>(ntasks, (i64)std::max(1, per_sm) * sm_count(device) * 8);
-    kern<<<(unsigned)std::max<i64>(1, grid), kPT, sm, s>>>(v, ngroups_p, x32, part, flag);
-    DNQ_CHECK_LAUNCH();
-}
+size_t panel_smem() { return (size_t)kPW * 4; }
 
 }  // namespace
 
 // Build the panel layout of a square block from its FP32 value copy
-// (diagonal already split off).  Temporary memory: ~24 bytes per entry.
-void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s) {
-    P.nr = m.nr;
-    P.nc = m.nc;
-    P.nnz = m.nnz;
-    P.nblocks = (m.nr + kRB - 1) / kRB;
-    const i64 npanels = std::max<i64>(1, (m.nc + kPW - 1) >> kPShift);
+// (diagonal already split off).  Temporary memory: ~60 bytes per entry.
+void build_panels(const Csr& M, const float* val32, Panels& P, cudaStream_t s) {
+    P.nr = M.nr;
+    P.nc = M.nc;
+    P.nnz = M.nnz;
+    const i64 npanels = std::max<i64>(1, (M.nc + kPW - 1) / kPW);
     P.npanels = npanels;
-    const i64 n = m.nnz;
-    P.col.alloc(n, s);
-    P.val.alloc(n, s);
-    P.blk_seg.alloc(P.nblocks + 1, s);
+    int dev = 0;
+    DNQ_CUDA(cudaGetDevice(&dev));
+    P.grid = sm_count(dev);
+    const i64 n = M.nnz;
+    P.rptr.alloc(M.nr + 1, s);
     if (n == 0) {
-        P.nseg = 0;
-        DNQ_CUDA(cudaMemsetAsync(P.blk_seg.p, 0, (P.nblocks + 1) * 8, s));
-        P.seg_panel.alloc(1, s);
-        P.seg_base.alloc(1, s);
-        P.seg_len.alloc(1, s);
-        P.part.alloc(2 * std::max<i64>(1, m.nr), s);
-        P.flag.alloc(std::max<i64>(1, P.nblocks), s);
-        DNQ_CUDA(cudaMemsetAsync(P.flag.p, 0, std::max<i64>(1, P.nblocks), s));
+        P.nslices = 0;
+        P.nent = 0;
+        P.nchunks = 0;
+        P.col.alloc(1, s);
+        P.val.alloc(1, s);
+        P.soff.alloc(1, s);
+        P.swidth.alloc(1, s);
+        P.schunk.alloc(32, s);
+        P.part.alloc(2, s);
+        P.split.alloc((size_t)npanels * (P.grid + 1), s);
+        DNQ_CUDA(cudaMemsetAsync(P.split.p, 0, P.split.bytes(), s));
+        DNQ_CUDA(cudaMemsetAsync(P.rptr.p, 0, P.rptr.bytes(), s));
+        DNQ_CUDA(cudaStreamSynchronize(s));
         P.ready = true;
         return;
     }
-    require(n < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "panel layout: more than 2^32 entries");
-    const int rbits = 11;   // log2(kRB)
-    int kbits = rbits;
-    while (kbits < 64 && ((u64)1 << (kbits - rbits)) < (u64)(P.nblocks * npanels)) ++kbits;
+    require(n < (i64)0x7fffffffll, DNQ_ERR_OVERFLOW, "panel layout: more than 2^31 entries");
+    require(npanels < 65536, DNQ_ERR_OVERFLOW, "panel layout: more than 65535 panels");
+    int pbits = 1;
+    while (((i64)1 << pbits) < npanels + 1) ++pbits;
+    // entries by (panel, row), stably: a row's entries of a panel keep their order
     DBuf<u64> key(n, s), skey(n, s);
     DBuf<u32> idx(n, s), perm(n, s);
-    k_pkeys<<<pg(n), 256, 0, s>>>(m.rowptr.p, m.nr, m.col.p, n, npanels, rbits, key.p, idx.p);
+    k_pkeys<<<pg(n), 256, 0, s>>>(M.rowptr.p, M.nr, M.col.p, n, key.p, idx.p);
     DNQ_CHECK_LAUNCH();
     {
         size_t tmp = 0;
         DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, skey.p, idx.p, perm.p, n, 0,
-                                                 kbits, s));
+                                                 32 + pbits, s));
         DBuf<u8> tb(tmp, s);
         DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, key.p, skey.p, idx.p, perm.p, n, 0,
-                                                 kbits, s));
+                                                 32 + pbits, s));
     }
     key.release();
     idx.release();
-    DBuf<u32> seg_head(n, s), row_head(n, s), seg_id(n, s);
-    k_pgather<<<pg(n), 256, 0, s>>>(skey.p, perm.p, m.col.p, val32, n, P.col.p, P.val.p,
-                                    seg_head.p, row_head.p, rbits);
+    // (panel, row) pairs: first entry
+    DBuf<u32> head(n, s), pair_id(n, s), pos(n, s), pstart(n, s);
+    DBuf<i64> npair_d(1, s);
+    k_heads<<<pg(n), 256, 0, s>>>(skey.p, n, head.p);
     DNQ_CHECK_LAUNCH();
-    perm.release();
+    k_iota<<<pg(n), 256, 0, s>>>(pos.p, n);
+    DNQ_CHECK_LAUNCH();
     {
         size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, seg_head.p, seg_id.p, n, s));
+        DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, pos.p, head.p, pstart.p, npair_d.p, n, s));
         DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb.p, tmp, seg_head.p, seg_id.p, n, s));
+        DNQ_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, pos.p, head.p, pstart.p, npair_d.p, n, s));
+        size_t t2 = 0;
+        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t2, head.p, pair_id.p, n, s));
+        DBuf<u8> tb2(t2, s);
+        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb2.p, t2, head.p, pair_id.p, n, s));
     }
-    u32 nseg = 0;
-    DNQ_CUDA(cudaMemcpyAsync(&nseg, seg_id.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
+    pos.release();
+    head.release();
+    i64 np = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&np, npair_d.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
-    P.nseg = nseg;
-    P.seg_panel.alloc(nseg, s);
-    P.seg_base.alloc(nseg, s);
-    P.seg_len.alloc((size_t)nseg * kRB, s);
-    DNQ_CUDA(cudaMemsetAsync(P.seg_len.p, 0, (size_t)nseg * kRB * 2, s));
-    DBuf<u32> seg_block(nseg, s);
-    k_pseg<<<pg(n), 256, 0, s>>>(skey.p, seg_head.p, seg_id.p, n, npanels, rbits, P.seg_panel.p,
-                                 seg_block.p, P.seg_base.p);
+    // chunks of every pair
+    DBuf<u32> pcount(np, s), pnch(np + 1, s);
+    DBuf<i64> cpre(np + 1, s);
+    k_pairs<<<pg(np), 256, 0, s>>>(pstart.p, np, n, pcount.p, pnch.p);
     DNQ_CHECK_LAUNCH();
-    {   // row runs
-        DBuf<u32> pos(n, s), rpos(n, s);
-        DBuf<i64> nr(1, s);
-        k_piota<<<pg(n), 256, 0, s>>>(pos.p, n);
+    DNQ_CUDA(cudaMemsetAsync(pnch.p + np, 0, 4, s));
+    {
+        size_t tmp = 0;
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, pnch.p, cpre.p, np + 1, s));
+        DBuf<u8> tb(tmp, s);
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, pnch.p, cpre.p, np + 1, s));
+    }
+    i64 mc = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&mc, cpre.p + np, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    P.nchunks = mc;
+    DBuf<u32> cpair(mc, s), clen(mc, s), ciota(mc, s), corder(mc, s), rorder(mc, s);
+    DBuf<u64> ckey(mc, s), sckey(mc, s), rkey(mc, s), srkey(mc, s);
+    k_chunks<<<pg(np), 256, 0, s>>>(skey.p, pstart.p, pcount.p, cpre.p, np, cpair.p, clen.p,
+                                    ckey.p, rkey.p);
+    DNQ_CHECK_LAUNCH();
+    k_iota<<<pg(mc), 256, 0, s>>>(ciota.p, mc);
+    DNQ_CHECK_LAUNCH();
+    {   // slicing order: panel, then length (longest first); row order: row, panel, chunk
+        size_t tmp = 0;
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ckey.p, sckey.p, ciota.p, corder.p,
+                                                 mc, 0, 32 + pbits, s));
+        DBuf<u8> tb(tmp, s);
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, ckey.p, sckey.p, ciota.p, corder.p,
+                                                 mc, 0, 32 + pbits, s));
+        size_t t2 = 0;
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, rkey.p, srkey.p, ciota.p, rorder.p,
+                                                 mc, 0, 64, s));
+        DBuf<u8> tb2(t2, s);
+        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb2.p, t2, rkey.p, srkey.p, ciota.p, rorder.p,
+                                                 mc, 0, 64, s));
+    }
+    DBuf<u32> pfirst(npanels + 1, s);
+    k_panel_first<<<pg(npanels + 1), 256, 0, s>>>(sckey.p, mc, npanels, pfirst.p);
+    DNQ_CHECK_LAUNCH();
+    std::vector<u32> hfirst(npanels + 1);
+    DNQ_CUDA(cudaMemcpyAsync(hfirst.data(), pfirst.p, 4 * (npanels + 1), cudaMemcpyDeviceToHost,
+                             s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    std::vector<i64> hsf(npanels + 1, 0);
+    for (i64 p = 0; p < npanels; ++p)
+        hsf[p + 1] = hsf[p] + ((i64)hfirst[p + 1] - hfirst[p] + 31) / 32;
+    const i64 ns = hsf[npanels];
+    P.nslices = ns;
+    DBuf<i64> sfirst(npanels + 1, s);
+    DNQ_CUDA(cudaMemcpyAsync(sfirst.p, hsf.data(), 8 * (npanels + 1), cudaMemcpyHostToDevice, s));
+    P.swidth.alloc(std::max<i64>(1, ns), s);
+    P.schunk.alloc((size_t)std::max<i64>(1, ns) * 32, s);
+    DNQ_CUDA(cudaMemsetAsync(P.schunk.p, 0xff, P.schunk.bytes(), s));
+    DBuf<u32> cslot(mc, s), rpos(mc, s);
+    k_inverse<<<pg(mc), 256, 0, s>>>(rorder.p, mc, rpos.p);   // chunk -> its place in row order
+    DNQ_CHECK_LAUNCH();
+    k_slices<<<pg(mc), 256, 0, s>>>(corder.p, sckey.p, pfirst.p, sfirst.p, clen.p, rpos.p, mc,
+                                    cslot.p, P.swidth.p, P.schunk.p);
+    DNQ_CHECK_LAUNCH();
+    // slot offsets of the slices
+    P.soff.alloc(ns + 1, s);
+    {
+        DBuf<i64> slots(ns + 1, s);
+        DNQ_CUDA(cudaMemsetAsync(slots.p + ns, 0, 8, s));
+        k_slots<<<pg(ns), 256, 0, s>>>(P.swidth.p, ns, slots.p);
         DNQ_CHECK_LAUNCH();
         size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, pos.p, row_head.p, rpos.p, nr.p, n, s));
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, slots.p, P.soff.p, ns + 1, s));
         DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, pos.p, row_head.p, rpos.p, nr.p, n, s));
-        i64 nruns = 0;
-        DNQ_CUDA(cudaMemcpyAsync(&nruns, nr.p, 8, cudaMemcpyDeviceToHost, s));
-        DNQ_CUDA(cudaStreamSynchronize(s));
-        k_plen<<<pg(nruns), 256, 0, s>>>(skey.p, rpos.p, nruns, n, seg_id.p, P.seg_len.p);
-        DNQ_CHECK_LAUNCH();
+        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, slots.p, P.soff.p, ns + 1, s));
     }
-    k_pblk<<<pg(P.nblocks + 1), 256, 0, s>>>(seg_block.p, nseg, P.nblocks, P.blk_seg.p);
+    DNQ_CUDA(cudaMemcpyAsync(&P.nent, P.soff.p + ns, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    P.col.alloc(std::max<i64>(1, P.nent), s);
+    P.val.alloc(std::max<i64>(1, P.nent), s);
+    DNQ_CUDA(cudaMemsetAsync(P.col.p, 0, P.col.bytes(), s));
+    DNQ_CUDA(cudaMemsetAsync(P.val.p, 0, P.val.bytes(), s));
+    k_scatter<<<pg(n), 256, 0, s>>>(skey.p, perm.p, pair_id.p, pstart.p, cpre.p, cslot.p,
+                                    P.soff.p, M.col.p, val32, n, P.col.p, P.val.p);
     DNQ_CHECK_LAUNCH();
-    // lanes per row by the average entries of a (row, segment)
-    const double avg = (double)n / ((double)nseg * kRB);
-    P.group = avg >= 48 ? 32 : avg >= 16 ? 8 : avg >= 6 ? 4 : 1;
-    {
-        const i64 ngp = (npanels + kPGS - 1) / kPGS;
-        P.part.alloc((size_t)ngp * m.nr * 2, s);
-        P.flag.alloc((size_t)P.nblocks * ngp, s);
-    }
+    // chunks of every row in (panel, chunk) order, for the finishing merge
+    k_row_first<<<pg(M.nr + 1), 256, 0, s>>>(srkey.p, mc, M.nr, P.rptr.p);
+    DNQ_CHECK_LAUNCH();
+    P.part.alloc((size_t)std::max<i64>(1, mc) * 2, s);
+    P.split.alloc((size_t)npanels * (P.grid + 1), s);
+    k_split<<<pg(npanels * (P.grid + 1)), 256, 0, s>>>(sfirst.p, P.soff.p, npanels, P.grid,
+                                                       P.split.p);
+    DNQ_CHECK_LAUNCH();
     DNQ_CUDA(cudaStreamSynchronize(s));
     P.ready = true;
 }
@@ -426,18 +481,19 @@ void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s) {
 // y = M x with the panel layout (x32: the FP32 copy of x, nc floats).
 void spmv_panels(const Panels& P, const float* x32, const double* diag, const double* x,
                  double* y, int device, cudaStream_t s) {
+    (void)device;
     if (P.nr == 0) return;
-    PanelView v{P.nr, P.nc, P.nblocks, P.blk_seg.p, P.seg_panel.p, P.seg_base.p, P.seg_len.p,
-                P.col.p, P.val.p};
-    const i64 ngp = (P.npanels + kPGS - 1) / kPGS;
     float2* part = reinterpret_cast<float2*>(P.part.p);
-    switch (P.group) {
-        case 32: launch_panel<32, 4, 1>(v, ngp, x32, part, P.flag.p, device, s); break;
-        case 8: launch_panel<8, 2, 2>(v, ngp, x32, part, P.flag.p, device, s); break;
-        case 4: launch_panel<4, 2, 4>(v, ngp, x32, part, P.flag.p, device, s); break;
-        default: launch_panel<1, 4, 4>(v, ngp, x32, part, P.flag.p, device, s); break;
+    if (P.nslices) {
+        SliceView v{P.nr, P.nc, P.npanels, P.col.p, P.val.p, P.soff.p, P.swidth.p, P.schunk.p,
+                    P.split.p};
+        const size_t sm = panel_smem();
+        DNQ_CUDA(cudaFuncSetAttribute(k_spmv_slices, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sm));
+        k_spmv_slices<<<P.grid, kPT, sm, s>>>(v, x32, part);
+        DNQ_CHECK_LAUNCH();
     }
-    k_panel_finish<<<pg(P.nr), 256, 0, s>>>(part, P.flag.p, P.nr, ngp, diag, x, y);
+    k_slices_finish<<<pg(P.nr), 256, 0, s>>>(part, P.rptr.p, P.nr, diag, x, y);
     DNQ_CHECK_LAUNCH();
 }
 

@@ -466,14 +466,14 @@ def test_spmv_every_lane_and_slot_count(core):
 
 
 def test_fp32_panel_layout_matches_csr_and_scipy(core):
-    """The column-panel FP32 operator (x staged in shared memory) over
-    several panels and row blocks: same results as the CSR FP32 kernel to
-    compensated precision, FP64 SciPy to FP32-value precision, and the same
-    bits on every call."""
+    """The column-panel FP32 operator (x staged in shared memory, rows in
+    slices of 32 by their entry count in a panel) over several panels:
+    same results as the CSR FP32 kernel to compensated precision, FP64 SciPy
+    to FP32-value precision, and the same bits on every call."""
     from detnqs_b200 import device as D
     from detnqs_b200 import native as N
     sysm = S.make_system(30, 12, 12, 60, 1001)
-    V = S.heat_bath_sample(sysm, 40000, 7)          # 3 panels of 16384 columns
+    V = S.heat_bath_sample(sysm, 110000, 7)         # 3 panels of 49152 columns
     ctx = core.IntCtx.from_arrays(30, sysm.h1e, sysm.eri, sysm.e_core)
     ctx.hb_prepare(1e-15)
     kw = dict(n_orb=30, policy=1, use_heatbath=True, eps1=1e-6, want_vp=False)
