@@ -556,9 +556,13 @@ constexpr int kBS = 512;   // beta singles of one row kept for the presence rows
 constexpr int kScanU = 4;
 constexpr int kRing = 32 + 32 * kScanU;
 
+constexpr int kWinW = 128;   // part C: words of group-start bits, a window of 4096 members
 struct WarpShared {
-    u32 start[32], pre[32];    // part C: group starts, exclusive prefix of lengths
-    u32 tg[32];                // part C: member tag of each group (alpha hole, particle)
+    u32 off[32];               // part C: position of member m of a nonempty group is m + off
+    u32 tg[32];                // part C: member tag of each nonempty group (alpha hole, particle)
+    u32 first[32];             // part C: first member of each nonempty group
+    uint2 sw[kWinW];           // part C: per word, bit m set where a nonempty group starts at
+                               // member m, and the nonempty groups started before the word
     u8 occa[64], vira[64], occb[64], virb[64];
     u32 bs_id[kBS];            // beta group of each indexed beta single of the row
     u16 bs_hp[kBS];            // its excitation, hole | particle << 8
@@ -660,8 +664,11 @@ template <> __device__ __forceinline__ const u32* b_others<u32>(const VVParams& 
 
 // Part C over the short groups of one round of 32 alpha singles, packed:
 // the members of all of them are numbered in group order and each step
-// tests 32 consecutive members; a lane finds its member's group by a
-// five-step search of the exclusive prefix of the group lengths.
+// tests 32 consecutive members.  The nonempty groups take slots in lane
+// order; a bitmap marks the member each slot starts at, with the number of
+// slots started before each of its words, so a lane finds its member's slot
+// as that count plus the start bits up to its own, minus one.  The bitmap
+// covers windows of 32 * kWinW members.
 template <class W, class Q>
 __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_other, W b,
                                               unsigned long long& tests, u32 gs, u32 sl, int hh,
@@ -675,12 +682,41 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_ot
     }
     const u32 total = __shfl_sync(0xffffffffu, incl, 31);
     if (total == 0) return;
-    S.start[lane] = gs;
-    S.pre[lane] = incl - sl;
-    S.tg[lane] = kHitC | ((u32)hh << 8) | ((u32)pp << 16);
-    __syncwarp();
+    const unsigned ne = __ballot_sync(0xffffffffu, sl != 0);
+    if (sl != 0) {
+        const int slot = __popc(ne & lanemask_lt());
+        const u32 pre = incl - sl;   // first member of this lane's group
+        S.off[slot] = gs - pre;
+        S.tg[slot] = kHitC | ((u32)hh << 8) | ((u32)pp << 16);
+        S.first[slot] = pre;
+    }
+    const int ns = __popc(ne);
     tests += total;
     for (u32 t0 = 0; t0 < total; t0 += 32 * kScanU) {
+        if ((t0 & (32u * kWinW - 1u)) == 0) {   // start bits of the window from t0
+            __syncwarp();
+            const int nw = (int)min((total - t0 + 31u) >> 5, (u32)kWinW);
+            for (int w = lane; w < nw; w += 32) S.sw[w].x = 0u;
+            __syncwarp();
+            const u32 f = lane < ns ? S.first[lane] : 0xffffffffu;
+            if (f >= t0 && f - t0 < 32u * kWinW) atomicOr(&S.sw[(f - t0) >> 5].x, 1u << (f & 31u));
+            u32 run = __popc(__ballot_sync(0xffffffffu, f < t0));
+            __syncwarp();
+            for (int w0 = 0; w0 < nw; w0 += 32) {   // exclusive prefix of the start counts
+                const int w = w0 + lane;
+                const u32 c = w < nw ? (u32)__popc(S.sw[w].x) : 0u;
+                u32 ic = c;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const u32 v = __shfl_up_sync(0xffffffffu, ic, d);
+                    if (lane >= d) ic += v;
+                }
+                if (w < nw) S.sw[w].y = run + ic - c;
+                run += __shfl_sync(0xffffffffu, ic, 31);
+            }
+            __syncwarp();
+        }
+        const int w0 = (int)((t0 >> 5) & (kWinW - 1));
         u32 at[kScanU];
         int gl[kScanU];
         W y[kScanU];
@@ -691,11 +727,10 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_ot
             gl[u] = 0;
             y[u] = b;   // no hit
             if (m < total) {
-                int l = 0;   // last group with pre[l] <= m (it holds m: its length is not 0)
-#pragma unroll
-                for (int bit = 16; bit; bit >>= 1)
-                    if (S.pre[l + bit] <= m) l += bit;
-                at[u] = S.start[l] + (m - S.pre[l]);
+                const u32 le = (2u << lane) - 1u;   // lanes up to this one
+                const uint2 e = S.sw[w0 + u];
+                const int l = (int)(e.y + __popc(e.x & le)) - 1;
+                at[u] = m + S.off[l];
                 gl[u] = l;
                 y[u] = __ldg(&a_other[at[u]]);
             }
@@ -745,19 +780,19 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     const W aw = (W)a, bw = (W)b;
     const u64 all = low_mask(P.n_orb);
     q.push(lane == 0, (u32)r, kHitD);
-    // ---- part A: same beta string (alpha singles and doubles)
+    // groups of parts A and B, looked up by lanes 0 and 1 side by side
     u32 st = 0, ln = 0;
     if (lane == 0 && !P.bmap.find(b, st, ln)) ln = 0;
-    st = __shfl_sync(0xffffffffu, st, 0);
-    ln = __shfl_sync(0xffffffffu, ln, 0);
-    tests += ln;
-    scan_same(q, b_others<W>(P), aw, st, ln, kHitA);
+    if (lane == 1 && !P.amap.find(a, st, ln)) ln = 0;
+    // ---- part A: same beta string (alpha singles and doubles)
+    u32 gst = __shfl_sync(0xffffffffu, st, 0), gln = __shfl_sync(0xffffffffu, ln, 0);
+    tests += gln;
+    scan_same(q, b_others<W>(P), aw, gst, gln, kHitA);
     // ---- part B: same alpha string (beta singles and doubles)
-    if (lane == 0 && !P.amap.find(a, st, ln)) ln = 0;
-    st = __shfl_sync(0xffffffffu, st, 0);
-    ln = __shfl_sync(0xffffffffu, ln, 0);
-    tests += ln;
-    scan_same(q, ao, bw, st, ln, kHitB);
+    gst = __shfl_sync(0xffffffffu, st, 1);
+    gln = __shfl_sync(0xffffffffu, ln, 1);
+    tests += gln;
+    scan_same(q, ao, bw, gst, gln, kHitB);
     // ---- part C: alpha single x beta single, via the groups of the a'
     const int na = __popcll(a), nva = __popcll(~a & all);
     const int nsa = na * nva;
@@ -779,6 +814,7 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
         const bool pbig = usep && gl > P.pres_min && gl > (u32)nbv;
         const bool big = !pbig && gl > P.big_group;
         const bool small = gl != 0 && !pbig && !big;
+        const u32 prw = pbig ? __ldg(&P.a_prow[__ldg(&P.a_gid[gs])]) : 0u;   // its presence row
         if (!P.c_groupwalk) {
             part_c_packed(q, S, ao, bw, tests, gs, small ? gl : 0u, hh, pp);
         } else {
@@ -844,29 +880,27 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
             const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
             const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
                             ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
-            const uint2* row =
-                P.pres + (i64)__ldg(&P.a_prow[__ldg(&P.a_gid[g0])]) * P.pres_words;
+            const uint2* row = P.pres + (i64)__shfl_sync(0xffffffffu, prw, L) * P.pres_words;
             tests += nbs;
             for (int q0 = 0; q0 < nbs; q0 += 32 * kScanU) {
                 uint2 w[kScanU];
-                u32 bit[kScanU];
+                u32 sh[kScanU];
 #pragma unroll
                 for (int u = 0; u < kScanU; ++u) {
                     const int qi = q0 + 32 * u + lane;
                     w[u] = make_uint2(0u, 0u);
-                    bit[u] = 0;
+                    sh[u] = 0;
                     if (qi < nbs) {
                         const u32 bid = S.bs_id[qi];
-                        bit[u] = bid & 31;
+                        sh[u] = ~bid & 31u;   // moves the group's bit to bit 31
                         w[u] = __ldg(&row[bid >> 5]);
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < kScanU; ++u) {
                     if (q0 + 32 * u >= nbs) break;
-                    const bool hit = (w[u].x >> bit[u]) & 1u;
-                    const u32 at = g0 + w[u].y + __popc(w[u].x & ((1u << bit[u]) - 1u));
-                    q.push(hit, at, tag);
+                    const u32 lo = w[u].x << sh[u];   // the group's bit and those below
+                    q.push((int)lo < 0, g0 + w[u].y + __popc(lo) - 1u, tag);
                 }
                 q.sync();
             }
@@ -916,31 +950,24 @@ __device__ __forceinline__ auto tag_value(const F& f) -> decltype(f()) {
 // the value slots [w, end) of an arena chunk (whole 8-byte words, so no
 // partial-sector writes); past the end it only counts.
 struct HitOut {
-    u64* mem;   // the arena's value array as u64
-    i64 w, end;
+    u64* mem;   // the row's first slot in the arena's value array (as u64)
+    u32 room;   // slots the row may fill
     uint4* sgl = nullptr;   // this warp's singles slice (null: singles stay members)
     u32* sgn = nullptr;     // its entries used
     u32 sslice = 0;         // its size
     u32 sbase = 0;          // index of its first entry in the list
     u32 row = 0;            // global row, recorded with its singles
-    u32 c = 0;
-    bool over = false;
+    u32 c = 0;              // members found; written while they fit the room
+    // The row overflowed its room (c only grows, so once a step does not
+    // fit, no later step writes).
+    __device__ __forceinline__ bool over() const { return c > room; }
     template <class T>
     __device__ __forceinline__ void push(bool hit, u32 pos, const T& t) {
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (m == 0) return;   // most steps find nothing
-        const int k = __popc(m);
-        if (!over) {
-            if (w + k > end) {
-                over = true;
-            } else {
-                if (hit) {
-                    const i64 at = w + __popc(m & lanemask_lt());
-                    mem[at] = (u64)pos | ((u64)tag_value(t) << 32);
-                }
-                w += k;
-            }
-        }
+        const u32 k = __popc(m);
+        if (hit && c + k <= room)
+            mem[c + __popc(m & lanemask_lt())] = (u64)pos | ((u64)tag_value(t) << 32);
         c += k;
     }
     // Parts A and B: a single (tag with kSingleBit) goes to the singles list
@@ -948,28 +975,20 @@ struct HitOut {
     __device__ __forceinline__ void push_ab(bool hit, u32 pos, u32 tg) {
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (m == 0) return;
-        const int k = __popc(m);
-        if (!over) {
-            if (w + k > end) {
-                over = true;
-            } else {
-                u64 rec = (u64)pos | ((u64)(tg & ~kSingleBit) << 32);
-                const bool sg = hit && (tg & kSingleBit) && sgl;
-                const unsigned sm = __ballot_sync(0xffffffffu, sg);
-                if (sm) {
-                    const u32 idx = *sgn + __popc(sm & lanemask_lt());
-                    if (sg && idx < sslice) {
-                        sgl[idx] = make_uint4(row, pos, tg & ~kSingleBit, 0u);
-                        rec = (u64)(sbase + idx) | ((u64)kHitS << 32);
-                    }
-                    *sgn += __popc(sm);
+        const u32 k = __popc(m);
+        if (c + k <= room) {
+            u64 rec = (u64)pos | ((u64)(tg & ~kSingleBit) << 32);
+            const bool sg = hit && (tg & kSingleBit) && sgl;
+            const unsigned sm = __ballot_sync(0xffffffffu, sg);
+            if (sm) {
+                const u32 idx = *sgn + __popc(sm & lanemask_lt());
+                if (sg && idx < sslice) {
+                    sgl[idx] = make_uint4(row, pos, tg & ~kSingleBit, 0u);
+                    rec = (u64)(sbase + idx) | ((u64)kHitS << 32);
                 }
-                if (hit) {
-                    const i64 at = w + __popc(m & lanemask_lt());
-                    mem[at] = rec;
-                }
-                w += k;
+                *sgn += __popc(sm);
             }
+            if (hit) mem[c + __popc(m & lanemask_lt())] = rec;
         }
         c += k;
     }
@@ -1108,20 +1127,20 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         const u32 sgn0 = sgn;   // a row that is walked again drops its singles
         for (int attempt = 0; attempt < 2; ++attempt) {
             sgn = sgn0;
-            HitOut out{reinterpret_cast<u64*>(A.aval), cpos, cend, slice, &sgn, A.sgl_slice,
-                       (u32)wid * A.sgl_slice, (u32)g};
+            HitOut out{reinterpret_cast<u64*>(A.aval) + cpos, (u32)(cend - cpos), slice, &sgn,
+                       A.sgl_slice, (u32)wid * A.sgl_slice, (u32)g};
             unsigned long long tt = 0;
             walk_any<W>(P, r, a, b, S, out, tt);
             if (attempt == 0) {
                 tests += tt;
                 hits += out.c;
             }
-            if (!out.over) {
+            if (!out.over()) {
                 if (lane == 0) {
                     A.row_pos[g] = cpos;
                     A.row_len[g] = out.c;
                 }
-                cpos = out.w;
+                cpos += out.c;
                 break;
             }
             // Only rows of at most `restart` entries restart in a fresh
@@ -1265,7 +1284,7 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
         double psr, cut;
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
-        HitOut out{reinterpret_cast<u64*>(A.aval), (i64)base, (i64)base + len};
+        HitOut out{reinterpret_cast<u64*>(A.aval) + base, (u32)len};
         unsigned long long tt = 0;
         walk_any<W>(P, r, a, b, S, out, tt);
         if (lane == 0) {
