@@ -292,6 +292,8 @@ def run_ours(args, rank: int, world: int):
     sysm, V, psi = workload(rank, n_dets)
     ctx = core.IntCtx.from_arrays(N_ORB, sysm.h1e, sysm.eri, sysm.e_core, device=local)
     ctx.hb_prepare(1e-15)
+    # the step runs FP32 H.psi on every build: its FP32 copy is written by the build
+    native.check(native.lib.dnq_set_option(native.OPT_BUILD_F32, 1))
     V_dev = torch.from_numpy(V.view(np.int64)).to(dev)
     psi_dev = torch.from_numpy(psi).to(dev)
     eloc = torch.empty(n_dets, dtype=torch.float64, device=dev)

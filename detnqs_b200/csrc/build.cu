@@ -466,6 +466,7 @@ bool g_force_walk = false;
 extern i64 g_arena_chunk;
 extern i64 g_arena_cap;
 extern int g_partc_groupwalk;
+extern int g_build_f32;
 void spmv_set_option(int lanes, int unroll);
 void spmv_set_panels(int mode);
 
@@ -845,7 +846,7 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
 
 int dnq_set_option(int option, int64_t value) {
     DNQ_API_BEGIN
-    require(option >= 1 && option <= 7, DNQ_ERR_INVALID, "unknown option");
+    require(option >= 1 && option <= 8, DNQ_ERR_INVALID, "unknown option");
     if (option == 6)
         require(value <= 2, DNQ_ERR_INVALID, "panel mode must be 0, 1 or 2");
     require(value >= 0, DNQ_ERR_INVALID, "option value must be >= 0");
@@ -862,6 +863,7 @@ int dnq_set_option(int option, int64_t value) {
     if (option == 5) spmv_set_option(-1, (int)value);
     if (option == 6) spmv_set_panels((int)value);
     if (option == 7) g_partc_groupwalk = value != 0;
+    if (option == 8) g_build_f32 = value != 0;
     DNQ_API_END
 }
 

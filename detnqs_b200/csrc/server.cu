@@ -476,7 +476,9 @@ void worker(dnq_server_s* S, int slot) {
         i64 bytes = 0;
         if (rc == DNQ_OK) {
             try {
-                if (H->vv.nnz > 0) make_f32(H->vv, s, &H->diag_op);
+                if (H->vv.nnz > 0 && (H->vv.val32.n != (size_t)H->vv.nnz ||
+                                      H->diag_op.n != (size_t)H->n_v))
+                    make_f32(H->vv, s, &H->diag_op);
                 DNQ_CUDA(cudaStreamSynchronize(s));
                 bytes = (i64)H->bytes();
             } catch (const Error& e) {

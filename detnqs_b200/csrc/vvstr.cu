@@ -44,6 +44,7 @@ namespace dnq {
 // round (default), 1 = one group at a time.  Both give the same entries in
 // the same order.
 int g_partc_groupwalk = 0;
+int g_build_f32 = 0;   // V->V-only builds write the FP32 copy and the diagonal as they compact
 
 namespace {
 
@@ -1522,11 +1523,13 @@ void launch_big(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s
 
 // Single-pass build of nrows rows of L into M (allocated here).  cap_hint:
 // expected nnz (0 = unknown).  Falls back to the exact two-pass walk when
-// the arena is too small.  Returns the number of member tests.
+// the arena is too small.  With dg, the compaction also writes M.val32 (the
+// FP32 values, diagonal entries zero) and the FP64 diagonal into *dg; the
+// two-pass fallback leaves both empty.  Returns the number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
            double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr,
-           int scan = 0) {
+           int scan = 0, DBuf<double>* dg = nullptr) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
@@ -1603,12 +1606,18 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
         DNQ_CUDA(cudaStreamSynchronize(s));
         M.col.alloc(M.nnz, s);
         M.val.alloc(M.nnz, s);
+        if (dg) {
+            M.val32.alloc(M.nnz, s);
+            dg->alloc(nrows, s);
+        }
+        float* v32 = dg ? M.val32.p : nullptr;
+        double* dgp = dg ? dg->p : nullptr;
         DNQ_CUDA(cudaEventRecord(ev[2], s));
         k_vv_compact<<<grid, kWS * 32, 0, s>>>(rpos.p, M.rowptr.p, nrows, acol.p, aval.p, M.col.p,
-                                               M.val.p, M.nnz, bad.p);
+                                               M.val.p, M.nnz, bad.p, v32, dgp);
         DNQ_CHECK_LAUNCH();
         k_vv_compact_long<<<grid, 256, 0, s>>>(big.p, blen.p, nbig.p, rpos.p, M.rowptr.p, nrows,
-                                               acol.p, aval.p, M.col.p, M.val.p, M.nnz);
+                                               acol.p, aval.p, M.col.p, M.val.p, M.nnz, v32, dgp);
         DNQ_CHECK_LAUNCH();
     } else {
         acol.release();
@@ -1710,7 +1719,7 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     i64 hits = 0;
     H->candidates =
         run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits,
-               narrow ? 1 : 0);
+               narrow ? 1 : 0, g_build_f32 ? &H->diag_op : nullptr);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);

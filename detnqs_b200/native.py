@@ -39,6 +39,7 @@ OPT_SPMV_LANES = 4
 OPT_SPMV_UNROLL = 5
 OPT_SPMV_PANELS = 6
 OPT_PARTC_GROUPWALK = 7
+OPT_BUILD_F32 = 8
 REQ_BUILD = 0
 REQ_ELOC = 1
 

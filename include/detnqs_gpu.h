@@ -131,10 +131,16 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          the string-group matcher's opposite-spin doubles
  *                          one group at a time, 0 packed across the groups of
  *                          a round (default); both give identical blocks,
- *                          entry order too. */
+ *                          entry order too;
+ *   DNQ_OPT_BUILD_F32   n: 1 makes V->V-only builds write the FP32 copy of
+ *                          the V block and its FP64 diagonal while they
+ *                          compact the rows, for handles whose first use is
+ *                          an FP32 H.psi (4 bytes per entry more memory);
+ *                          0 makes them on first FP32 use (default).  The
+ *                          copies are the same either way. */
 enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
        DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6,
-       DNQ_OPT_PARTC_GROUPWALK = 7 };
+       DNQ_OPT_PARTC_GROUPWALK = 7, DNQ_OPT_BUILD_F32 = 8 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */

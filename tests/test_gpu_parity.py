@@ -401,6 +401,42 @@ def test_partc_walks_identical(core, policy):
     B.close()
 
 
+@pytest.mark.parametrize("chunk,cap", [(0, 0), (64, 0), (0, 5000)])
+def test_build_f32_copy_matches(core, chunk, cap):
+    """DNQ_OPT_BUILD_F32 writes the FP32 copy and the diagonal while the rows
+    are compacted (short rows, and long rows with small chunks); the two-pass
+    fallback (tiny arena) leaves them to the first FP32 use.  FP32 H.psi is
+    bit-identical to the copy made on first use, before and after a sort of
+    the rows."""
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(18, 6, 6, 36, 23)
+    V = S.heat_bath_sample(sysm, 12000, 3)
+    psi = S.normalized_psi(len(V), 4)
+    ctx = core.IntCtx.from_arrays(18, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    kw = dict(n_orb=18, policy=1, use_heatbath=True, eps1=1e-6, want_vp=False)
+    N.check(N.lib.dnq_set_option(N.OPT_ARENA_CHUNK, chunk))
+    N.check(N.lib.dnq_set_option(N.OPT_ARENA_CAP, cap))
+    try:
+        A = D.build(ctx, V, **kw)
+        N.check(N.lib.dnq_set_option(N.OPT_BUILD_F32, 1))
+        B = D.build(ctx, V, **kw)
+    finally:
+        N.check(N.lib.dnq_set_option(N.OPT_BUILD_F32, 0))
+        N.check(N.lib.dnq_set_option(N.OPT_ARENA_CHUNK, 0))
+        N.check(N.lib.dnq_set_option(N.OPT_ARENA_CAP, 0))
+    ya = A.spmv(psi, precision=N.F32)
+    yb = B.spmv(psi, precision=N.F32)
+    np.testing.assert_array_equal(ya.view(np.uint64), yb.view(np.uint64))
+    np.testing.assert_array_equal(A.spmv(psi).view(np.uint64), B.spmv(psi).view(np.uint64))
+    assert_coo_equal(A.to_coo(0), B.to_coo(0))   # sorts the rows
+    np.testing.assert_array_equal(A.spmv(psi, precision=N.F32).view(np.uint64),
+                                  B.spmv(psi, precision=N.F32).view(np.uint64))
+    A.close()
+    B.close()
+
+
 @pytest.mark.parametrize("chunk,cap", [(64, 0), (512, 0), (0, 5000)])
 def test_arena_paths_match(core, chunk, cap):
     """Small warp chunks force row restarts and the long-row pass; a tiny
