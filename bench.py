@@ -35,6 +35,10 @@ dynamic amplitude screening at eps1 = 1e-5 into C ~ 1e7 external
 determinants, and the downfolded H_eff in FP64 and FP32 values; |dE| of the
 lowest eigenvalue (device Lanczos) between the two.
 
+`--workload det_batch`: the neural models' determinant batch features
+(prepare_det_batch) for the single workload's 1e6 determinants, every
+field, relative to HF.
+
 `--impl reference` times the reference DetNQS C++ core (compiled from its
 sources into oracle/_ref) on a bounded sample of rows of the same workload.
 """
@@ -1132,10 +1136,151 @@ def run_downfold(args, rank: int, world: int):
     return result
 
 
+# ---------------------------------------------------------------------------
+# Determinant batch features: the single workload's 1e6 determinants
+# ---------------------------------------------------------------------------
+
+DB_KMAX = 8          # holes/particles kept: twice the deepest excitation of the space
+DB_WORKLOAD = ("30 orbitals, 12a/12b, the 1e6 heat-bath-sampled dets of the single "
+               "workload; every feature (occ, k, phase, holes/parts kmax=8, hp_mask, "
+               "positions) relative to HF")
+
+
+def det_batch_inputs(rank: int, n_dets: int):
+    _, V, _ = workload(rank, n_dets)
+    hf = np.array([(1 << N_ALPHA) - 1, (1 << N_BETA) - 1], np.uint64)
+    return V, hf
+
+
+def det_batch_bytes(n: int) -> int:
+    """Algorithmic bytes: dets read; occ, k, phase, holes, parts, positions
+    and mask written."""
+    return n * (16 + 4 * (N_ALPHA + N_BETA) + 2 + DB_KMAX * (4 * 4 + 1))
+
+
+def run_det_batch(args, rank: int, world: int):
+    import torch
+    from detnqs_b200 import core, native
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    V, hf = det_batch_inputs(rank, args.n_dets)
+    n = len(V)
+    Vd = torch.from_numpy(V.view(np.int64)).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    kw = dict(kmax=DB_KMAX, need_k=True, need_phase=True, need_hp=True, need_hp_pos=True,
+              device=local)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        core.prepare_det_batch(Vd, hf, N_ORB, N_ALPHA, N_BETA, **kw)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = native.lib.dnq_launch_count()
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = core.prepare_det_batch(Vd, hf, N_ORB, N_ALPHA, N_BETA, **kw)
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    clocks = clk.stop()
+    launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
+    ms = max_over_ranks(float(np.mean(ts)), world, dev)
+    # end to end: host determinants in, host features out
+    pin_V = torch.from_numpy(V.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    e2e = []
+    for k in range(1 + max(1, args.steps)):
+        flush.zero_()
+        barrier()
+        t0 = time.perf_counter()
+        host = core.prepare_det_batch(pin_V, hf, N_ORB, N_ALPHA, N_BETA, **kw)
+        if k:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), world, dev)
+    d2h = sum(v.nbytes for v in host.values())
+    peak, peak_kind = measured_peaks()
+    alg = det_batch_bytes(n)
+    result = {
+        "metric": "determinant batch features per second (occ, k, phase, holes/parts, "
+                  "positions, mask)",
+        "value": world * n / (ms * 1e-3), "unit": "dets/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (heat-bath sampled determinants)",
+        "config": {"workload": DB_WORKLOAD, "n_dets": n, "kmax": DB_KMAX,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps"},
+        "roofline": {"bound": "hbm", "kernel": "k_det_batch", "achieved": alg / (ms * 1e-3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                     "traffic": ncu_traffic("k_det_batch"), "peak_kind": peak_kind,
+                     "note": "timed over the whole call (staging, kernel, error read-back)"},
+        "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "dets/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    for k, v in out.items():   # the last timed batch equals the host one
+        assert np.array_equal(v.cpu().numpy(), host[k]), k
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, m, t, kind = cpu_det_batch(V, hf)
+        result["cpu_baseline"] = {"value": rate, "unit": "dets/s", "cores": 1, "kind": kind,
+                                  "sample": f"{m} dets of the batch in {t:.2f} s "
+                                            "(prepare_det_batch is a serial loop)"}
+    return result
+
+
+def cpu_det_batch(V, hf, seconds: float = 10.0):
+    """The reference's prepare_det_batch (oracle/_ref) on the host, every
+    feature, over repeated passes of the batch for about `seconds`."""
+    from oracle import Checker
+    kind = "reference" if Checker.reference_available() else "port"
+    chk = Checker.reference() if kind == "reference" else Checker.port()
+    m, t0 = 0, time.perf_counter()
+    while True:
+        chk.prepare_det_batch(V, hf, N_ORB, N_ALPHA, N_BETA, DB_KMAX, True, True, True, True)
+        m += len(V)
+        t = time.perf_counter() - t0
+        if t >= seconds:
+            return m / t, m, t, kind
+
+
 def run_reference(args, rank: int, world: int):
     """Reference CPU implementation on the same workload (rank 0 only)."""
     if rank != 0:
         return None
+    if args.workload == "det_batch":
+        V, hf = det_batch_inputs(0, args.n_dets)
+        vals, info = [], None
+        for _ in range(max(1, args.steps)):
+            rate, m, t, kind = cpu_det_batch(V, hf, max(1.0, args.cpu_seconds / max(1, args.steps)))
+            vals.append(rate)
+            info = (m, t, kind)
+        m, t, kind = info
+        v = float(np.mean(vals))
+        return {
+            "impl": "reference",
+            "metric": "determinant batch features per second (occ, k, phase, holes/parts, "
+                      "positions, mask)",
+            "value": v, "unit": "dets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": DB_WORKLOAD, "n_dets": len(V), "kmax": DB_KMAX},
+            "cpu_baseline": {"value": v, "unit": "dets/s", "cores": 1, "kind": kind,
+                             "sample": f"{m} dets per step in {t:.2f} s (serial loop)"},
+            "e2e": {"value": v, "unit": "dets/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
     if args.workload in ("batched", "serving"):
         if args.workload == "batched":
             W, _ = batch_workload(0)
@@ -1211,7 +1356,8 @@ def main():
                     help="size of S for --workload downfold (a smaller S for profiling)")
     ap.add_argument("--serve-slots", type=int, default=2,
                     help="build worker streams of the served path")
-    ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold"],
+    ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold",
+                                           "det_batch"],
                     default="single",
                     help="single: one 30-orbital system, 1e6 dets (default); batched: 64 "
                          "systems of uneven size per step; serving: Poisson request stream")
@@ -1229,7 +1375,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     run = {"single": run_ours, "batched": run_batched, "serving": run_serving,
-           "downfold": run_downfold}[args.workload]
+           "downfold": run_downfold, "det_batch": run_det_batch}[args.workload]
     res = run(args, rank, world)
     if world > 1:
         import torch

@@ -142,6 +142,60 @@ def excitations(bra, ket, device: int = 0):
     return deg, ph
 
 
+def prepare_det_batch(dets, ref, n_orb: int, n_alpha: int, n_beta: int, kmax: int = 0,
+                      need_k: bool = False, need_phase: bool = False, need_hp: bool = False,
+                      need_hp_pos: bool = False, device: int = 0) -> dict:
+    """Features of a determinant batch for the neural models, as
+    detnqs.core.prepare_det_batch (bridge.cpp:347-430): a dict with "occ"
+    int32[B, n_e] and, as asked, "k" / "phase" int8[B], "holes" / "parts"
+    int32[B, kmax], "hp_mask" bool[B, kmax], "holes_pos" / "parts_pos"
+    int32[B, kmax].  need_hp implies need_k.  Host determinants give numpy
+    arrays (in page-locked memory); CUDA-tensor determinants give CUDA
+    tensors on their device, computed on torch's current stream with no host
+    copy."""
+    d = _dets(dets)
+    r = np.ascontiguousarray(ref, dtype=np.uint64).reshape(-1)
+    if r.shape != (2,):
+        raise ValueError(f"ref must be (2,), got {r.shape}")
+    need_k = bool(need_k or need_hp)
+    B, ne = int(d.shape[0]), int(n_alpha) + int(n_beta)
+    kdim = max(int(kmax), 0)
+    on_dev = hasattr(d, "is_cuda") and d.is_cuda
+    import torch
+    if on_dev:
+        dev = d.device
+        device = dev.index if dev.index is not None else torch.cuda.current_device()
+
+        def new(shape, dt):
+            return torch.empty(shape, dtype=getattr(torch, dt), device=dev)
+    else:
+        def new(shape, dt):   # page-locked, so the copies back run at full speed
+            return torch.empty(shape, dtype=getattr(torch, dt), pin_memory=True).numpy()
+    out = {"occ": new((B, max(ne, 0)), "int32")}
+    if need_k:
+        out["k"] = new((B,), "int8")
+    if need_phase:
+        out["phase"] = new((B,), "int8")
+    if need_hp:
+        out["holes"] = new((B, kdim), "int32")
+        out["parts"] = new((B, kdim), "int32")
+        out["hp_mask"] = new((B, kdim), "uint8")
+        if need_hp_pos:
+            out["holes_pos"] = new((B, kdim), "int32")
+            out["parts_pos"] = new((B, kdim), "int32")
+    flags = ((N.NEED_K if need_k else 0) | (N.NEED_PHASE if need_phase else 0) |
+             (N.NEED_HP if need_hp else 0) | (N.NEED_HP_POS if need_hp_pos else 0))
+    p = lambda key: N.ptr(out[key]) if key in out else None  # noqa: E731
+    N.check(N.lib.dnq_prepare_det_batch(N.ptr(d), B, r.ctypes.data, int(n_orb), int(n_alpha),
+                                        int(n_beta), int(kmax), flags, p("occ"), p("k"),
+                                        p("phase"), p("holes"), p("parts"), p("hp_mask"),
+                                        p("holes_pos"), p("parts_pos"), int(device),
+                                        N.stream_of(d)))
+    if "hp_mask" in out:
+        out["hp_mask"] = out["hp_mask"].bool() if on_dev else out["hp_mask"].view(np.bool_)
+    return out
+
+
 def _blocks(H: DeviceHamiltonian, with_p: bool) -> dict:
     out = {"H_VV": H.to_coo(0), "H_VP": H.to_coo(1)}
     if with_p:
@@ -379,6 +433,7 @@ __all__ = [
     "get_ham_diag",
     "get_ham_elems",
     "excitations",
+    "prepare_det_batch",
     "get_ham_vv",
     "get_ham_block",
     "get_ham_conn",

@@ -96,6 +96,25 @@ int dnq_ham_elems(dnq_ctx_t ctx, const uint64_t* bra, const uint64_t* ket,
 int dnq_excitations(const uint64_t* bra, const uint64_t* ket, int64_t n,
                     int32_t* degree, double* phase, int device, void* stream);
 
+/* ---- determinant batch features ------------------------------------------
+ * detnqs.core.prepare_det_batch (bridge.cpp:347-430; det_batch.cpp:184-318,
+ * det_batch.hpp:38-79): for B determinants and a reference `ref` (host
+ * uint64[2]), occ int32[B][n_alpha + n_beta] (alpha orbitals ascending,
+ * then beta + n_orb ascending); with DNQ_NEED_K the excitation rank
+ * k int8[B] (capped at 127); with DNQ_NEED_PHASE the sign int8[B]; with
+ * DNQ_NEED_HP (which implies DNQ_NEED_K) holes and parts int32[B][kmax]
+ * (-1 padded) and hp_mask uint8[B][kmax]; with DNQ_NEED_HP_POS (requires
+ * DNQ_NEED_HP) their positions in the reference's occupied / virtual lists.
+ * Buffers may be host or device memory; outputs not asked for may be null.
+ * Errors are the reference's std::invalid_argument cases (DNQ_ERR_INVALID
+ * with its message), for the first failing determinant in batch order. */
+enum { DNQ_NEED_K = 1, DNQ_NEED_PHASE = 2, DNQ_NEED_HP = 4, DNQ_NEED_HP_POS = 8 };
+int dnq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref,
+                          int n_orb, int n_alpha, int n_beta, int kmax, int flags,
+                          int32_t* occ, int8_t* k, int8_t* phase, int32_t* holes,
+                          int32_t* parts, uint8_t* hp_mask, int32_t* holes_pos,
+                          int32_t* parts_pos, int device, void* stream);
+
 /* ---- screened Hamiltonian build ------------------------------------------
  * One call covers the four reference builders (build_ham.cpp:402-535):
  *   get_ham_vv      : policy KNOWN_SETS, ext = NULL, want_vp = 0

@@ -88,6 +88,8 @@ def _bind(lib: C.CDLL) -> None:
     f("dq_res_offsets", None, _P, _i32p)
     f("dq_res_values", None, _P, _f64p)
     f("dq_res_free", None, _P)
+    f("dq_prepare_det_batch", C.c_int, _u64p, C.c_int64, _u64p, C.c_int, C.c_int, C.c_int,
+      C.c_int, C.c_int, _i32p, _P, _P, _P, _P, _P, _P, _P)
 
 
 def _dets(x) -> np.ndarray:
@@ -169,6 +171,37 @@ class Checker:
         self.lib.dq_analyze(np.ascontiguousarray(bra, np.uint64),
                             np.ascontiguousarray(ket, np.uint64), C.byref(d), C.byref(ph))
         return d.value, ph.value
+
+    def prepare_det_batch(self, dets, ref, n_orb: int, n_alpha: int, n_beta: int,
+                          kmax: int = 0, need_k: bool = False, need_phase: bool = False,
+                          need_hp: bool = False, need_hp_pos: bool = False) -> dict:
+        """Features of a determinant batch, as the bridge's prepare_det_batch
+        (bridge.cpp:347-430): a dict of occ and the fields asked for."""
+        d = _dets(dets)
+        r = np.ascontiguousarray(ref, np.uint64).reshape(2)
+        B, ne = len(d), n_alpha + n_beta
+        need_k = need_k or need_hp
+        out = {"occ": np.zeros((B, max(ne, 0)), np.int32)}
+        if need_k:
+            out["k"] = np.zeros(B, np.int8)
+        if need_phase:
+            out["phase"] = np.zeros(B, np.int8)
+        if need_hp:
+            for key in ("holes", "parts", "holes_pos", "parts_pos")[:4 if need_hp_pos else 2]:
+                out[key] = np.zeros((B, max(kmax, 0)), np.int32)
+            out["hp_mask"] = np.zeros((B, max(kmax, 0)), np.uint8)
+        ptr = lambda key: out[key].ctypes.data if key in out else None  # noqa: E731
+        flags = (1 if need_k else 0) | (2 if need_phase else 0) | (4 if need_hp else 0) | \
+                (8 if need_hp_pos else 0)
+        rc = self.lib.dq_prepare_det_batch(d, B, r, n_orb, n_alpha, n_beta, kmax, flags,
+                                           out["occ"], ptr("k"), ptr("phase"), ptr("holes"),
+                                           ptr("parts"), ptr("hp_mask"), ptr("holes_pos"),
+                                           ptr("parts_pos"))
+        if rc != 0:
+            raise ValueError(self.lib.dq_last_error().decode())
+        if "hp_mask" in out:
+            out["hp_mask"] = out["hp_mask"].astype(bool)
+        return out
 
     def gen_connected_dets(self, ref_dets, n_orb: int) -> np.ndarray:
         d = _dets(ref_dets)

@@ -100,6 +100,19 @@ void    dq_res_offsets(void* r, int32_t* out);
 void    dq_res_values(void* r, double* out);
 void    dq_res_free(void* r);
 
+/* ---- determinant batch features (det_batch.hpp:38-79) -------------------
+ * flags: 1 need_k, 2 need_phase, 4 need_hp, 8 need_hp_pos (the bridge's
+ * prepare_det_batch, bridge.cpp:347-430, turns need_hp into need_k too).
+ * occ int32[B][n_alpha + n_beta]; k, phase int8[B]; holes, parts,
+ * holes_pos, parts_pos int32[B][kmax]; hp_mask uint8[B][kmax] (C++ bool).
+ * Outputs not asked for may be null.  Returns 0, or -1 with
+ * dq_last_error() holding the reference's message. */
+int dq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref,
+                         int n_orb, int n_alpha, int n_beta, int kmax, int flags,
+                         int32_t* occ, int8_t* k, int8_t* phase, int32_t* holes,
+                         int32_t* parts, uint8_t* hp_mask, int32_t* holes_pos,
+                         int32_t* parts_pos);
+
 #ifdef __cplusplus
 }
 #endif

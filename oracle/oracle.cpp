@@ -1005,6 +1005,107 @@ void* dq_gen_perturbative(void* c, const uint64_t* V, int64_t n, int n_orb,
     GUARD_END(nullptr)
 }
 
+// Determinant batch features for the neural models, restated from
+// det_batch.cpp:184-318 (checks and their messages in the same order, then
+// per determinant: occupied list, excitation rank, phase, hole/particle
+// lists).  The phase applies the holes highest first, then the particles
+// lowest first, each flipping the sign by the parity of the occupied
+// orbitals below it (det_batch.cpp:61-98).
+int dq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref,
+                         int n_orb, int n_alpha, int n_beta, int kmax, int flags,
+                         int32_t* occ, int8_t* kout, int8_t* phase, int32_t* holes,
+                         int32_t* parts, uint8_t* hp_mask, int32_t* holes_pos,
+                         int32_t* parts_pos) {
+    GUARD_BEGIN
+    const bool need_hp = flags & 4, need_pos = flags & 8, need_phase = flags & 2;
+    const bool need_k = (flags & 1) || need_hp;
+    if (n_orb < 0 || n_orb > 64) throw std::invalid_argument("n_orb out of range [0,64]");
+    if (!dets || !occ) throw std::invalid_argument("null pointer in required outputs");
+    if (need_pos && !need_hp) throw std::invalid_argument("need_hp_pos requires need_hp");
+    if (need_hp && kmax < 0) throw std::invalid_argument("kmax must be non-negative");
+    const u64 m = n_orb == 64 ? ~0ull : ((1ull << n_orb) - 1);
+    const u64 ra = ref[0], rb = ref[1];
+    const int ne = n_alpha + n_beta;
+    // position of a spin orbital in the reference's occupied list (alpha
+    // ascending, then beta) or in its virtual list (the rest, ascending)
+    auto below = [](u64 x, int o) { return popc(x & ((1ull << o) - 1)); };
+    auto occ_pos = [&](int so) {
+        return so < n_orb ? below(ra & m, so) : n_alpha + below(rb & m, so - n_orb);
+    };
+    auto vir_pos = [&](int so) {
+        return so < n_orb ? so - below(ra & m, so) : so - n_alpha - below(rb & m, so - n_orb);
+    };
+    if (need_pos && (popc(ra & m) != n_alpha || popc(rb & m) != n_beta))
+        throw std::invalid_argument("reference electron count mismatch");
+    auto spin_phase = [](u64 r, u64 d, u64 mk) {
+        r &= mk;
+        d &= mk;
+        u64 h = r & ~d, p = d & ~r, o = r;
+        if (popc(h) != popc(p)) throw std::invalid_argument("holes != parts in spin channel");
+        int par = 0;
+        for (int q = 63; q >= 0; --q)
+            if ((h >> q) & 1) {
+                par += popc(o & ((1ull << q) - 1));
+                o ^= 1ull << q;
+            }
+        for (int q = 0; q < 64; ++q)
+            if ((p >> q) & 1) {
+                par += popc(o & ((1ull << q) - 1));
+                o ^= 1ull << q;
+            }
+        return (par & 1) ? -1 : 1;
+    };
+    for (int64_t i = 0; i < B; ++i) {
+        const u64 a = dets[2 * i], b = dets[2 * i + 1];
+        if ((a & ~m) || (b & ~m)) throw std::invalid_argument("det bits outside n_orb range");
+        if (popc(a) != n_alpha || popc(b) != n_beta)
+            throw std::invalid_argument("electron count mismatch");
+        int32_t* orow = occ + i * ne;
+        int c = 0;
+        for (int o = 0; o < n_orb; ++o)
+            if ((a >> o) & 1) orow[c++] = o;
+        for (int o = 0; o < n_orb; ++o)
+            if ((b >> o) & 1) orow[c++] = o + n_orb;
+        const u64 ha = ra & ~a & m, hb = rb & ~b & m;
+        const int kk = popc(ha) + popc(hb);
+        if (need_k) {
+            if (!kout) throw std::invalid_argument("k_out is null");
+            kout[i] = (int8_t)std::min(kk, 127);
+        }
+        if (need_phase) {
+            if (!phase) throw std::invalid_argument("phase_out is null");
+            phase[i] = (int8_t)(spin_phase(ra, a, m) * spin_phase(rb, b, m));
+        }
+        if (!need_hp) continue;
+        if (!holes || !parts || !hp_mask) throw std::invalid_argument("hp outputs are null");
+        if (need_pos && (!holes_pos || !parts_pos))
+            throw std::invalid_argument("pos outputs are null");
+        int32_t* hrow = holes + i * kmax;
+        int32_t* prow = parts + i * kmax;
+        std::vector<int> hl, pl;   // holes alpha then beta, each highest first;
+        for (int o = n_orb - 1; o >= 0; --o)   // particles lowest first
+            if ((ha >> o) & 1) hl.push_back(o);
+        for (int o = n_orb - 1; o >= 0; --o)
+            if ((hb >> o) & 1) hl.push_back(o + n_orb);
+        const u64 pa = a & ~ra & m, pb = b & ~rb & m;
+        for (int o = 0; o < n_orb; ++o)
+            if ((pa >> o) & 1) pl.push_back(o);
+        for (int o = 0; o < n_orb; ++o)
+            if ((pb >> o) & 1) pl.push_back(o + n_orb);
+        for (int j = 0; j < kmax; ++j) {
+            hrow[j] = j < (int)hl.size() ? hl[j] : -1;
+            prow[j] = j < (int)pl.size() ? pl[j] : -1;
+            hp_mask[i * kmax + j] = j < std::min(kk, kmax);
+            if (need_pos) {
+                holes_pos[i * kmax + j] = j < (int)hl.size() ? occ_pos(hl[j]) : -1;
+                parts_pos[i * kmax + j] = j < (int)pl.size() ? vir_pos(pl[j]) : -1;
+            }
+        }
+    }
+    return 0;
+    GUARD_END(-1)
+}
+
 }  // extern "C"
 
 DQ_RESULT_ACCESSORS

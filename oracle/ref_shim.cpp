@@ -9,6 +9,7 @@
 #include "dq_result.hpp"
 
 #include <detnqs/determinant/det.hpp>
+#include <detnqs/determinant/det_batch.hpp>
 #include <detnqs/determinant/det_ops.hpp>
 #include <detnqs/determinant/det_space.hpp>
 #include <detnqs/hamiltonian/build_ham.hpp>
@@ -346,6 +347,25 @@ void* dq_gen_perturbative(void* c, const uint64_t* V, int64_t n, int n_orb,
              r->dets);
     return r;
     GUARD_END(nullptr)
+}
+
+int dq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref,
+                         int n_orb, int n_alpha, int n_beta, int kmax, int flags,
+                         int32_t* occ, int8_t* k, int8_t* phase, int32_t* holes,
+                         int32_t* parts, uint8_t* hp_mask, int32_t* holes_pos,
+                         int32_t* parts_pos) {
+    GUARD_BEGIN
+    det_batch::PrepareOptions opt;   // as bridge.cpp:363-368
+    opt.kmax = kmax;
+    opt.need_k = (flags & 1) || (flags & 4);
+    opt.need_phase = (flags & 2) != 0;
+    opt.need_hp = (flags & 4) != 0;
+    opt.need_hp_pos = (flags & 8) != 0;
+    det_batch::prepare_det_batch(dets, (std::size_t)B, Det{ref[0], ref[1]}, n_orb, n_alpha,
+                                 n_beta, opt, occ, k, phase, holes, parts,
+                                 reinterpret_cast<bool*>(hp_mask), holes_pos, parts_pos);
+    return 0;
+    GUARD_END(-1)
 }
 
 }  // extern "C"
