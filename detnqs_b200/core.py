@@ -179,7 +179,7 @@ def prepare_det_batch(dets, ref, n_orb: int, n_alpha: int, n_beta: int, kmax: in
     if need_hp:
         out["holes"] = new((B, kdim), "int32")
         out["parts"] = new((B, kdim), "int32")
-        out["hp_mask"] = new((B, kdim), "uint8")
+        out["hp_mask"] = new((B, kdim), "bool")   # one byte, 0 or 1
         if need_hp_pos:
             out["holes_pos"] = new((B, kdim), "int32")
             out["parts_pos"] = new((B, kdim), "int32")
@@ -191,8 +191,6 @@ def prepare_det_batch(dets, ref, n_orb: int, n_alpha: int, n_beta: int, kmax: in
                                         p("phase"), p("holes"), p("parts"), p("hp_mask"),
                                         p("holes_pos"), p("parts_pos"), int(device),
                                         N.stream_of(d)))
-    if "hp_mask" in out:
-        out["hp_mask"] = out["hp_mask"].bool() if on_dev else out["hp_mask"].view(np.bool_)
     return out
 
 

@@ -3,8 +3,10 @@
 // detnqs.core.prepare_det_batch in csrc/bridge/bridge.cpp:347-430).
 //
 // One thread per determinant, grid-stride: every field is a short loop over
-// set bits, so a warp keeps 32 determinants in flight; a thread's rows are
-// contiguous and the L2 merges the warp's strided stores into whole sectors.
+// set bits, so a warp keeps 32 determinants in flight.  A thread's rows are
+// contiguous: it writes them four int32 (or eight mask bytes) to a store
+// where the row is aligned, and the L2 merges the warp's strided stores into
+// whole sectors.
 // The sign is the reference's sequence: holes removed highest first,
 // particles added lowest first, each flipping it by the parity of the
 // occupied orbitals below (det_batch.cpp:61-98), over the set bits only.
@@ -15,6 +17,9 @@
 #include "common.cuh"
 
 namespace dnq {
+
+void keep_pool(int device);
+
 namespace {
 
 enum : int { kNeedK = 1, kNeedPhase = 2, kNeedHp = 4, kNeedPos = 8 };
@@ -38,6 +43,35 @@ __device__ __forceinline__ int spin_sign(u64 r, u64 d) {
     }
     return (par & 1) ? -1 : 1;
 }
+
+// Consecutive int32 values of one output row: four to a 16-byte store when
+// the row starts on a 16-byte boundary, one by one otherwise.
+struct RowOut {
+    int32_t* p;
+    bool vec;
+    int n = 0, b0 = 0, b1 = 0, b2 = 0;
+    __device__ __forceinline__ explicit RowOut(int32_t* row)
+        : p(row), vec((reinterpret_cast<uintptr_t>(row) & 15) == 0) {}
+    __device__ __forceinline__ void put(int v) {
+        if (!vec) {
+            p[n++] = v;
+            return;
+        }
+        const int r = n & 3;
+        if (r == 3) *reinterpret_cast<int4*>(p + n - 3) = make_int4(b0, b1, b2, v);
+        else if (r == 0) b0 = v;
+        else if (r == 1) b1 = v;
+        else b2 = v;
+        ++n;
+    }
+    __device__ __forceinline__ void flush() {   // the last partial group
+        if (!vec) return;
+        const int r = n & 3, s = n - r;
+        if (r > 0) p[s] = b0;
+        if (r > 1) p[s + 1] = b1;
+        if (r > 2) p[s + 2] = b2;
+    }
+};
 
 struct BatchOut {
     int32_t* occ;
@@ -71,10 +105,10 @@ __global__ void __launch_bounds__(256) k_det_batch(const u64* dets, i64 B, u64 r
             atomicMin(err, ((unsigned long long)i << 2) | bad);
             continue;
         }
-        int32_t* orow = o.occ + i * ne;
-        int c = 0;
-        for (u64 x = a; x; x &= x - 1) orow[c++] = __ffsll((long long)x) - 1;
-        for (u64 x = b; x; x &= x - 1) orow[c++] = __ffsll((long long)x) - 1 + n_orb;
+        RowOut occ(o.occ + i * ne);
+        for (u64 x = a; x; x &= x - 1) occ.put(__ffsll((long long)x) - 1);
+        for (u64 x = b; x; x &= x - 1) occ.put(__ffsll((long long)x) - 1 + n_orb);
+        occ.flush();
         const u64 ha = ra & ~a, hb = rb & ~b, pa = a & ~ra, pb = b & ~rb;
         const int kk = __popcll(ha) + __popcll(hb);
         if (flags & (kNeedK | kNeedHp)) o.k[i] = (int8_t)min(kk, 127);
@@ -84,44 +118,65 @@ __global__ void __launch_bounds__(256) k_det_batch(const u64* dets, i64 B, u64 r
         const i64 row = i * kmax;
         // holes: alpha then beta (+ n_orb), each highest first; position in
         // the reference's occupied list (alpha ascending, then beta)
-        int j = 0;
-        for (u64 x = ha; x && j < kmax; ++j) {
-            const int q = 63 - __clzll((long long)x);
-            x ^= 1ull << q;
-            o.holes[row + j] = q;
-            if (pos) o.hpos[row + j] = __popcll(ra & low_mask(q));
-        }
-        for (u64 x = hb; x && j < kmax; ++j) {
-            const int q = 63 - __clzll((long long)x);
-            x ^= 1ull << q;
-            o.holes[row + j] = q + n_orb;
-            if (pos) o.hpos[row + j] = na + __popcll(rb & low_mask(q));
-        }
-        for (; j < kmax; ++j) {
-            o.holes[row + j] = -1;
-            if (pos) o.hpos[row + j] = -1;
+        {
+            RowOut ho(o.holes + row), hp(pos ? o.hpos + row : o.holes + row);
+            int j = 0;
+            for (u64 x = ha; x && j < kmax; ++j) {
+                const int q = 63 - __clzll((long long)x);
+                x ^= 1ull << q;
+                ho.put(q);
+                if (pos) hp.put(__popcll(ra & low_mask(q)));
+            }
+            for (u64 x = hb; x && j < kmax; ++j) {
+                const int q = 63 - __clzll((long long)x);
+                x ^= 1ull << q;
+                ho.put(q + n_orb);
+                if (pos) hp.put(na + __popcll(rb & low_mask(q)));
+            }
+            for (; j < kmax; ++j) {
+                ho.put(-1);
+                if (pos) hp.put(-1);
+            }
+            ho.flush();
+            if (pos) hp.flush();
         }
         // particles: alpha then beta (+ n_orb), each lowest first; position
         // in the reference's virtual list (the other spin orbitals, ascending)
-        j = 0;
-        for (u64 x = pa; x && j < kmax; ++j) {
-            const int q = __ffsll((long long)x) - 1;
-            x &= x - 1;
-            o.parts[row + j] = q;
-            if (pos) o.ppos[row + j] = q - __popcll(ra & low_mask(q));
+        {
+            RowOut po(o.parts + row), pp(pos ? o.ppos + row : o.parts + row);
+            int j = 0;
+            for (u64 x = pa; x && j < kmax; ++j) {
+                const int q = __ffsll((long long)x) - 1;
+                x &= x - 1;
+                po.put(q);
+                if (pos) pp.put(q - __popcll(ra & low_mask(q)));
+            }
+            for (u64 x = pb; x && j < kmax; ++j) {
+                const int q = __ffsll((long long)x) - 1;
+                x &= x - 1;
+                po.put(q + n_orb);
+                if (pos) pp.put(q + n_orb - na - __popcll(rb & low_mask(q)));
+            }
+            for (; j < kmax; ++j) {
+                po.put(-1);
+                if (pos) pp.put(-1);
+            }
+            po.flush();
+            if (pos) pp.flush();
         }
-        for (u64 x = pb; x && j < kmax; ++j) {
-            const int q = __ffsll((long long)x) - 1;
-            x &= x - 1;
-            o.parts[row + j] = q + n_orb;
-            if (pos) o.ppos[row + j] = q + n_orb - na - __popcll(rb & low_mask(q));
-        }
-        for (; j < kmax; ++j) {
-            o.parts[row + j] = -1;
-            if (pos) o.ppos[row + j] = -1;
-        }
+        // mask: the first min(k, kmax) bytes set, eight to a store when the
+        // row starts on an 8-byte boundary and holds whole words
         const int kcap = min(kk, kmax);
-        for (j = 0; j < kmax; ++j) o.mask[row + j] = j < kcap;
+        uint8_t* mrow = o.mask + row;
+        if ((reinterpret_cast<uintptr_t>(mrow) & 7) == 0 && (kmax & 7) == 0) {
+            for (int w = 0; w < kmax; w += 8) {
+                const int on = min(max(kcap - w, 0), 8);
+                const u64 lo = on == 8 ? ~0ull : ((1ull << (8 * on)) - 1ull);
+                *reinterpret_cast<u64*>(mrow + w) = 0x0101010101010101ull & lo;
+            }
+        } else {
+            for (int j = 0; j < kmax; ++j) mrow[j] = j < kcap;
+        }
     }
 }
 
@@ -186,6 +241,7 @@ int dnq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref, 
     require(!need_pos || kmax == 0 || (holes_pos && parts_pos), DNQ_ERR_INVALID,
             "pos outputs are null");
     DeviceGuard g(device);
+    keep_pool(device);   // the device pool keeps freed memory, as for every other entry point
     cudaStream_t s = (cudaStream_t)stream;
     const int ne = n_alpha + n_beta;
     const size_t nk = need_hp ? (size_t)B * (size_t)kmax : 0;
