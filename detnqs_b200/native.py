@@ -50,6 +50,7 @@ EXPORTS = (
     "dnq_ctx_create", "dnq_ctx_create_fcidump", "dnq_ctx_destroy", "dnq_ctx_e_nuc",
     "dnq_ctx_device_bytes", "dnq_hb_prepare", "dnq_hb_clear", "dnq_hb_row",
     "dnq_ham_diag", "dnq_ham_elems", "dnq_excitations", "dnq_prepare_det_batch",
+    "dnq_slogdet", "dnq_slogdet_grad",
     "dnq_build", "dnq_set_option", "dnq_ham_destroy", "dnq_ham_info", "dnq_ham_timings", "dnq_ham_copy_coo",
     "dnq_ham_copy_csr", "dnq_ham_copy_dets_p", "dnq_ham_copy_diag",
     "dnq_ham_spmv", "dnq_ham_proxy_spmv", "dnq_ham_local_energy",
@@ -110,6 +111,8 @@ _sig("dnq_hb_row", _P, _I, _I, _P, _P, _P, _I64, C.POINTER(_I64))
 _sig("dnq_ham_diag", _P, _P, _I64, _P, _P)
 _sig("dnq_ham_elems", _P, _P, _P, _I64, _P, _P)
 _sig("dnq_excitations", _P, _P, _I64, _P, _P, _I, _P)
+_sig("dnq_slogdet", _P, _I64, _I, _I, _P, _P, _I, _P)
+_sig("dnq_slogdet_grad", _P, _P, _I64, _I, _I, _P, _I, _P)
 _sig("dnq_prepare_det_batch", _P, _I64, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P,
      _I, _P)
 _sig("dnq_build", _P, _P, _I64, _P, _I64, _P, _I, _I, _I, _D, _I, _P, C.POINTER(_P))

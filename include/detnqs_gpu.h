@@ -109,6 +109,23 @@ int dnq_excitations(const uint64_t* bra, const uint64_t* ket, int64_t n,
  * Errors are the reference's std::invalid_argument cases (DNQ_ERR_INVALID
  * with its message), for the first failing determinant in batch order. */
 enum { DNQ_NEED_K = 1, DNQ_NEED_PHASE = 2, DNQ_NEED_HP = 4, DNQ_NEED_HP_POS = 8 };
+
+/* ---- batched log-determinant ---------------------------------------------
+ * The fused log-det kernels of the reference's XLA FFI module
+ * (csrc/ffi/logdet_cuda.cu:187-331, bound by detnqs/models/slogdet.py:
+ * slogdet(..., use_fast_kernel=True)).  a holds B row-major n x n matrices,
+ * 2 <= n <= 64, in FP64 (precision DNQ_F64) or FP32 (DNQ_F32); sign and
+ * logabs (B values each) and grad (B matrices) are in the same type.
+ * dnq_slogdet: sign and log|det| by LU with partial pivoting; a matrix whose
+ * factorisation meets a zero pivot column gets sign 0 and log|det| -inf.
+ * dnq_slogdet_grad: grad = cot_logabs[b] * A_b^{-T} (the gradient of
+ * log|det|), 0 for such singular matrices.  Buffers may be host or device
+ * memory.  Errors: "N must be in [2, 64]", "Batch size out of int32 range"
+ * (B < 1 too), as the reference. */
+int dnq_slogdet(const void* a, int64_t B, int n, int precision, void* sign,
+                void* logabs, int device, void* stream);
+int dnq_slogdet_grad(const void* a, const void* cot_logabs, int64_t B, int n,
+                     int precision, void* grad, int device, void* stream);
 int dnq_prepare_det_batch(const uint64_t* dets, int64_t B, const uint64_t* ref,
                           int n_orb, int n_alpha, int n_beta, int kmax, int flags,
                           int32_t* occ, int8_t* k, int8_t* phase, int32_t* holes,
