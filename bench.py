@@ -39,6 +39,9 @@ lowest eigenvalue (device Lanczos) between the two.
 (prepare_det_batch) for the single workload's 1e6 determinants, every
 field, relative to HF.
 
+`--workload slogdet`: sign, log|det| and its gradient for 32768 10x10 FP64
+matrices (the batched log-det of the neural models).
+
 `--impl reference` times the reference DetNQS C++ core (compiled from its
 sources into oracle/_ref) on a bounded sample of rows of the same workload.
 """
@@ -1255,10 +1258,153 @@ def cpu_det_batch(V, hf, seconds: float = 10.0):
             return m / t, m, t, kind
 
 
+# ---------------------------------------------------------------------------
+# Batched log-determinant: sign, log|det| and its gradient
+# ---------------------------------------------------------------------------
+
+SL_B, SL_N = 32768, 10     # the reference's largest "typical SPO" case (test_logdet.py:195-200)
+SL_WORKLOAD = ("32768 FP64 10x10 matrices N(0,1) + 10 I (the reference's largest typical-SPO "
+               "benchmark case); sign, log|det| and the gradient of log|det|")
+
+
+def slogdet_inputs(rank: int):
+    rng = np.random.default_rng(4242 + rank)
+    a = rng.normal(size=(SL_B, SL_N, SL_N)) + np.eye(SL_N) * SL_N
+    return a, rng.normal(size=SL_B)
+
+
+def run_slogdet(args, rank: int, world: int):
+    import torch
+    from detnqs_b200 import native
+    from detnqs_b200 import slogdet as L
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a, cot = slogdet_inputs(rank)
+    ad = torch.from_numpy(a).to(dev)
+    cd = torch.from_numpy(cot).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def step(x, c):
+        sign, logabs = L.slogdet(x, device=local)
+        return sign, logabs, L.slogdet_grad(x, c, device=local)
+
+    for _ in range(args.warmup):
+        step(ad, cd)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    l0 = native.lib.dnq_launch_count()
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = step(ad, cd)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    clocks = clk.stop()
+    launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
+    ms = max_over_ranks(float(np.mean(ts)), world, dev)
+    pin_a = torch.from_numpy(a).pin_memory().numpy()
+    pin_c = torch.from_numpy(cot).pin_memory().numpy()
+    e2e = []
+    for k in range(1 + max(1, args.steps)):
+        barrier()
+        t0 = time.perf_counter()
+        host = step(pin_a, pin_c)
+        if k:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(float(np.mean(e2e)), world, dev)
+    for got, want in zip(out, host):
+        assert np.array_equal(got.cpu().numpy(), want)
+    peak, peak_kind = measured_peaks()
+    alg = SL_B * (8 * SL_N * SL_N * 2 + 8 * 3 + 8 * SL_N * SL_N)   # a read twice, cot, sign, log, grad
+    result = {
+        "metric": "matrices per second (sign, log|det| and the gradient of log|det|)",
+        "value": world * SL_B / (ms * 1e-3), "unit": "matrices/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded N(0,1) + n I matrices)",
+        "config": {"workload": SL_WORKLOAD, "batch": SL_B, "n": SL_N,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB buffer written between timed steps"},
+        "roofline": {"bound": "hbm", "kernel": "k_slogdet + k_slogdet_grad",
+                     "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms * 1e-3) / 1e9 / peak, "traffic": None,
+                     "peak_kind": peak_kind,
+                     "note": "timed over both calls; the LU is shared-memory FMA work"},
+        "e2e": {"value": world * SL_B / (e2e_ms * 1e-3), "unit": "matrices/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": 2 * a.nbytes + cot.nbytes,
+                "d2h_bytes_per_step": 2 * 8 * SL_B + a.nbytes},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, m, t = cpu_slogdet(a, cot)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "matrices/s", "cores": 1, "kind": "port",
+            "sample": f"{m} matrices in {t:.2f} s: numpy (LAPACK) slogdet and inverse, the "
+                      "CPU path of the reference's slogdet (use_fast_kernel=False under XLA)"}
+    return result
+
+
+def cpu_slogdet(a, cot, seconds: float = 10.0):
+    """LAPACK slogdet + inverse on one host thread over repeated passes."""
+    try:
+        from threadpoolctl import threadpool_limits
+        lim = threadpool_limits(1)
+    except ImportError:
+        lim = None
+    m, t0 = 0, time.perf_counter()
+    while True:
+        np.linalg.slogdet(a)
+        cot[:, None, None] * np.swapaxes(np.linalg.inv(a), -1, -2)
+        m += len(a)
+        t = time.perf_counter() - t0
+        if t >= seconds:
+            break
+    if lim is not None:
+        lim.unregister()
+    return m / t, m, t
+
+
 def run_reference(args, rank: int, world: int):
     """Reference CPU implementation on the same workload (rank 0 only)."""
     if rank != 0:
         return None
+    if args.workload == "slogdet":
+        a, cot = slogdet_inputs(0)
+        vals, info = [], None
+        for _ in range(max(1, args.steps)):
+            rate, m, t = cpu_slogdet(a, cot, max(1.0, args.cpu_seconds / max(1, args.steps)))
+            vals.append(rate)
+            info = (m, t)
+        m, t = info
+        v = float(np.mean(vals))
+        return {
+            "impl": "reference",
+            "metric": "matrices per second (sign, log|det| and the gradient of log|det|)",
+            "value": v, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": SL_WORKLOAD, "batch": SL_B, "n": SL_N},
+            "cpu_baseline": {"value": v, "unit": "matrices/s", "cores": 1, "kind": "port",
+                             "sample": f"{m} matrices per step in {t:.2f} s: LAPACK slogdet and "
+                                       "inverse (the reference's fused kernel needs cuSolverDx, "
+                                       "absent here; its XLA fallback is LAPACK on the host)"},
+            "e2e": {"value": v, "unit": "matrices/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
     if args.workload == "det_batch":
         V, hf = det_batch_inputs(0, args.n_dets)
         vals, info = [], None
@@ -1357,7 +1503,7 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=2,
                     help="build worker streams of the served path")
     ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold",
-                                           "det_batch"],
+                                           "det_batch", "slogdet"],
                     default="single",
                     help="single: one 30-orbital system, 1e6 dets (default); batched: 64 "
                          "systems of uneven size per step; serving: Poisson request stream")
@@ -1375,7 +1521,8 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     run = {"single": run_ours, "batched": run_batched, "serving": run_serving,
-           "downfold": run_downfold, "det_batch": run_det_batch}[args.workload]
+           "downfold": run_downfold, "det_batch": run_det_batch,
+           "slogdet": run_slogdet}[args.workload]
     res = run(args, rank, world)
     if world > 1:
         import torch
