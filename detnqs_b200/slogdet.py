@@ -9,6 +9,8 @@ reference wires the kernels into JAX with ``jax.custom_vjp``,
 
 from __future__ import annotations
 
+from functools import lru_cache
+
 import numpy as np
 
 from . import native as N
@@ -77,6 +79,7 @@ def slogdet_grad(a, cot_logabs, device: int = 0):
     return g
 
 
+@lru_cache(maxsize=None)
 def _autograd():
     import torch
 
