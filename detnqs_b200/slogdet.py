@@ -85,7 +85,7 @@ def _autograd():
 
     class SlogdetFunction(torch.autograd.Function):
         """(sign, logabsdet) with the gradient of logabsdet; sign carries
-        none (the reference's _fused_logdet custom VJP, slogdet.py:103-130)."""
+        none (the reference's _fused_logdet custom VJP, slogdet.py:103-154)."""
 
         @staticmethod
         def forward(ctx, a):
