@@ -469,7 +469,7 @@ def run_ours(args, rank: int, world: int):
                                     ("f32", nnz + (nnz * 8 + n_dets * 36) / 32))},
             "note": "one L1 sector per gathered x value plus the streamed CSR sectors; peak = 1 "
                     "sector per SM clock, the rate ncu measured for the FP32 kernel on the 200k "
-                    "case (profiles/spmv_200k_full.md)"},
+                    "case"},
         "e2e": {"value": world * nnz / (e2e_ms * 1e-3), "unit": "elements/s",
                 "ms_per_step": e2e_ms, "ms_steps": [round(x, 3) for x in e2e],
                 "h2d_bytes_per_step": n_dets * 16 + 2 * n_dets * 8,

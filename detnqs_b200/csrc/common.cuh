@@ -133,8 +133,31 @@ inline bool is_device_ptr(const void* p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Rejects device memory that belongs to a GPU other than `device` (managed
+// memory is reachable from every GPU and passes).  Kernels of this library
+// read caller buffers without peer access, so such a buffer would fault.
+inline void require_on_device(const void* p, int device, const char* what) {
+    if (!p) return;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    if (a.type == cudaMemoryTypeDevice && a.device != device)
+        throw Error(DNQ_ERR_INVALID, std::string(what) + " is device memory of GPU " +
+                                         std::to_string(a.device) + ", not of GPU " +
+                                         std::to_string(device));
+}
+
+inline int current_device() {
+    int d = 0;
+    DNQ_CUDA(cudaGetDevice(&d));
+    return d;
+}
+
 // Device view of caller data: either the caller's device pointer or a fresh
-// device copy of a host buffer.
+// device copy of a host buffer.  A device pointer must be memory of the
+// current device.
 template <class T>
 struct DIn {
     const T* p = nullptr;
@@ -143,7 +166,11 @@ struct DIn {
     DIn(const T* src, size_t count, cudaStream_t st) { set(src, count, st); }
     void set(const T* src, size_t count, cudaStream_t st) {
         if (!src || count == 0) { p = nullptr; return; }
-        if (is_device_ptr(src)) { p = src; return; }
+        if (is_device_ptr(src)) {
+            require_on_device(src, current_device(), "input buffer");
+            p = src;
+            return;
+        }
         own.alloc(count, st);
         DNQ_CUDA(cudaMemcpyAsync(own.p, src, count * sizeof(T),
                                  cudaMemcpyHostToDevice, st));

@@ -9,6 +9,7 @@
 #include <sstream>
 
 #include "context.cuh"
+#include "refsort.cuh"
 
 namespace dnq {
 
@@ -92,15 +93,15 @@ __global__ void k_table_count(const double* eri, int nso, double thr, i64* count
     }
 }
 
-// Writes candidates in generation order (a ascending, then b ascending):
-// key = |v| bits, val = a | b << 8 | signbit(v) << 16.
-__global__ void k_table_fill(const double* eri, int nso, double thr, const i64* off,
-                             u64* keys, u32* vals) {
-    const i64 row = blockIdx.x;
-    int i, j;
-    row_pair(row, i, j);
+// Writes the candidates of row (i, j) with |v| >= thr in generation order
+// (a ascending, then b ascending; hb_table.cpp:103-126) at keys / vals:
+// key = |v| bits, val = a | b << 8 | signbit(v) << 16.  Called by a whole
+// block; returns the number written.
+__device__ int gen_row(const double* eri, int nso, double thr, int i, int j, u64* keys,
+                       u32* vals) {
     const int ncand = nso * (nso - 1) / 2;
     __shared__ int base;
+    __shared__ int wcount[32];
     if (threadIdx.x == 0) base = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31;
@@ -117,7 +118,6 @@ __global__ void k_table_fill(const double* eri, int nso, double thr, const i64* 
             }
         }
         // block-ordered compaction: warp ballots in warp order
-        __shared__ int wcount[32];
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) wcount[threadIdx.x >> 5] = __popc(m);
         __syncthreads();
@@ -128,8 +128,8 @@ __global__ void k_table_fill(const double* eri, int nso, double thr, const i64* 
             const double w = fabs(v);
             u64 bits;
             memcpy(&bits, &w, 8);
-            keys[off[row] + pos] = bits;
-            vals[off[row] + pos] = (u32)a | ((u32)b << 8) | ((signbit(v) ? 1u : 0u) << 16);
+            keys[pos] = bits;
+            vals[pos] = (u32)a | ((u32)b << 8) | ((signbit(v) ? 1u : 0u) << 16);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -138,6 +138,62 @@ __global__ void k_table_fill(const double* eri, int nso, double thr, const i64* 
             base += s;
         }
         __syncthreads();
+    }
+    return base;
+}
+
+__global__ void k_table_fill(const double* eri, int nso, double thr, const i64* off,
+                             u64* keys, u32* vals) {
+    const i64 row = blockIdx.x;
+    int i, j;
+    row_pair(row, i, j);
+    gen_row(eri, nso, thr, i, j, keys + off[row], vals + off[row]);
+}
+
+
+// Rows whose entries with |v| >= thr contain equal weights are rewritten in
+// the reference's order: the candidates are generated again in generation
+// order into the scratch (sk, sv at the row's offset) and sorted by the
+// restated std::sort.  Rows without ties are already in the unique
+// descending order.  One block per table row.
+__global__ void k_table_ties(const double* eri, int nso, double thr, const i64* off, u16* ab,
+                             double* tv, u64* sk, u32* sv, int* n_fixed) {
+    const i64 row = blockIdx.x;
+    const i64 lo = off[row], len = off[row + 1] - lo;
+    __shared__ i64 plen;
+    if (threadIdx.x == 0) {
+        i64 L = 0, R = len;
+        while (L < R) {
+            const i64 mid = L + (R - L) / 2;
+            if (fabs(tv[lo + mid]) >= thr) L = mid + 1; else R = mid;
+        }
+        plen = L;
+    }
+    __syncthreads();
+    const i64 P = plen;
+    int tie = 0;
+    for (i64 e = 1 + threadIdx.x; e < P; e += blockDim.x)
+        tie |= fabs(tv[lo + e]) == fabs(tv[lo + e - 1]);
+    if (!__syncthreads_or(tie)) return;
+    int i, j;
+    row_pair(row, i, j);
+    const int got = gen_row(eri, nso, thr, i, j, sk + lo, sv + lo);
+    if (threadIdx.x == 0) {
+        if (got == P) {
+            refsort::sort(refsort::Seq{sk + lo, sv + lo}, (int64_t)P);
+            atomicAdd(n_fixed, 1);
+        } else {
+            plen = 0;     // cannot happen: same candidates, same threshold
+        }
+    }
+    __syncthreads();
+    for (i64 e = threadIdx.x; e < plen; e += blockDim.x) {
+        double w;
+        const u64 bits = sk[lo + e];
+        memcpy(&w, &bits, 8);
+        const u32 x = sv[lo + e];
+        ab[lo + e] = (u16)(x & 0xffffu);
+        tv[lo + e] = (x >> 16) ? -w : w;
     }
 }
 
@@ -194,7 +250,39 @@ void build_pair_table(dnq_ctx_s* c, double thr) {
         T.off.p + 1, 0, 64, s));
     k_table_unpack<<<1024, 256, 0, s>>>(k1.p, v1.p, total, T.ab.p, T.v.p);
     DNQ_CHECK_LAUNCH();
+    // Tied weights in the reference's order; k1/v1 serve as the scratch.
+    T.tie_rows = 0;
+    DBuf<int> nfix(1, s);
+    DNQ_CUDA(cudaMemsetAsync(nfix.p, 0, sizeof(int), s));
+    k_table_ties<<<(unsigned)nrows, 256, 0, s>>>(c->erid.p, nso, thr, T.off.p, T.ab.p, T.v.p,
+                                                  k1.p, v1.p, nfix.p);
+    DNQ_CHECK_LAUNCH();
+    int nf = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&nf, nfix.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
+    T.tie_rows = nf;
+    T.tie_threshold = thr;
+}
+
+// Re-orders the tied weights of every row for a heat-bath threshold above
+// the table's own (the reference's table then holds only entries >= thr,
+// and its sort sees only those).
+void order_ties_for(dnq_ctx_s* c, double thr) {
+    PairTable& T = c->tab;
+    if (T.tie_threshold == thr || T.n_entries == 0) return;
+    cudaStream_t s = 0;
+    DBuf<u64> sk(T.n_entries, s);
+    DBuf<u32> sv(T.n_entries, s);
+    DBuf<int> nfix(1, s);
+    DNQ_CUDA(cudaMemsetAsync(nfix.p, 0, sizeof(int), s));
+    k_table_ties<<<(unsigned)T.n_rows, 256, 0, s>>>(c->erid.p, c->nso, thr, T.off.p, T.ab.p,
+                                                     T.v.p, sk.p, sv.p, nfix.p);
+    DNQ_CHECK_LAUNCH();
+    int nf = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&nf, nfix.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    T.tie_rows = nf;
+    T.tie_threshold = thr;
 }
 
 void upload_tables(dnq_ctx_s* c) {
@@ -410,6 +498,7 @@ int dnq_hb_prepare(dnq_ctx_t ctx, double threshold) {
     // The resident table keeps |v| >= 1e-15; a lower heat-bath threshold
     // needs the entries in between as well.
     if (threshold < ctx->tab.threshold) build_pair_table(ctx, threshold);
+    else order_ties_for(ctx, threshold);
     ctx->has_hb = true;
     ctx->hb_thr = threshold;
     DNQ_API_END

@@ -43,8 +43,25 @@ struct CtxView {
     const double* dos = nullptr;
     const double* sss = nullptr;
     const double* sos = nullptr;
+    const double* eri = nullptr;   // packed 8-fold (pq|rs), integral_mo.hpp:40-49
     PairTableView tab;
 };
+
+// <ij||ab> = <ij|ab> - <ij|ba> over spin-orbitals (even = alpha, odd = beta)
+// from the packed ERIs, with the spin zeroing of integral_so.hpp:89-108:
+// the value the pair table stores for row (i, j), entry (a, b).
+__host__ __device__ __forceinline__ i64 tri_index(i64 p, i64 q) {
+    return p >= q ? p * (p + 1) / 2 + q : q * (q + 1) / 2 + p;
+}
+__host__ __device__ __forceinline__ double phys_so_of(const double* eri, int mu, int ka, int nu,
+                                                      int la) {
+    if (((mu ^ nu) & 1) || ((ka ^ la) & 1)) return 0.0;
+    return eri[tri_index(tri_index(mu >> 1, nu >> 1), tri_index(ka >> 1, la >> 1))];
+}
+__host__ __device__ __forceinline__ double anti_so_of(const double* eri, int i, int j, int a,
+                                                      int b) {
+    return phys_so_of(eri, i, j, a, b) - phys_so_of(eri, i, j, b, a);
+}
 
 __host__ __device__ __forceinline__ i64 pair_row(int i, int j) {
     if (i < j) { int t = i; i = j; j = t; }
@@ -58,6 +75,8 @@ struct PairTable {
     i64 n_rows = 0;
     i64 n_entries = 0;
     double threshold = 0.0;   // entries kept: |v| >= threshold
+    double tie_threshold = -1.0;   // tied weights >= this are in the reference's order
+    i64 tie_rows = 0;              // rows re-ordered for ties at tie_threshold
     size_t bytes() const { return off.bytes() + ab.bytes() + v.bytes(); }
 };
 
@@ -84,6 +103,7 @@ struct dnq_ctx_s {
         c.dos = dos.p;
         c.sss = sss.p;
         c.sos = sos.p;
+        c.eri = erid.p;
         c.tab.off = tab.off.p;
         c.tab.ab = tab.ab.p;
         c.tab.v = tab.v.p;

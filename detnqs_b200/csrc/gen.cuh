@@ -159,11 +159,12 @@ struct Cand {
 // length of every table row for a cut shared by all rows; otherwise the
 // prefix is searched with `cut`.  Sink::step(const Cand&) is called by all
 // 32 lanes together.
+// Singles of the bra in R: alpha then beta, holes ascending outer and
+// particles ascending inner (det_ops.hpp:123-159, :248-253).
 template <class Sink>
-__device__ __forceinline__ void enumerate_row(const CtxView& C, const WarpRow& R,
-                                              const i64* plen, double cut, Sink& sink) {
+__device__ __forceinline__ void enumerate_singles(const CtxView& C, const WarpRow& R,
+                                                  Sink& sink) {
     const int lane = threadIdx.x & 31;
-    // ---- singles
     const int nsa = R.na * R.nva;
     const int nst = nsa + R.nb * R.nvb;
     for (int t0 = 0; t0 < nst; t0 += 32) {
@@ -192,6 +193,13 @@ __device__ __forceinline__ void enumerate_row(const CtxView& C, const WarpRow& R
         }
         sink.step(c);
     }
+}
+
+template <class Sink>
+__device__ __forceinline__ void enumerate_row(const CtxView& C, const WarpRow& R,
+                                              const i64* plen, double cut, Sink& sink) {
+    const int lane = threadIdx.x & 31;
+    enumerate_singles(C, R, sink);
     // ---- doubles
     for (int x = 1; x < R.ne; ++x) {
         const int i = R.occ[x];
@@ -234,6 +242,75 @@ __device__ __forceinline__ void enumerate_row(const CtxView& C, const WarpRow& R
             }
         }
     }
+}
+
+// All candidates of the bra in the order get_local_conn visits them without
+// heat-bath screening (local_conn.cpp:69-91): the singles, then every double
+// in det_ops::for_each_double's order -- alpha-alpha (hole pairs h1 < h2
+// outer, particle pairs p1 < p2 inner; det_ops.hpp:161-187), beta-beta
+// (:189-215), alpha-beta (alpha hole, alpha particle, beta hole, beta
+// particle; :217-246).  A double's element comes from the ERIs through the
+// same antisymmetrised value the pair table stores, so it has the same bits
+// as on the table walk.
+template <class Sink>
+__device__ __forceinline__ void enumerate_row_full(const CtxView& C, const WarpRow& R,
+                                                   Sink& sink) {
+    const int lane = threadIdx.x & 31;
+    enumerate_singles(C, R, sink);
+    for (int s = 0; s < 2; ++s) {
+        const u8* occ = s ? R.occb : R.occa;
+        const u8* vir = s ? R.virb : R.vira;
+        const int no = s ? R.nb : R.na, nv = s ? R.nvb : R.nva;
+        if (no < 2 || nv < 2) continue;
+        const int npv = nv * (nv - 1) / 2;
+        for (int x1 = 0; x1 < no; ++x1)
+            for (int x2 = x1 + 1; x2 < no; ++x2) {
+                const int h1 = occ[x1], h2 = occ[x2];
+                for (int t0 = 0; t0 < npv; t0 += 32) {
+                    Cand c;
+                    const int t = t0 + lane;
+                    c.valid = t < npv;
+                    c.single = false;
+                    c.a = R.a;
+                    c.b = R.b;
+                    c.h = 0.0;
+                    if (c.valid) {
+                        int y1 = 0, rem = t;          // t-th pair y1 < y2, lexicographic
+                        while (rem >= nv - 1 - y1) { rem -= nv - 1 - y1; ++y1; }
+                        const int p1 = vir[y1], p2 = vir[y1 + 1 + rem];
+                        const u64 m = (1ull << h1) | (1ull << h2) | (1ull << p1) | (1ull << p2);
+                        if (s) c.b ^= m; else c.a ^= m;
+                        const int i = 2 * h2 + s, j = 2 * h1 + s, A = 2 * p2 + s, B = 2 * p1 + s;
+                        c.h = double_elem(R.a, R.b, i, j, A, B, anti_so_of(C.eri, i, j, A, B));
+                    }
+                    sink.step(c);
+                }
+            }
+    }
+    if (!R.na || !R.nva || !R.nb || !R.nvb) return;
+    const int nsb = R.nb * R.nvb;
+    for (int xa = 0; xa < R.na; ++xa)
+        for (int ya = 0; ya < R.nva; ++ya) {
+            const int ha = R.occa[xa], pa = R.vira[ya];
+            const u64 ka = R.a ^ (1ull << ha) ^ (1ull << pa);
+            for (int t0 = 0; t0 < nsb; t0 += 32) {
+                Cand c;
+                const int t = t0 + lane;
+                c.valid = t < nsb;
+                c.single = false;
+                c.a = ka;
+                c.b = R.b;
+                c.h = 0.0;
+                if (c.valid) {
+                    const int hb = R.occb[t / R.nvb], pb = R.virb[t % R.nvb];
+                    c.b = R.b ^ (1ull << hb) ^ (1ull << pb);
+                    const int sa = 2 * ha, sb = 2 * hb + 1, ta = 2 * pa, tb = 2 * pb + 1;
+                    const int i = max(sa, sb), j = min(sa, sb), A = max(ta, tb), B = min(ta, tb);
+                    c.h = double_elem(R.a, R.b, i, j, A, B, anti_so_of(C.eri, i, j, A, B));
+                }
+                sink.step(c);
+            }
+        }
 }
 
 }  // namespace dnq

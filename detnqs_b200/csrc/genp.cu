@@ -279,6 +279,7 @@ struct ConnParams {
     double single_thr;
     const i64* plen;
     double cut;
+    bool full_order;     // no heat-bath screening: doubles in for_each_double's order
     int* next_row;
     u32* cnt;
     const i64* off;
@@ -335,7 +336,8 @@ __global__ void __launch_bounds__(kW * 32) k_conn(ConnParams P) {
         } else if (dk && lane == 0) {
             sink.c = 1;
         }
-        enumerate_row(P.C, R, P.plen, P.cut, sink);
+        if (P.full_order) enumerate_row_full(P.C, R, sink);
+        else enumerate_row(P.C, R, P.plen, P.cut, sink);
         if (!FILL) {
             const u32 c = __reduce_add_sync(0xffffffffu, sink.c);
             if (lane == 0) P.cnt[r] = c;
@@ -629,6 +631,7 @@ void local_connections(dnq_ctx_s* ctx, const u64* Vd, i64 n, int n_orb, bool use
     P.single_thr = use_hb ? std::max(eps1, kElemThresh) : kElemThresh;   // local_conn.cpp:56-58
     P.plen = plen.p;
     P.cut = cut;
+    P.full_order = !use_hb;
     P.next_row = next.p;
     P.cnt = cnt.p;
     const int grid = grid_of((const void*)k_conn<false>, ctx->device, kW * 32);

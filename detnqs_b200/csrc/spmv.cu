@@ -579,6 +579,7 @@ int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc, double* out
         spmv_block(h, h->vv, xd.p, y.p, nullptr, DNQ_F64, s, nullptr, nullptr);
     }
     const bool dev_eloc = eloc && is_device_ptr(eloc);
+    if (dev_eloc) require_on_device(eloc, h->device, "eloc");
     DBuf<double> ebuf;
     double* ed = nullptr;
     if (eloc) {

@@ -229,11 +229,17 @@ int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc,
  * scratch (FP32 copy of x, reduction partials) is a file-scope device array
  * of 4 MiB + 74 KiB that every GPU loading the library holds until exit, so
  * n_V is limited to 1048576 (larger handles are rejected).  x and eloc must
- * be device memory; eloc first receives H x and then y_i / x_i.  DNQ_F32
- * needs the handle's FP32 values to exist (one earlier FP32 call).  The
- * first call on a device sets up the scratch address with that device
- * current: make it before any stream capture.  All calls share the scratch:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * be non-overlapping device memory of the handle's GPU (eloc is required; it
+ * first receives H x and then y_i / x_i).  out2 may be device memory of that
+ * GPU (the call then only enqueues work on the stream) or host memory (the
+ * call copies the pair back and waits for the stream).  DNQ_F32 needs the
+ * handle's FP32 values to exist (one earlier FP32 call); the sums always use
+ * the CSR kernel, so with DNQ_OPT_SPMV_PANELS on they match the allocating
+ * FP32 path to compensated precision, not bit for bit.  The first call on a
+ * device sets up the scratch address with that device current: make it
+ * before any stream capture; the address is cached per device ordinal and
+ * does not survive cudaDeviceReset.  All calls share the scratch: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
 int dnq_ham_local_energy_noalloc(dnq_ham_t h, const double* x, double* eloc,
                                  double* out2, int precision, void* stream);
 

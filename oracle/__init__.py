@@ -40,9 +40,22 @@ class OracleError(RuntimeError):
     pass
 
 
-def build(reference_root: str | None = "/root/reference", quiet: bool = True) -> None:
-    """Compile the restatement and, if the reference tree exists, the
-    reference core.  Building the checker is not using it."""
+REFERENCE_ENV = "DETNQS_REFERENCE_ROOT"
+
+
+def reference_root() -> str | None:
+    """The reference source tree named by $DETNQS_REFERENCE_ROOT, if that
+    variable is set and the tree is there."""
+    root = os.environ.get(REFERENCE_ENV)
+    return root if root and os.path.isdir(os.path.join(root, "csrc")) else None
+
+
+def build(reference_root: str | None = None, quiet: bool = True) -> None:
+    """Compile the restatement and, if a reference tree is given (or named
+    by $DETNQS_REFERENCE_ROOT) and exists, the reference core.  Building the
+    checker is not using it."""
+    if reference_root is None:
+        reference_root = globals()["reference_root"]()
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True,
                    stdout=out, stderr=out)

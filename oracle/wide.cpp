@@ -145,8 +145,11 @@ struct HB {
                         const double w = std::abs(I.anti(i, j, a, b));
                         if (w >= thr) r.push_back({w, {(int16_t)a, (int16_t)b}});
                     }
-                std::stable_sort(r.begin(), r.end(),
-                                 [](auto& x, auto& y) { return x.first > y.first; });
+                // std::ranges::sort(row, std::greater{}, &Entry::w) of the
+                // reference (hb_table.cpp:133) is libstdc++'s std::sort with
+                // this comparison: the same (unstable) order of tied weights.
+                std::sort(r.begin(), r.end(),
+                          [](const auto& x, const auto& y) { return x.first > y.first; });
             }
         off.assign(nrows + 1, 0);
         for (size_t t = 0; t < nrows; ++t) off[t + 1] = off[t] + rows[t].size();

@@ -16,7 +16,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE_TREE = "/root/reference"
+# The reference source tree, when $DETNQS_REFERENCE_ROOT names one (tests
+# that read its files skip without it).
+REFERENCE_TREE = os.environ.get("DETNQS_REFERENCE_ROOT", "")
 
 
 def pytest_configure(config):

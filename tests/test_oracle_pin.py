@@ -17,7 +17,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import REFERENCE_TREE, assert_coo_equal, coo_of
+from conftest import GOLDEN, assert_coo_equal, coo_of
 from detnqs_b200 import synthetic as S
 
 
@@ -155,16 +155,23 @@ def test_collector_counts(port):
     assert len(c) == 26
 
 
-def _ref_fcidump(name):
-    p = os.path.join(REFERENCE_TREE, "benchmark", "FCIDUMP", name)
-    if not os.path.exists(p):
-        pytest.skip("reference FCIDUMP fixtures not present")
-    return p
+def _ref_fcidump(name, tmp_path):
+    """One of the reference's FCIDUMP fixtures, rewritten from the packed
+    integrals committed in tests/golden/molecules.npz (%.17e, exact), so the
+    checker's FCIDUMP reader runs without the reference tree."""
+    from types import SimpleNamespace
+    z = np.load(os.path.join(GOLDEN, "molecules.npz"))
+    n, na, nb = (int(x) for x in z[name + "_shape"])
+    path = str(tmp_path / (name + ".FCIDUMP"))
+    S.write_fcidump(path, SimpleNamespace(n_orb=n, n_alpha=na, n_beta=nb, n_elec=na + nb,
+                                          h1e=z[name + "_h1e"], eri=z[name + "_eri"],
+                                          e_core=float(z[name + "_e_nuc"])))
+    return path
 
 
-def test_h2_integrals_known_answers(port):
+def test_h2_integrals_known_answers(port, tmp_path):
     """H2/6-31G values (test_integral.cpp:65-117) through the oracle."""
-    ctx = port.ctx_from_fcidump(_ref_fcidump("H2_631g_2.00.FCIDUMP"), 4)
+    ctx = port.ctx_from_fcidump(_ref_fcidump("h2_631g", tmp_path), 4)
     assert abs(ctx.get_e_nuc() - 0.26458860546) < 1e-10
     # diagonal of the HF determinant = h00 + h00 + (00|00) (alpha 0, beta 0)
     hf = np.array([[1, 1]], np.uint64)
@@ -179,9 +186,9 @@ def _fci_dets(n, na, nb):
     return np.array([[a, b] for a in A for b in B], np.uint64)
 
 
-def test_h2o_fci_energy(port):
+def test_h2o_fci_energy(port, tmp_path):
     """E_FCI(H2O/STO-3G) = -75.01240139 Ha, 441 dets (test_hamiltonian.cpp:282-295)."""
-    ctx = port.ctx_from_fcidump(_ref_fcidump("H2O_sto3g.FCIDUMP"), 7)
+    ctx = port.ctx_from_fcidump(_ref_fcidump("h2o_sto3g", tmp_path), 7)
     V = _fci_dets(7, 5, 5)
     assert len(V) == 441
     h = ctx.get_ham_vv(V)
@@ -192,10 +199,10 @@ def test_h2o_fci_energy(port):
     assert abs(e - (-75.01240139)) <= 1e-7 * 75.01240139
 
 
-def test_h2o_heatbath_discovery(port):
+def test_h2o_heatbath_discovery(port, tmp_path):
     """HB discovery from HF at eps1=1e-6 gives |P| in [20, 140] without HF
     (test_hamiltonian.cpp:201-225), and H_eff lowers E(HF) (:260-279)."""
-    ctx = port.ctx_from_fcidump(_ref_fcidump("H2O_sto3g.FCIDUMP"), 7)
+    ctx = port.ctx_from_fcidump(_ref_fcidump("h2o_sto3g", tmp_path), 7)
     ctx.hb_prepare(1e-15)
     hf = np.array([[0b11111, 0b11111]], np.uint64)
     r = ctx.get_ham_conn(hf, True, 1e-6)
