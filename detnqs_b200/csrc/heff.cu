@@ -373,31 +373,32 @@ __global__ void k_compact(const i64* capoff, const u32* tcol, const double* tval
 // Long rows.  For t in [t0, t1) of H_VP row i: the diagonal term of k =
 // col[t] (H_PV[k, i] is the same stored value as H_VP[i, k], the transpose
 // copies it), a flag for k's whose column holds other rows, and whether any
-// k is kept.  FP64 terms are a*D^-1*a with the kernel's unfused operations;
-// FP32 terms are the TwoProduct pair of the float-pair a*D^-1 and a.
-__global__ void k_long_terms(const u32* vpcol, const double* vpval, const float* vpval32,
-                             const i64* pvrp, const double* dinv, const u8* skip, i64 t0, i64 t1,
-                             bool f32, double* term, float2* term2, u8* multi, u32* touch) {
+// k is kept.  FP64 terms are a*D^-1*a with the kernel's unfused operations.
+// In FP32 mode a long row keeps its FP64 values: such a row (a reference
+// determinant's, millions of entries whose terms all add to one diagonal
+// element) would otherwise carry the rounding of every stored value into the
+// energy (measured: 1.4e-6 Ha on 100 orbitals).  Its FP32-mode terms are the
+// same FP64 products, split into (hi, lo) float pairs for the float-float
+// sum.
+__global__ void k_long_terms(const u32* vpcol, const double* vpval, const i64* pvrp,
+                             const double* dinv, const u8* skip, i64 t0, i64 t1, bool f32,
+                             double* term, float2* term2, u8* multi, u32* touch) {
     for (i64 t = t0 + blockIdx.x * (i64)blockDim.x + threadIdx.x; t < t1;
          t += (i64)gridDim.x * blockDim.x) {
         const u32 k = vpcol[t];
         const bool sk = skip[k] != 0;
         const double s = dinv[k];
-        const double a = f32 ? (double)vpval32[t] : vpval[t];
+        const double a = vpval[t];
         const bool need = !sk && !(a == 0.0 || s == 0.0);
         const i64 x = t - t0;
         multi[x] = (!sk && pvrp[k + 1] - pvrp[k] > 1) ? 1 : 0;
         if (!sk) atomicOr(touch, 1u);
+        const double v = need ? __dmul_rn(__dmul_rn(a, s), a) : 0.0;
         if (!f32) {
-            term[x] = need ? __dmul_rn(__dmul_rn(a, s), a) : 0.0;
+            term[x] = v;
         } else {
-            const double asd = __dmul_rn(a, s);
-            const float as = (float)asd;
-            const float as_lo = (float)(asd - (double)as);
-            const float b = (float)a;
-            const float p = __fmul_rn(as, b);
-            const float pe = fmaf(as, b, -p) + __fmul_rn(as_lo, b);
-            term2[x] = need ? make_float2(p, pe) : make_float2(0.0f, 0.0f);
+            const float hi = (float)v;
+            term2[x] = make_float2(hi, (float)(v - (double)hi));
         }
     }
 }
@@ -473,7 +474,8 @@ __global__ void k_long_merge32(const float2* part, float2* out) {
 // Expansion of a long row's shared columns: for each kept k (list of VP
 // positions t, ascending) every H_PV entry (j != i) of column k gives one
 // term; FP64 terms a*D^-1*b with the kernel's unfused operations, FP32
-// terms the TwoProduct pair of the float-pair a*D^-1 and b.
+// terms the TwoProduct pair of the float pair of a*D^-1 (a is the long
+// row's FP64 value in both modes) and the FP32 b.
 __global__ void k_esc_count(const u32* list, i64 n, const u32* vpcol, const i64* pvrp, u32* cnt) {
     for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n;
          x += (i64)gridDim.x * blockDim.x) {
@@ -483,7 +485,7 @@ __global__ void k_esc_count(const u32* list, i64 n, const u32* vpcol, const i64*
 }
 
 __global__ void k_esc_fill(const u32* list, i64 n, const i64* off, u32 row, const u32* vpcol,
-                           const double* vpval, const float* vpval32, const i64* pvrp,
+                           const double* vpval, const i64* pvrp,
                            const u32* pvcol, const double* pvval, const float* pvval32,
                            const double* dinv, bool f32, u32* key, double* term, float2* term2) {
     for (i64 x = blockIdx.x * (i64)blockDim.x + threadIdx.x; x < n;
@@ -491,7 +493,7 @@ __global__ void k_esc_fill(const u32* list, i64 n, const i64* off, u32 row, cons
         const i64 t = list[x];
         const u32 k = vpcol[t];
         const double s = dinv[k];
-        const double a = f32 ? (double)vpval32[t] : vpval[t];
+        const double a = vpval[t];          // the long row's FP64 value, in both modes
         const bool need = !(a == 0.0 || s == 0.0);
         const double asd = __dmul_rn(a, s);
         const float as = (float)asd;
@@ -741,7 +743,7 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             if (precision == DNQ_F32) term2.alloc(m, s);
             else term.alloc(m, s);
             DBuf<u8> multi(m, s);
-            k_long_terms<<<gs(m), 256, 0, s>>>(VP.col.p, VP.val.p, P.vpval32, PV.rowptr.p, dinv.p,
+            k_long_terms<<<gs(m), 256, 0, s>>>(VP.col.p, VP.val.p, PV.rowptr.p, dinv.p,
                                                skip.p, t0, t1, precision == DNQ_F32, term.p,
                                                term2.p, multi.p, ltouch.p + q);
             DNQ_CHECK_LAUNCH();
@@ -788,7 +790,7 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             i64 nruns = 0;
             if (ne) {
                 k_esc_fill<<<gs(ns), 256, 0, s>>>(sel.p, ns, eoff.p, (u32)longs[q], VP.col.p,
-                                                  VP.val.p, P.vpval32, PV.rowptr.p, PV.col.p,
+                                                  VP.val.p, PV.rowptr.p, PV.col.p,
                                                   PV.val.p, P.pvval32, dinv.p,
                                                   precision == DNQ_F32, ekey.p, eterm.p,
                                                   eterm2.p);

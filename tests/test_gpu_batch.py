@@ -121,3 +121,71 @@ def test_apply_on_resident_blocks(workload, prec):
     t = bt.timings()
     assert set(t) == {"diag", "build", "compact", "hpsi"} and t["build"] > 0
     bt.close()
+
+
+# ---------------------------------------------------------------------------
+# Mixed widths: systems of at most and of more than 32 orbitals in one batch
+# (the per-row scan word), with one system above 20000 determinants (arena
+# chunks overflow, long rows inside the batch)
+# ---------------------------------------------------------------------------
+
+@pytest.fixture(scope="module")
+def mixed_workload():
+    from detnqs_b200 import batch as B
+    from detnqs_b200 import core
+    # n_orb = [36, 33, 40, 34, 26, 28], dets = [22500, 4708, 6306, 2290, 39901, 4037]
+    w = B.make_batch_workload(n_sys=6, seed=5, n_min=26, n_max=40, dets_min=2000,
+                              dets_max=40000)
+    ctxs = []
+    for bs in w:
+        c = core.IntCtx.from_arrays(bs.sysm.n_orb, bs.sysm.h1e, bs.sysm.eri, bs.sysm.e_core)
+        c.hb_prepare(1e-15)
+        ctxs.append(c)
+    yield w, ctxs
+    for c in ctxs:
+        c.close()
+
+
+def test_mixed_width_batch_matches_single_builds_and_oracle(mixed_workload, port):
+    from detnqs_b200 import batch as B
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    from detnqs_b200 import synthetic as S
+    w, ctxs = mixed_workload
+    n_orbs = [x.sysm.n_orb for x in w]
+    sizes = [len(x.dets) for x in w]
+    assert min(n_orbs) <= 32 < max(n_orbs)
+    assert max(sizes) > 20000
+    bt = B.Batch(ctxs, [x.dets for x in w], n_orbs, eps1=1e-7)
+    blocks = [bt.coo(k) for k in range(bt.n_sys)]
+    for k, (bs, c) in enumerate(zip(w, ctxs)):
+        H = D.build(c, bs.dets, n_orb=bs.sysm.n_orb, policy=N.POLICY_STATIC,
+                    use_heatbath=True, eps1=1e-7, want_vp=False)
+        assert_coo_equal(blocks[k], H.to_coo(0))
+        H.close()
+    # the largest system of each width, row by row against the oracle:
+    # 32 random rows and the 16 longest
+    for k in (int(np.argmax([s if n <= 32 else -1 for n, s in zip(n_orbs, sizes)])),
+              int(np.argmax([s if n > 32 else -1 for n, s in zip(n_orbs, sizes)]))):
+        bs, blk = w[k], blocks[k]
+        lens = np.bincount(blk["row"].astype(np.int64), minlength=sizes[k])
+        rows = np.unique(np.concatenate([
+            np.argsort(-lens, kind="stable")[:16],
+            np.random.default_rng(k).choice(sizes[k], 32, replace=False)]))
+        o = port.ctx_from_arrays(bs.sysm.n_orb, bs.sysm.h1e, bs.sysm.eri, bs.sysm.e_core)
+        o.hb_prepare(1e-15)
+        want = o.vv_hb_rows(bs.dets, rows, 1e-7)
+        sel = np.isin(blk["row"], rows)
+        got = {"row": blk["row"][sel], "col": blk["col"][sel], "val": blk["val"][sel],
+               "shape": blk["shape"]}
+        assert_coo_equal(got, want)
+    # energies of one step against the single-system path
+    psi = np.concatenate([S.normalized_psi(n, 60 + k) for k, n in enumerate(sizes)])
+    e, _ = bt.step(psi, precision=N.F64, graph=True)
+    for k, (bs, c) in enumerate(zip(w, ctxs)):
+        H = D.build(c, bs.dets, n_orb=bs.sysm.n_orb, policy=N.POLICY_STATIC,
+                    use_heatbath=True, eps1=1e-7, want_vp=False)
+        num, den = H.local_energy(psi[bt.offsets[k]:bt.offsets[k + 1]])
+        assert abs(e[k, 0] / e[k, 1] - num / den) < 1e-12
+        H.close()
+    bt.close()

@@ -268,6 +268,40 @@ def test_spmv_device_tensors(core, c0):
 
 
 # ---------------------------------------------------------------------------
+# The bench's single-system workload itself: 30 orbitals, 12 alpha / 12 beta,
+# K = 60, 10^6 heat-bath-sampled determinants, eps1 = 1e-6, default arena
+# chunk.  Rows longer than a chunk go through the long-row kernels.
+# ---------------------------------------------------------------------------
+
+def test_bench_workload_rows_match_oracle(core, port):
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(30, 12, 12, 60, 1001)
+    V = S.heat_bath_sample(sysm, 1_000_000, 2002)
+    ctx = core.IntCtx.from_arrays(30, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    H = D.build(ctx, V, n_orb=30, policy=N.POLICY_STATIC, use_heatbath=True, eps1=1e-6,
+                want_vp=False)
+    rp, cols, vals = H.to_csr_arrays(0)
+    lens = np.diff(rp)
+    assert lens.max() > 8192                    # rows over one arena chunk exist
+    rows = np.unique(np.concatenate([np.argsort(-lens, kind="stable")[:16],
+                                     np.random.default_rng(1).choice(len(V), 64,
+                                                                     replace=False)]))
+    octx = port.ctx_from_arrays(30, sysm.h1e, sysm.eri, sysm.e_core)
+    octx.hb_prepare(1e-15)
+    o = octx.vv_hb_rows(V, rows, 1e-6)
+    got = {"row": np.repeat(rows, lens[rows]).astype(np.uint32),
+           "col": np.concatenate([cols[rp[r]:rp[r + 1]] for r in rows]),
+           "val": np.concatenate([vals[rp[r]:rp[r + 1]] for r in rows]),
+           "shape": (len(V), len(V))}
+    # copy_csr returns each row sorted by column, as the COO the oracle gives
+    assert_coo_equal(got, o)
+    H.close()
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------
 # Larger heat-bath-sampled space (30 orbitals): row subset vs the oracle
 # ---------------------------------------------------------------------------
 
