@@ -39,6 +39,20 @@ def _f64(x, n: int | None = None):
     return a
 
 
+def _f64_2d(X, n: int):
+    """n x k FP64, C order (numpy or CUDA tensor)."""
+    if hasattr(X, "is_cuda") and X.is_cuda:
+        import torch
+        t = X.to(torch.float64).contiguous()
+        if t.dim() != 2 or t.shape[0] != n:
+            raise ValueError("X must be n_V x k")
+        return t
+    a = np.ascontiguousarray(X, dtype=np.float64)
+    if a.ndim != 2 or a.shape[0] != n:
+        raise ValueError("X must be n_V x k")
+    return a
+
+
 class DeviceHamiltonian:
     """Owner of one ``dnq_ham_t``."""
 
@@ -139,6 +153,33 @@ class DeviceHamiltonian:
         N.check(N.lib.dnq_ham_proxy_spmv(self._h, N.ptr(xv), N.ptr(xp), N.ptr(dp), N.ptr(yv),
                                          N.ptr(yp), precision, N.stream_of(xv, xp)))
         return yv, yp
+
+    def spmv_multi(self, X, out=None, precision: int = N.F64):
+        """Y = H_VV X for the k columns of X (n_V x k, C order): one pass over
+        the CSR for up to 8 (FP32) or 4 (FP64) vectors.  X, out may be numpy
+        (host) or CUDA tensors."""
+        X = _f64_2d(X, self.n_v)
+        k = X.shape[1]
+        if out is None:
+            if isinstance(X, np.ndarray):
+                out = np.empty((self.n_v, k), np.float64)
+            else:
+                import torch
+                out = torch.empty((self.n_v, k), dtype=torch.float64, device=X.device)
+        N.check(N.lib.dnq_ham_spmv_multi(self._h, N.ptr(X), N.ptr(out), k, precision,
+                                         N.stream_of(X, out)))
+        return out
+
+    def local_energy_multi(self, X, eloc=None, precision: int = N.F64) -> np.ndarray:
+        """Returns out[k, 2] = (x_j.Hx_j, x_j.x_j) of the columns of X; fills
+        ``eloc`` (n_V x k) when given."""
+        X = _f64_2d(X, self.n_v)
+        k = X.shape[1]
+        out = np.zeros(2 * k)
+        N.check(N.lib.dnq_ham_local_energy_multi(self._h, N.ptr(X), N.ptr(eloc),
+                                                 out.ctypes.data, k, precision,
+                                                 N.stream_of(X, eloc)))
+        return out.reshape(k, 2)
 
     def local_energy(self, x, eloc=None, precision: int = N.F64):
         """Returns (x.Hx, x.x); fills ``eloc`` (y_i / x_i) when given."""

@@ -56,7 +56,8 @@ EXPORTS = (
     "dnq_ham_spmv", "dnq_ham_proxy_spmv", "dnq_ham_local_energy",
     "dnq_variational_energy", "dnq_ham_eff", "dnq_ham_eff_from", "dnq_ham_p_diag",
     "dnq_ham_block_spmv", "dnq_gen_dets", "dnq_local_connections", "dnq_conn_copy",
-    "dnq_pt2", "dnq_ham_local_energy_noalloc",
+    "dnq_pt2", "dnq_ham_local_energy_noalloc", "dnq_ham_spmv_multi",
+    "dnq_ham_local_energy_multi",
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
     "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
@@ -129,6 +130,8 @@ _sig("dnq_ham_proxy_spmv", _P, _P, _P, _P, _P, _P, _I, _P)
 _sig("dnq_ham_local_energy", _P, _P, _P, _P, _I, _P)
 _sig("dnq_ham_block_spmv", _P, _I, _P, _P, _I, _P)
 _sig("dnq_ham_local_energy_noalloc", _P, _P, _P, _P, _I, _P)
+_sig("dnq_ham_spmv_multi", _P, _P, _P, _I, _I, _P)
+_sig("dnq_ham_local_energy_multi", _P, _P, _P, _P, _I, _I, _P)
 _sig("dnq_ham_p_diag", _P, _P, _P, _P)
 _sig("dnq_gen_dets", _P, _P, _I64, _I, _P, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_local_connections", _P, _P, _I64, _I, _I, _D, _P, C.POINTER(_P))

@@ -222,6 +222,22 @@ int dnq_ham_block_spmv(dnq_ham_t h, int block, const double* x, double* y,
 int dnq_ham_local_energy(dnq_ham_t h, const double* x, double* eloc,
                          double* out2, int precision, void* stream);
 
+/* H applied to k amplitude vectors at once (no reference counterpart: the
+ * reference applies H to one psi per SciPy call, kernel.py:75-78).  X and Y
+ * are n_V x k row-major FP64 arrays (vector j is column j), host or device
+ * memory.  The vectors are gathered interleaved, 8 FP32 or 4 FP64 values
+ * per 32-byte sector, so one pass over the CSR serves up to 8 (FP32) or 4
+ * (FP64) vectors; larger k runs in passes.  Every column equals
+ * dnq_ham_spmv of that vector bit for bit (CSR kernel, same lanes per
+ * row).  1 <= k <= 1024. */
+int dnq_ham_spmv_multi(dnq_ham_t h, const double* X, double* Y, int k,
+                       int precision, void* stream);
+/* Local energies of k vectors in one pass: out[2j] = x_j.H x_j,
+ * out[2j+1] = x_j.x_j (the sums of dnq_ham_local_energy, bit for bit);
+ * eloc (n_V x k row-major, may be NULL) = (H x_j)_i / x_ij. */
+int dnq_ham_local_energy_multi(dnq_ham_t h, const double* X, double* eloc,
+                               double* out, int k, int precision, void* stream);
+
 /* Same result as dnq_ham_local_energy without allocating device memory.
  * No counterpart in the reference: it serves callers that may not allocate
  * on their own -- an XLA custom call (JAX FFI) that runs inside XLA's memory
