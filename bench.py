@@ -376,6 +376,32 @@ def run_ours(args, rank: int, world: int):
         torch.cuda.synchronize()
         ss[key] = a.elapsed_time(b) / reps
 
+    # ---- several amplitude sets per pass: k vectors gathered interleaved
+    # (8 FP32 or 4 FP64 per 32-byte sector), each column equal to the
+    # single-vector result bit for bit
+    from detnqs_b200 import synthetic as S
+    multi = {}
+    for prec, key, kv in ((native.F32, "f32_k8", 8), (native.F64, "f64_k4", 4)):
+        Xk = torch.from_numpy(np.stack([S.normalized_psi(n_dets, PSI_SEED + 100 + j)
+                                        for j in range(kv)], 1)).to(dev)
+        Yk = torch.empty_like(Xk)
+        for _ in range(2):
+            last.spmv_multi(Xk, out=Yk, precision=prec)
+        reps = 20
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            last.spmv_multi(Xk, out=Yk, precision=prec)
+        b.record()
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / reps
+        multi[key] = {"vectors": kv, "ms_per_pass": t,
+                      "e_loc_per_s": kv * n_dets / (t * 1e-3),
+                      "speedup_vs_fp64_single_vector": kv * ss["f64"] / t}
+        del Xk, Yk
+
     # ---- end to end through the C ABI with host buffers
     pin_V = torch.from_numpy(V.view(np.int64)).pin_memory()
     pin_psi = torch.from_numpy(psi).pin_memory()
@@ -431,6 +457,7 @@ def run_ours(args, rank: int, world: int):
         "e_loc_per_s_fp32": n_dets / (float(np.mean(t_e32)) * 1e-3),
         "hpsi_steady_ms": ss,
         "e_loc_per_s_steady": {k: n_dets / (v * 1e-3) for k, v in ss.items()},
+        "hpsi_multi_vector": multi,
         "build_elements_per_s": nnz / (float(np.mean(t_build)) * 1e-3),
         "candidates_per_s": cand / (float(np.mean(t_build)) * 1e-3),
         "dE_fp32_vs_fp64_Ha": dE,

@@ -77,10 +77,19 @@ struct Gather<2, double> {
 
 // Y[r][j] (j < kx) = sum_k H_rk X[k][j], for K interleaved columns.  The
 // slot walk, masking and accumulation order are those of row_acc in
-// spmv.cu, with K accumulators per lane.
+// spmv.cu, with K accumulators per lane.  Entries outside the row read the
+// zero row nr of Xg (and a zero value), which adds the same +0 products as
+// the single-vector kernel's masking without a branch per entry.
 //   T = double: FP64 values and X (AccF64)
-//   T = float : FP32 off-diagonal values and X32, Dot2 sums, plus the FP64
+//   T = float : FP32 off-diagonal values and X32, Kahan sums, plus the FP64
 //               diagonal term diag_r * X64[r][j] added in FP64 (AccF32)
+// The G lanes of a row then combine their K sums with the single-vector
+// kernel's butterfly pairs (lane ^ G/2, ..., lane ^ 1) as a reduce-scatter:
+// while a lane holds more than one column, each step it keeps half of them
+// (the lower half when its bit o is clear) and hands the other half to its
+// partner, so a column is merged with exactly the values it meets in the
+// single-vector butterfly, at a fraction of the shuffles.  Lane l ends with
+// columns [j0, j0 + K / min(K, G)).
 template <int G, int U, int K, class T, class Acc>
 __global__ void __launch_bounds__(256)
 k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restrict__ val,
@@ -90,6 +99,7 @@ k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
     const int sub = threadIdx.x & (G - 1);
     const i64 ngroups = (gridDim.x * (i64)blockDim.x) / G;
     const i64 rounds = (nr + ngroups - 1) / ngroups;
+    const u32 zrow = (u32)nr;
     for (i64 it = 0; it < rounds; ++it) {
         const i64 r = gid + it * ngroups;
         Acc acc[K];
@@ -109,7 +119,7 @@ k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const bool ok = k < e && k + q < nnz;
-                            c[u][q] = ok ? __ldg(&col[k + q]) : 0u;
+                            c[u][q] = ok ? __ldg(&col[k + q]) : zrow;
                             v[u][q] = ok ? __ldg(&val[k + q]) : T(0);
                         }
                     }
@@ -121,13 +131,8 @@ k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
                     for (int q = 0; q < 4; ++q) {
                         const i64 kk = k0 + (i64)u * 4 * G + q;
                         const bool in = kk >= b && kk < e;
-                        if (in) {
-                            Gather<K, T>::get(Xg, c[u][q], xv[u][q]);
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < K; ++j) xv[u][q][j] = T(0);
-                            v[u][q] = T(0);
-                        }
+                        Gather<K, T>::get(Xg, in ? c[u][q] : zrow, xv[u][q]);
+                        if (!in) v[u][q] = T(0);
                     }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -139,30 +144,54 @@ k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
                     }
             }
         }
+        // reduce-scatter over the butterfly pairs
+        int j0 = 0;
 #pragma unroll
-        for (int j = 0; j < K; ++j) acc[j].reduce(G);
-        if (sub == 0 && r < nr) {
+        for (int o = G / 2, kc = K; o; o >>= 1) {
+            if (kc > 1) {
+                const int h = kc / 2;
+                const bool upper = (sub & o) != 0;
 #pragma unroll
-            for (int j = 0; j < K; ++j) {
-                if (j >= kx) break;
-                double y = acc[j].value();
-                if (diag) y += diag[r] * X[r * (i64)ldx + j];
-                Y[r * (i64)ldy + j] = y;
+                for (int i = 0; i < K / 2; ++i) {
+                    if (i >= h) break;
+                    const Acc give = upper ? acc[i] : acc[i + h];
+                    const Acc got = give.shfl(o);
+                    Acc keep = upper ? acc[i + h] : acc[i];
+                    keep.merge(got);
+                    acc[i] = keep;
+                }
+                if (upper) j0 += h;
+                kc = h;
+            } else {
+                acc[0].merge(acc[0].shfl(o));
+            }
+        }
+        constexpr int kOwn = K > G ? K / G : 1;
+        const bool writer = (K >= G) || (sub & (G / K - 1)) == 0;
+        if (r < nr && writer) {
+#pragma unroll
+            for (int i = 0; i < kOwn; ++i) {
+                const int j = j0 + i;
+                if (j < kx) {
+                    double y = acc[i].value();
+                    if (diag) y += diag[r] * X[r * (i64)ldx + j];
+                    Y[r * (i64)ldy + j] = y;
+                }
             }
         }
     }
 }
 
 // Interleaved gather copy of the first kx columns of X (n x ldx, FP64):
-// FP32 or FP64, zero-padded to K columns.
+// FP32 or FP64, zero-padded to K columns, plus a zero row n.
 template <int K, class T>
 __global__ void k_interleave(const double* __restrict__ X, int ldx, int kx, i64 n,
                              T* __restrict__ Xg) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n * K;
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < (n + 1) * K;
          t += (i64)gridDim.x * blockDim.x) {
         const i64 r = t / K;
         const int j = (int)(t - r * K);
-        Xg[t] = j < kx ? (T)X[r * ldx + j] : T(0);
+        Xg[t] = (j < kx && r < n) ? (T)X[r * ldx + j] : T(0);
     }
 }
 
@@ -247,12 +276,13 @@ void launch_spmm(const Csr& m, const T* val, const T* Xg, const double* diag, co
     DNQ_CHECK_LAUNCH();
 }
 
-// Slots per lane in flight: the single-vector choice, at most 2 for 8
-// columns (registers).  Results do not depend on it.
+// Slots per lane in flight: the single-vector choice for 2 columns, 2 for 4
+// and 8 (measured best on the 10^6-determinant matrix; 4 would not fit the
+// registers of 8 columns).  Results do not depend on it.
 template <int K, class T, class Acc>
 void spmm_g(int G, int U, const Csr& m, const T* val, const T* Xg, const double* diag,
             const double* X, int ldx, int kx, double* Y, int ldy, int device, cudaStream_t s) {
-    if (K >= 8 && U > 2) U = 2;
+    if (K >= 4) U = 2;
 #define DNQ_SPMM_U(GG)                                                                        \
     switch (U) {                                                                              \
         case 4: launch_spmm<GG, 4, K, T, Acc>(m, val, Xg, diag, X, ldx, kx, Y, ldy, device, s); \
@@ -317,10 +347,10 @@ void spmm_vv(dnq_ham_s* h, const double* X, int ldx, int kx, double* Y, int ldy,
     }
 }
 
-// Bytes of the interleaved scratch for kx columns.
+// Bytes of the interleaved scratch for kx columns (n rows and a zero row).
 size_t spmm_scratch_bytes(i64 n, int kx, int precision) {
-    if (precision == DNQ_F32) return (size_t)n * 4 * (kx <= 2 ? 2 : kx <= 4 ? 4 : 8);
-    return (size_t)n * 8 * (kx <= 2 ? 2 : 4);
+    if (precision == DNQ_F32) return (size_t)(n + 1) * 4 * (kx <= 2 ? 2 : kx <= 4 ? 4 : 8);
+    return (size_t)(n + 1) * 8 * (kx <= 2 ? 2 : 4);
 }
 
 // out[2j] = x_j.Hx_j, out[2j+1] = x_j.x_j (device), eloc[r][j] = y/x.

@@ -3,13 +3,13 @@
 // the local-energy / Rayleigh-quotient reductions.
 //
 // FP64 operator: y_i = sum_k H_ik x_k with FP64 values, FP64 x.
-// FP32 operator: off-diagonal values and x stored in FP32; products and sums
-// are kept exact to second order with TwoProduct (fmaf residual) and TwoSum
-// (Knuth) per lane, the per-lane (sum, error) pairs are combined with TwoSum
-// across the row group, and the FP64 diagonal term diag_i * x_i is added in
-// FP64 (Ogita, Rump, Oishi, "Accurate sum and dot product", SIAM J. Sci.
-// Comput. 26 (2005), Dot2).
-// Reductions x.Hx and x.x use the same Dot2 scheme in FP64.
+// FP32 operator: off-diagonal values and x stored in FP32; each lane sums
+// its products with Kahan's compensated summation, every product entering
+// through one fused multiply-add (AccF32 in spmv.cuh), the per-lane
+// (sum, compensation) pairs are combined with TwoSum across the row group,
+// and the FP64 diagonal term diag_i * x_i is added in FP64.
+// Reductions x.Hx and x.x use Dot2 in FP64 (Ogita, Rump, Oishi, "Accurate
+// sum and dot product", SIAM J. Sci. Comput. 26 (2005)).
 #include <cub/cub.cuh>
 
 #include "ham.cuh"
@@ -28,8 +28,8 @@ namespace {
 // (results are identical for every U).  The last entries of the arrays are
 // read with scalar loads.
 //   T = double: y_r = sum H_rk x_k                         (val, x)
-//   T = float : y_r = Dot2 sum of val32 * x32 + diag_r x_r (FP32 off-diagonal
-//               values, FP64 diagonal term)
+//   T = float : y_r = Kahan sum of val32 * x32 + diag_r x_r (FP32
+//               off-diagonal values, FP64 diagonal term)
 template <int G, int U, class T, class Acc>
 __device__ __forceinline__ Acc row_acc(const i64* __restrict__ rp, const u32* __restrict__ col,
                                        const T* __restrict__ val, const T* __restrict__ xg,

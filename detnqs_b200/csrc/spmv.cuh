@@ -1,7 +1,8 @@
 // spmv.cuh -- device pieces shared by the H.psi kernels (spmv.cu, spmm.cu):
-// compensated FP32 / FP64 accumulators (Ogita, Rump, Oishi, "Accurate sum
-// and dot product", SIAM J. Sci. Comput. 26 (2005): Dot2 = TwoProduct with
-// an fma residual + Knuth's TwoSum) and streaming 128-bit loads of the CSR.
+// the row accumulators (FP64 fused multiply-adds; FP32 Kahan summation),
+// Dot2 for the FP64 energy sums (Ogita, Rump, Oishi, "Accurate sum and dot
+// product", SIAM J. Sci. Comput. 26 (2005): TwoProduct with an fma
+// residual + Knuth's TwoSum) and streaming 128-bit loads of the CSR.
 #pragma once
 
 #include "ham.cuh"
@@ -70,22 +71,58 @@ __device__ __forceinline__ Dot2<T> shfl_xor(const Dot2<T>& d, int o, unsigned ma
 }
 
 // Row accumulators: FP64 plain fused multiply-add, FP32 Dot2.
+// reduce(G) combines the G lanes of a row group by a butterfly: at offset
+// o = G/2, ..., 1 every lane merges with lane ^ o.  A merge is symmetric
+// (a + b == b + a, and TwoSum's error term is exact whatever the order), so
+// both lanes of a pair hold the same value after each step.  shfl(o) and
+// merge(x) are the two halves of one step, for callers that exchange only
+// part of their accumulators.
 struct AccF64 {
     double s = 0.0;
     __device__ __forceinline__ void add_prod(double v, double x) { s = fma(v, x, s); }
     __device__ __forceinline__ void reduce(int G) {
         for (int o = G / 2; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     }
+    __device__ __forceinline__ AccF64 shfl(int o) const {
+        AccF64 r;
+        r.s = __shfl_xor_sync(0xffffffffu, s, o);
+        return r;
+    }
+    __device__ __forceinline__ void merge(const AccF64& x) { s += x.s; }
     __device__ __forceinline__ double value() const { return s; }
 };
 
+// FP32 accumulator: Kahan's compensated summation of the products, each
+// product entering through one fused multiply-add, y = v*x - c, with a
+// single rounding (Kahan, "Further remarks on reducing truncation errors",
+// CACM 8 (1965); the product needs no separate rounding).  (s, c) hold the
+// sum as s - c.  Lanes merge their pairs with TwoSum: s1 + s2 = s + e
+// exactly, so the merged pair is (s, (c1 + c2) - e), symmetric in its two
+// arguments.
 struct AccF32 {
-    Dot2<float> d;
-    __device__ __forceinline__ void add_prod(float v, float x) { d.add_prod(v, x); }
-    __device__ __forceinline__ void reduce(int G) {
-        for (int o = G / 2; o; o >>= 1) d.merge(shfl_xor(d, o, 0xffffffffu));
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add_prod(float v, float x) {
+        const float y = fmaf(v, x, -c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
     }
-    __device__ __forceinline__ double value() const { return (double)d.s + (double)d.c; }
+    __device__ __forceinline__ void merge(const AccF32& o) {
+        float s2, e;
+        two_sum(s, o.s, s2, e);
+        s = s2;
+        c = __fsub_rn(__fadd_rn(c, o.c), e);
+    }
+    __device__ __forceinline__ AccF32 shfl(int o) const {
+        AccF32 r;
+        r.s = __shfl_xor_sync(0xffffffffu, s, o);
+        r.c = __shfl_xor_sync(0xffffffffu, c, o);
+        return r;
+    }
+    __device__ __forceinline__ void reduce(int G) {
+        for (int o = G / 2; o; o >>= 1) merge(shfl(o));
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
 // Four consecutive values from a 16-byte aligned position, streamed past L1

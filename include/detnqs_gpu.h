@@ -203,8 +203,8 @@ int dnq_ham_p_diag(dnq_ham_t h, dnq_ctx_t ctx, double* out, void* stream);
  * Replaces the SciPy CSR matvec of detnqs/operator/kernel.py:75-78
  * (build_vv_operator) with y = H_VV x on the device.  precision DNQ_F64
  * computes in FP64; DNQ_F32 reads FP32 off-diagonal values and FP32 x with
- * two-sum compensated FP32 accumulation, adds the FP64 diagonal term in FP64
- * and writes FP64 y. */
+ * Kahan-compensated FP32 accumulation (each product through one fused
+ * multiply-add), adds the FP64 diagonal term in FP64 and writes FP64 y. */
 int dnq_ham_spmv(dnq_ham_t h, const double* x, double* y, int precision,
                  void* stream);
 /* Proxy operator (kernel.py:127-139):
