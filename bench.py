@@ -605,6 +605,17 @@ def run_batched(args, rank: int, world: int):
             _, ms = bt.apply(psi_dev, precision=prec, graph=True, stream=sp, eloc=eloc_dev)
             ts.append(ms)
         t_apply[key] = float(np.mean(ts))
+    # several amplitude sets per system in one pass (8 FP32 sets per sector)
+    Xk = torch.stack([psi_dev] + [torch.roll(psi_dev, 17 * j) for j in range(1, 8)], 1)
+    bt.apply_multi(Xk, precision=native.F32)
+    ts = []
+    for _ in range(max(args.steps, 5)):
+        flush.zero_()
+        barrier()
+        _, ms = bt.apply_multi(Xk, precision=native.F32)
+        ts.append(ms)
+    t_multi = float(np.mean(ts))
+    del Xk
     clocks = clk.stop()
     ms_step = max_over_ranks(float(np.mean(t_step)), world, dev)
     e64b, _ = bt.step(psi_dev, precision=native.F64, stream=sp)
@@ -724,8 +735,10 @@ def run_batched(args, rank: int, world: int):
         "plain_fp64": {"step_ms": ms_plain, "hpsi_ms": t_plain_hpsi,
                        "what": "one system at a time: dnq_build + FP64 local energy; H.psi "
                                "alone on the resident blocks"},
+        "hpsi_multi_8sets_ms": t_multi,
         "speedup_vs_plain_fp64": {"step": ms_plain / ms_step,
-                                  "hpsi": t_plain_hpsi / t_apply["f32"]},
+                                  "hpsi": t_plain_hpsi / t_apply["f32"],
+                                  "hpsi_per_set_8sets": 8 * t_plain_hpsi / t_multi},
         "dE_fp32_vs_fp64_Ha": dE32,
         "dE_batched_fp64_vs_plain_Ha": dE64,
         "roofline": roof_build if build_ms >= phase["hpsi"] else roof_hpsi,

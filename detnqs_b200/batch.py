@@ -81,6 +81,25 @@ class Batch:
         """H.psi and energies on the resident H_VV blocks (no rebuild)."""
         return self._run(N.lib.dnq_batch_apply, psi, precision, graph, stream, eloc)
 
+    def apply_multi(self, X, *, precision: int = N.F32, stream=None, eloc=None):
+        """k amplitude sets per system in one pass over the resident blocks:
+        X is total x k (C order, numpy or CUDA tensor; column j = the
+        concatenated psi_j).  Returns (energies[n_sys, k, 2], device ms);
+        column j equals apply(X[:, j]) bit for bit."""
+        if hasattr(X, "data_ptr"):
+            import torch
+            Xp = X.to(torch.float64).contiguous()
+        else:
+            Xp = np.ascontiguousarray(X, np.float64)
+        if Xp.ndim != 2 or Xp.shape[0] != self.total:
+            raise ValueError("X must be total x k")
+        k = int(Xp.shape[1])
+        e2 = np.zeros((self.n_sys, k, 2))
+        ms = C.c_double()
+        N.check(N.lib.dnq_batch_apply_multi(self._h, N.ptr(Xp), N.ptr(eloc), e2.ctypes.data, k,
+                                            int(precision), stream, C.byref(ms)))
+        return e2, ms.value
+
     def _run(self, fn, psi, precision, graph, stream, eloc):
         p = psi if hasattr(psi, "data_ptr") else np.ascontiguousarray(psi, np.float64)
         e2 = np.zeros((self.n_sys, 2))

@@ -305,33 +305,37 @@ constexpr int kEnergyBlocks = 592;   // the single-vector reduction's grid
 
 }  // namespace
 
-// Y (n x ldy) = H_VV X (n x ldx) for kx <= 8 (FP32) or <= 4 (FP64) columns;
-// X, Y device memory.  scratch: interleaved copy of X.
-void spmm_vv(dnq_ham_s* h, const double* X, int ldx, int kx, double* Y, int ldy, int precision,
-             void* scratch, cudaStream_t s) {
-    const Csr& m = h->vv;
+// Y (nr x ldy) = M X (nc x ldx) for kx <= 8 (FP32) or <= 4 (FP64) columns
+// of a square CSR; X, Y device memory.  FP32 uses val32 (off-diagonal
+// values) and the FP64 diagonal diag32.  G = 0 picks the lanes per row as
+// the single-vector kernel does (same option, same rule), so columns match
+// it bit for bit.  scratch: interleaved copy of X (spmm_scratch_bytes).
+void spmm_csr(const Csr& m, const float* val32, const double* diag32, const double* X, int ldx,
+              int kx, double* Y, int ldy, int precision, int G, int U, void* scratch,
+              int dev, cudaStream_t s) {
     if (m.nr == 0) return;
-    int G, U;
-    spmv_shape(m, G, U);
-    const int dev = h->device;
+    if (G == 0) {
+        int u = 0;
+        spmv_shape(m, G, u);
+        if (U == 0) U = u;
+    }
+    if (U == 0) U = 1;
     const unsigned gi = (unsigned)std::max<i64>(1, std::min<i64>(4096, (m.nr * 8 + 255) / 256));
     if (precision == DNQ_F32) {
         float* Xg = static_cast<float*>(scratch);
         const int K = kx <= 2 ? 2 : kx <= 4 ? 4 : 8;
-        const float* val = m.val32.p;
-        const double* diag = h->diag_op.p;
         if (K == 2) {
             k_interleave<2, float><<<gi, 256, 0, s>>>(X, ldx, kx, m.nr, Xg);
             DNQ_CHECK_LAUNCH();
-            spmm_g<2, float, AccF32>(G, U, m, val, Xg, diag, X, ldx, kx, Y, ldy, dev, s);
+            spmm_g<2, float, AccF32>(G, U, m, val32, Xg, diag32, X, ldx, kx, Y, ldy, dev, s);
         } else if (K == 4) {
             k_interleave<4, float><<<gi, 256, 0, s>>>(X, ldx, kx, m.nr, Xg);
             DNQ_CHECK_LAUNCH();
-            spmm_g<4, float, AccF32>(G, U, m, val, Xg, diag, X, ldx, kx, Y, ldy, dev, s);
+            spmm_g<4, float, AccF32>(G, U, m, val32, Xg, diag32, X, ldx, kx, Y, ldy, dev, s);
         } else {
             k_interleave<8, float><<<gi, 256, 0, s>>>(X, ldx, kx, m.nr, Xg);
             DNQ_CHECK_LAUNCH();
-            spmm_g<8, float, AccF32>(G, U, m, val, Xg, diag, X, ldx, kx, Y, ldy, dev, s);
+            spmm_g<8, float, AccF32>(G, U, m, val32, Xg, diag32, X, ldx, kx, Y, ldy, dev, s);
         }
     } else {
         double* Xg = static_cast<double*>(scratch);
@@ -345,6 +349,13 @@ void spmm_vv(dnq_ham_s* h, const double* X, int ldx, int kx, double* Y, int ldy,
             spmm_g<4, double, AccF64>(G, U, m, m.val.p, Xg, nullptr, X, ldx, kx, Y, ldy, dev, s);
         }
     }
+}
+
+// The V block of a handle (FP32: its prepared split).
+void spmm_vv(dnq_ham_s* h, const double* X, int ldx, int kx, double* Y, int ldy, int precision,
+             void* scratch, cudaStream_t s) {
+    spmm_csr(h->vv, h->vv.val32.p, h->diag_op.p, X, ldx, kx, Y, ldy, precision, 0, 0, scratch,
+             h->device, s);
 }
 
 // Bytes of the interleaved scratch for kx columns (n rows and a zero row).

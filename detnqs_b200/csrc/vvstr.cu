@@ -1746,6 +1746,10 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
 namespace dnq {
 
 void launch_f32_split(const Csr& m, float* val32, double* diag_out, cudaStream_t s);
+void spmm_csr(const Csr& m, const float* val32, const double* diag32, const double* X, int ldx,
+              int kx, double* Y, int ldy, int precision, int G, int U, void* scratch,
+              int dev, cudaStream_t s);
+size_t spmm_scratch_bytes(i64 n, int kx, int precision);
 void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
                   cudaStream_t s, const float* x32, const float* val32, const double* diag,
                   int G, int device, int U);
@@ -1818,6 +1822,42 @@ __global__ void k_energy_sys(const i64* row_off, const double* x, const double* 
         }
         e2[2 * sy] = a.s + a.c;
         e2[2 * sy + 1] = c.s + c.c;
+    }
+}
+
+// Same sums for column j = blockIdx.y of row-major X / Y (k columns): the
+// block of (system, column) runs k_energy_sys's order on that column, so
+// each column's energies equal a single-column apply bit for bit.
+// e2[(sy * k + j) * 2 + {0, 1}].
+__global__ void k_energy_sys_multi(const i64* row_off, const double* X, const double* Y,
+                                   int k, double* eloc, double* e2) {
+    const int sy = blockIdx.x, j = blockIdx.y;
+    const i64 b = row_off[sy], e = row_off[sy + 1];
+    DDb num, den;
+    for (i64 t = b + threadIdx.x; t < e; t += blockDim.x) {
+        const double xv = X[t * k + j], yv = Y[t * k + j];
+        num.add_prod(xv, yv);
+        den.add_prod(xv, xv);
+        if (eloc) eloc[t * k + j] = yv / xv;
+    }
+    for (int o = 16; o; o >>= 1) {
+        num.merge(__shfl_xor_sync(0xffffffffu, num.s, o), __shfl_xor_sync(0xffffffffu, num.c, o));
+        den.merge(__shfl_xor_sync(0xffffffffu, den.s, o), __shfl_xor_sync(0xffffffffu, den.c, o));
+    }
+    __shared__ double sh[4][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sh[0][w] = num.s; sh[1][w] = num.c; sh[2][w] = den.s; sh[3][w] = den.c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DDb a, c;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            a.merge(sh[0][q], sh[1][q]);
+            c.merge(sh[2][q], sh[3][q]);
+        }
+        e2[((i64)sy * k + j) * 2] = a.s + a.c;
+        e2[((i64)sy * k + j) * 2 + 1] = c.s + c.c;
     }
 }
 
@@ -2285,6 +2325,57 @@ int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc, double* energ
 int dnq_batch_apply(dnq_batch_t b, const double* psi, double* eloc, double* energies,
                     int precision, int use_graph, void* stream, double* step_ms) {
     return batch_run(b, 1, psi, eloc, energies, precision, use_graph, stream, step_ms);
+}
+
+// k amplitude sets per system in one pass over the resident CSR: X and
+// eloc are total x k row-major, energies n_sys x k x 2.
+int dnq_batch_apply_multi(dnq_batch_t b, const double* X, double* eloc, double* energies, int k,
+                          int precision, void* stream, double* step_ms) {
+    DNQ_API_BEGIN
+    require(b && X, DNQ_ERR_INVALID, "null argument");
+    require(k >= 1 && k <= 1024, DNQ_ERR_INVALID, "k must be in [1, 1024]");
+    require(precision == DNQ_F64 || precision == DNQ_F32, DNQ_ERR_INVALID, "invalid precision");
+    DeviceGuard g(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const i64 n = b->total;
+    if (precision == DNQ_F32 && !b->f32_ready) {
+        launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);
+        b->f32_ready = true;
+    }
+    DIn<double> xd(X, (size_t)n * k, s);
+    DBuf<double> yd((size_t)n * k, s), e2((size_t)b->n_sys * k * 2, s);
+    const bool dev_eloc = eloc && is_device_ptr(eloc);
+    if (dev_eloc) require_on_device(eloc, b->device, "eloc");
+    DBuf<double> ebuf;
+    double* ed = nullptr;
+    if (eloc) {
+        if (dev_eloc) ed = eloc;
+        else { ebuf.alloc((size_t)n * k, s); ed = ebuf.p; }
+    }
+    const int step = precision == DNQ_F32 ? 8 : 4;
+    DBuf<unsigned char> scratch(spmm_scratch_bytes(n, std::min(k, step), precision), s);
+    cudaEvent_t e0, e1;
+    DNQ_CUDA(cudaEventCreate(&e0));
+    DNQ_CUDA(cudaEventCreate(&e1));
+    DNQ_CUDA(cudaEventRecord(e0, s));
+    for (int j0 = 0; j0 < k; j0 += step) {
+        const int kx = std::min(step, k - j0);
+        spmm_csr(b->M, b->val32.p, b->diag_op.p, xd.p + j0, k, kx, yd.p + j0, k, precision,
+                 b->spmv_group, b->spmv_unroll, scratch.p, b->device, s);
+    }
+    k_energy_sys_multi<<<dim3((unsigned)b->n_sys, (unsigned)k), 256, 0, s>>>(
+        b->row_off.p, xd.p, yd.p, k, ed, e2.p);
+    DNQ_CHECK_LAUNCH();
+    DNQ_CUDA(cudaEventRecord(e1, s));
+    if (eloc && !dev_eloc) copy_out(eloc, ed, (size_t)n * k, s);
+    copy_out(energies, e2.p, (size_t)b->n_sys * k * 2, s);
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (step_ms) *step_ms = ms;
+    DNQ_API_END
 }
 
 // Sorted COO of one system's block, local indices (reference format).

@@ -354,6 +354,15 @@ int dnq_batch_step(dnq_batch_t b, const double* psi, double* eloc,
 int dnq_batch_apply(dnq_batch_t b, const double* psi, double* eloc,
                     double* energies, int precision, int use_graph, void* stream,
                     double* step_ms);
+/* k amplitude sets of every system in one pass over the resident CSR
+ * (dnq_ham_spmv_multi on the block-diagonal batch): X and eloc are
+ * total x k row-major (eloc may be NULL), energies n_sys x k x 2 =
+ * {psi_j.H psi_j, psi_j.psi_j}; each column equals dnq_batch_apply of that
+ * column bit for bit.  Eager (no graph); *step_ms = device time of the
+ * H.psi and energy kernels. */
+int dnq_batch_apply_multi(dnq_batch_t b, const double* X, double* eloc,
+                          double* energies, int k, int precision, void* stream,
+                          double* step_ms);
 /* Device ms of the phases of the last eager (use_graph = 0) step:
  * {diagonal, build (arena + long rows), scan + compaction (+ FP32 split),
  *  H.psi + energies}. */

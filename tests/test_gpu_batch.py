@@ -189,3 +189,24 @@ def test_mixed_width_batch_matches_single_builds_and_oracle(mixed_workload, port
         assert abs(e[k, 0] / e[k, 1] - num / den) < 1e-12
         H.close()
     bt.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_apply_multi_equals_apply_per_column(workload, prec):
+    """Several amplitude sets per system in one pass: every column's
+    energies and local energies equal a single-set apply bit for bit."""
+    from detnqs_b200 import batch as B
+    from detnqs_b200 import native as N
+    P = N.F64 if prec == "f64" else N.F32
+    w, ctxs = workload
+    bt = B.Batch(ctxs, [x.dets for x in w], [x.sysm.n_orb for x in w], eps1=1e-7)
+    k = 6
+    X = np.random.default_rng(12).normal(size=(bt.total, k))
+    eloc = np.empty((bt.total, k))
+    e, _ = bt.apply_multi(X, precision=P, eloc=eloc)
+    for j in range(k):
+        el = np.empty(bt.total)
+        ej, _ = bt.apply(X[:, j].copy(), precision=P, eloc=el)
+        np.testing.assert_array_equal(e[:, j, :].view(np.uint64), ej.view(np.uint64))
+        np.testing.assert_array_equal(eloc[:, j].view(np.uint64), el.view(np.uint64))
+    bt.close()
