@@ -363,7 +363,7 @@ def run_ours(args, rank: int, world: int):
     # ---- steady state of the inner loop: repeated H.psi on the resident H
     ss = {}
     for prec, key in ((native.F64, "f64"), (native.F32, "f32")):
-        for _ in range(2):   # FP32 values and their panel layout prepared outside timing
+        for _ in range(2):   # FP32 values prepared outside timing
             last.local_energy(psi_dev, eloc=eloc, precision=prec)
         reps = 20
         torch.cuda.synchronize()
@@ -1529,6 +1529,67 @@ def run_reference(args, rank: int, world: int):
     }
 
 
+# The default single-GPU run also measures the other workloads briefly, each
+# in its own process (3 timed steps after 2 warm-up steps, 3 s of CPU
+# baseline; the serving stream three times for its tail), and reports them
+# under "extras" beside the headline numbers.
+EXTRAS = (("batched", 1), ("serving", 3), ("downfold", 1), ("slogdet", 1), ("det_batch", 1))
+
+
+def _extra_summary(w: str, runs: list) -> dict:
+    def pick(d, *keys):
+        return {k: d.get(k) for k in keys if k in d}
+    ok = [d for d in runs if "error" not in d]
+    out = {"wall_s": [round(d.get("_wall_s", 0.0), 1) for d in runs]}
+    if not ok:
+        out["error"] = runs[-1].get("error") if runs else "not run"
+        return out
+    d = ok[-1]
+    out.update(pick(d, "metric", "value", "unit", "ms_per_step", "ms_steps", "dtype",
+                    "dE_fp32_vs_fp64_Ha", "gpu_launches", "clocks"))
+    out["config"] = {"workload": d.get("config", {}).get("workload")}
+    if "cpu_baseline" in d:
+        out["cpu_baseline"] = d["cpu_baseline"]
+    if "e2e" in d:
+        out["e2e"] = d["e2e"]
+    if w == "batched":
+        out.update(pick(d, "plain_fp64", "speedup_vs_plain_fp64", "hpsi_ms",
+                        "hpsi_multi_8sets_ms", "phase_ms_eager", "build_speedup_vs_cpu"))
+    elif w == "serving":
+        out["repeats"] = [{"p50_ms": r["latency_ms"]["p50"], "p99_ms": r["latency_ms"]["p99"],
+                           "plain_p50_ms": r["plain_fp64"]["latency_ms"]["p50"],
+                           "plain_p99_ms": r["plain_fp64"]["latency_ms"]["p99"],
+                           "requests_per_s": r["throughput"]["requests_per_s"]} for r in ok]
+        out["p99_ms_median"] = float(np.median([r["latency_ms"]["p99"] for r in ok]))
+        out["plain_p99_ms_median"] = float(np.median(
+            [r["plain_fp64"]["latency_ms"]["p99"] for r in ok]))
+    elif w == "downfold":
+        out.update(pick(d, "heff_ms", "build_ms", "phase_ms"))
+    return out
+
+
+def run_extras(args) -> dict:
+    import subprocess
+    out = {}
+    for w, reps in EXTRAS:
+        runs = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            try:
+                p = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", w,
+                                    "--steps", "3", "--warmup", "2", "--cpu-seconds", "3"],
+                                   capture_output=True, text=True, timeout=args.extras_timeout)
+                lines = [x for x in p.stdout.strip().splitlines() if x.startswith("{")]
+                d = json.loads(lines[-1]) if lines else {
+                    "error": f"rc={p.returncode}: {p.stderr.strip()[-300:]}"}
+            except Exception as e:   # an extra never takes the headline line down
+                d = {"error": f"{type(e).__name__}: {e}"[:300]}
+            d["_wall_s"] = time.perf_counter() - t0
+            runs.append(d)
+        out[w] = _extra_summary(w, runs)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1542,6 +1603,10 @@ def main():
                     help="size of S for --workload downfold (a smaller S for profiling)")
     ap.add_argument("--serve-slots", type=int, default=2,
                     help="build worker streams of the served path")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the short runs of the other workloads (default single-GPU "
+                         "run only)")
+    ap.add_argument("--extras-timeout", type=float, default=600.0)
     ap.add_argument("--workload", choices=["single", "batched", "serving", "downfold",
                                            "det_batch", "slogdet"],
                     default="single",
@@ -1569,6 +1634,8 @@ def main():
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
+        if args.workload == "single" and world == 1 and not args.no_extras:
+            res["extras"] = run_extras(args)
         print(json.dumps(res), flush=True)
 
 

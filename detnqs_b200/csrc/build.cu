@@ -12,14 +12,13 @@
 //   6. per-row sort by column; for discovered P: radix sort of the 128-bit
 //      keys, run-length unique (lexicographic (alpha, beta) order of
 //      finalize_vp_deferred, build_ham.cpp:346-380) and column relabelling.
-#include <cub/cub.cuh>
-#include <cuda/std/tuple>
 
 #include <cmath>
 #include <memory>
 
 #include "gen.cuh"
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 
@@ -191,13 +190,6 @@ k_build(BuildParams P) {
     }
 }
 
-struct Key2 {
-    __host__ __device__ ::cuda::std::tuple<unsigned long long&, unsigned long long&>
-    operator()(ulonglong2& k) const {
-        return {k.x, k.y};
-    }
-};
-
 __global__ void k_unique_flags(const ulonglong2* k, i64 n, u32* flag) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x)
@@ -217,10 +209,18 @@ __global__ void k_unique_scatter(const ulonglong2* k, const u32* perm, const u32
     }
 }
 
-__global__ void k_iota(u32* p, i64 n) {
+// (alpha, beta) <-> alpha << n_orb | beta, for n_orb <= 32.
+__global__ void k_pack_keys(const ulonglong2* k, i64 n, int n_orb, u64* out) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x)
-        p[t] = (u32)t;
+        out[t] = (k[t].x << n_orb) | k[t].y;
+}
+
+__global__ void k_unpack_keys(const u64* p, i64 n, int n_orb, ulonglong2* out) {
+    const u64 lo = n_orb >= 64 ? ~0ull : ((1ull << n_orb) - 1);
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        out[t] = make_ulonglong2(p[t] >> n_orb, p[t] & lo);
 }
 
 // FP32 copy of every value (streaming, 2 values per thread step).
@@ -272,10 +272,7 @@ inline int grid_for(i64 n, int threads = 256) {
 
 template <class T>
 void exclusive_scan(const T* in, i64* out, i64 n, cudaStream_t s) {
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+    prim::scan<T, i64, false>(in, out, n, s);
 }
 
 i64 read_i64(const i64* d, cudaStream_t s) {
@@ -291,88 +288,14 @@ void ensure_sorted(Csr& m, cudaStream_t s) {
     if (!m.sorted) sort_rows(m, s);
 }
 
-namespace {
-__global__ void k_max_rowlen(const i64* rowptr, i64 nr, unsigned long long* out) {
-    unsigned long long m = 0;
-    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < nr;
-         r += (i64)gridDim.x * blockDim.x)
-        m = max(m, (unsigned long long)(rowptr[r + 1] - rowptr[r]));
-    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
-}
-
-// (row << 32 | col) of every entry; the row by binary search of rowptr.
-__global__ void k_row_col_keys(const i64* rowptr, i64 nr, const u32* col, i64 nnz, u64* key,
-                               u32* idx) {
-    for (i64 k = blockIdx.x * (i64)blockDim.x + threadIdx.x; k < nnz;
-         k += (i64)gridDim.x * blockDim.x) {
-        i64 lo = 0, hi = nr;
-        while (hi - lo > 1) {
-            const i64 mid = (lo + hi) >> 1;
-            if (rowptr[mid] <= k) lo = mid; else hi = mid;
-        }
-        key[k] = ((u64)lo << 32) | col[k];
-        idx[k] = (u32)k;
-    }
-}
-
-__global__ void k_gather_sorted(const u64* skey, const u32* perm, const double* val, i64 n,
-                                u32* col, double* oval) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
-         t += (i64)gridDim.x * blockDim.x) {
-        col[t] = (u32)(skey[t] & 0xffffffffull);
-        oval[t] = val[perm[t]];
-    }
-}
-}  // namespace
 
 void sort_rows(Csr& m, cudaStream_t s) {
     m.sorted = true;
     m.val32.release();   // an FP32 copy follows the old order: rebuilt on next use
     if (m.nnz == 0 || m.nr == 0) return;
-    require(m.nnz < (i64)0x7fffffff, DNQ_ERR_OVERFLOW,
-            "block has more than 2^31-1 entries for the segmented sort");
     DBuf<u32> col2(m.nnz, s);
     DBuf<double> val2(m.nnz, s);
-    {   // a row longer than 65536 entries would occupy one block of the
-        // segmented sort: sort all entries by (row, column) instead
-        DBuf<unsigned long long> mx(1, s);
-        DNQ_CUDA(cudaMemsetAsync(mx.p, 0, 8, s));
-        k_max_rowlen<<<grid_for(m.nr), 256, 0, s>>>(m.rowptr.p, m.nr, mx.p);
-        DNQ_CHECK_LAUNCH();
-        unsigned long long longest = 0;
-        DNQ_CUDA(cudaMemcpyAsync(&longest, mx.p, 8, cudaMemcpyDeviceToHost, s));
-        DNQ_CUDA(cudaStreamSynchronize(s));
-        if (longest > (1ull << 16)) {
-            DBuf<u64> key(m.nnz, s), skey(m.nnz, s);
-            DBuf<u32> idx(m.nnz, s), perm(m.nnz, s);
-            k_row_col_keys<<<grid_for(m.nnz), 256, 0, s>>>(m.rowptr.p, m.nr, m.col.p, m.nnz,
-                                                          key.p, idx.p);
-            DNQ_CHECK_LAUNCH();
-            int hb = 33;
-            while (hb < 64 && ((u64)1 << (hb - 32)) <= (u64)m.nr) ++hb;
-            size_t tmp = 0;
-            DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, skey.p, idx.p, perm.p,
-                                                     m.nnz, 0, hb, s));
-            DBuf<u8> tb(tmp, s);
-            DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, key.p, skey.p, idx.p, perm.p,
-                                                     m.nnz, 0, hb, s));
-            k_gather_sorted<<<grid_for(m.nnz), 256, 0, s>>>(skey.p, perm.p, m.val.p, m.nnz,
-                                                           col2.p, val2.p);
-            DNQ_CHECK_LAUNCH();
-            m.col = std::move(col2);
-            m.val = std::move(val2);
-            return;
-        }
-    }
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp, m.col.p, col2.p, m.val.p,
-                                                 val2.p, (int)m.nnz, (int)m.nr,
-                                                 m.rowptr.p, m.rowptr.p + 1, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceSegmentedSort::SortPairs(tb.p, tmp, m.col.p, col2.p, m.val.p,
-                                                 val2.p, (int)m.nnz, (int)m.nr,
-                                                 m.rowptr.p, m.rowptr.p + 1, s));
+    prim::sort_row_columns(m.rowptr.p, m.nr, m.col.p, m.val.p, col2.p, val2.p, s);
     m.col = std::move(col2);
     m.val = std::move(val2);
 }
@@ -468,7 +391,6 @@ extern i64 g_arena_cap;
 extern int g_partc_groupwalk;
 extern int g_build_f32;
 void spmv_set_option(int lanes, int unroll);
-void spmv_set_panels(int mode);
 
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
@@ -615,19 +537,26 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
         T.fill(H->t_ms);
         return;
     }
-    // P discovery: sort keys with their positions, unique, relabel.
+    // P discovery: sort the keys with their positions (stable), unique,
+    // relabel.  The sort visits the n_orb bits of each spin string only; for
+    // n_orb <= 32 both strings are packed into one word, alpha above beta,
+    // which keeps the (alpha, beta) order.
     require(nvp < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "H_VP has more than 2^32 entries");
     DBuf<ulonglong2> ks(nvp, s);
-    DBuf<u32> perm(nvp, s), perm2(nvp, s);
+    DBuf<u32> perm2(nvp, s);
     if (nvp) {
-        k_iota<<<grid_for(nvp), 256, 0, s>>>(perm.p, nvp);
-        DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, vp_key.p, ks.p, perm.p, perm2.p,
-                                                 (i64)nvp, Key2{}, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, vp_key.p, ks.p, perm.p, perm2.p,
-                                                 (i64)nvp, Key2{}, s));
+        if (2 * n_orb <= 64) {
+            DBuf<u64> pk(nvp, s), pks(nvp, s);
+            k_pack_keys<<<grid_for(nvp), 256, 0, s>>>(vp_key.p, nvp, n_orb, pk.p);
+            DNQ_CHECK_LAUNCH();
+            const int bits[1] = {2 * n_orb};
+            prim::radix_sort<u64, u32>(pk.p, pks.p, nullptr, perm2.p, nvp, bits, s);
+            k_unpack_keys<<<grid_for(nvp), 256, 0, s>>>(pks.p, nvp, n_orb, ks.p);
+            DNQ_CHECK_LAUNCH();
+        } else {
+            const int bits[2] = {n_orb, n_orb};
+            prim::radix_sort<ulonglong2, u32>(vp_key.p, ks.p, nullptr, perm2.p, nvp, bits, s);
+        }
     }
     vp_key.release();
     DBuf<u32> flag(nvp, s), runid(nvp, s);
@@ -635,10 +564,7 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
     if (nvp) {
         k_unique_flags<<<grid_for(nvp), 256, 0, s>>>(ks.p, nvp, flag.p);
         DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, flag.p, runid.p, nvp, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb.p, tmp, flag.p, runid.p, nvp, s));
+        prim::scan_inclusive<u32, u32>(flag.p, runid.p, nvp, s);
         u32 last = 0;
         DNQ_CUDA(cudaMemcpyAsync(&last, runid.p + nvp - 1, 4, cudaMemcpyDeviceToHost, s));
         DNQ_CUDA(cudaStreamSynchronize(s));
@@ -846,9 +772,7 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
 
 int dnq_set_option(int option, int64_t value) {
     DNQ_API_BEGIN
-    require(option >= 1 && option <= 8, DNQ_ERR_INVALID, "unknown option");
-    if (option == 6)
-        require(value <= 2, DNQ_ERR_INVALID, "panel mode must be 0, 1 or 2");
+    require(option >= 1 && option <= 8 && option != 6, DNQ_ERR_INVALID, "unknown option");
     require(value >= 0, DNQ_ERR_INVALID, "option value must be >= 0");
     if (option == 4)
         require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
@@ -861,7 +785,6 @@ int dnq_set_option(int option, int64_t value) {
     if (option == 3) g_arena_cap = value;
     if (option == 4) spmv_set_option((int)value, -1);
     if (option == 5) spmv_set_option(-1, (int)value);
-    if (option == 6) spmv_set_panels((int)value);
     if (option == 7) g_partc_groupwalk = value != 0;
     if (option == 8) g_build_f32 = value != 0;
     DNQ_API_END

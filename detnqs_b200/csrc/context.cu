@@ -1,6 +1,4 @@
 // context.cu -- integral context: upload, derived tables, signed pair table.
-#include <cub/cub.cuh>
-
 #include <atomic>
 #include <cmath>
 #include <memory>
@@ -9,6 +7,7 @@
 #include <sstream>
 
 #include "context.cuh"
+#include "prim.cuh"
 #include "refsort.cuh"
 
 namespace dnq {
@@ -197,6 +196,19 @@ __global__ void k_table_ties(const double* eri, int nso, double thr, const i64* 
     }
 }
 
+// Sort keys of the table: (row, ~|v| bits), one block per row.
+__global__ void k_table_keys(const i64* off, const u64* k, ulonglong2* out) {
+    const i64 row = blockIdx.x;
+    for (i64 t = off[row] + threadIdx.x; t < off[row + 1]; t += blockDim.x)
+        out[t] = make_ulonglong2((u64)row, ~k[t]);
+}
+
+__global__ void k_table_keys_back(const ulonglong2* k, i64 n, u64* out) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        out[t] = ~k[t].y;
+}
+
 __global__ void k_table_unpack(const u64* keys, const u32* vals, i64 n, u16* ab,
                                double* v) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
@@ -224,10 +236,7 @@ void build_pair_table(dnq_ctx_s* c, double thr) {
         DNQ_CHECK_LAUNCH();
     }
     T.off.alloc(nrows + 1, s);
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, counts.p, T.off.p, nrows + 1, s));
-    DBuf<u8> tbuf(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tbuf.p, tmp, counts.p, T.off.p, nrows + 1, s));
+    prim::scan<i64, i64, false>(counts.p, T.off.p, nrows + 1, s);
     i64 total = 0;
     DNQ_CUDA(cudaMemcpyAsync(&total, T.off.p + nrows, sizeof(i64), cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
@@ -239,15 +248,19 @@ void build_pair_table(dnq_ctx_s* c, double thr) {
     DBuf<u32> v0(total, s), v1(total, s);
     k_table_fill<<<(unsigned)nrows, 256, 0, s>>>(c->erid.p, nso, thr, T.off.p, k0.p, v0.p);
     DNQ_CHECK_LAUNCH();
-    // Stable descending sort of each row by weight.
-    size_t tmp2 = 0;
-    DNQ_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
-        nullptr, tmp2, k0.p, k1.p, v0.p, v1.p, (int)total, (int)nrows, T.off.p,
-        T.off.p + 1, 0, 64, s));
-    DBuf<u8> tbuf2(tmp2, s);
-    DNQ_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
-        tbuf2.p, tmp2, k0.p, k1.p, v0.p, v1.p, (int)total, (int)nrows, T.off.p,
-        T.off.p + 1, 0, 64, s));
+    // Stable descending sort of each row by weight: one ascending radix sort
+    // of (row, ~weight bits) over the whole table.
+    {
+        DBuf<ulonglong2> kk(total, s), ks(total, s);
+        k_table_keys<<<(unsigned)nrows, 256, 0, s>>>(T.off.p, k0.p, kk.p);
+        DNQ_CHECK_LAUNCH();
+        int rb = 1;
+        while (rb < 63 && ((i64)1 << rb) < nrows) ++rb;
+        const int bits[2] = {rb, 64};
+        prim::radix_sort<ulonglong2, u32>(kk.p, ks.p, v0.p, v1.p, total, bits, s);
+        k_table_keys_back<<<1024, 256, 0, s>>>(ks.p, total, k1.p);
+        DNQ_CHECK_LAUNCH();
+    }
     k_table_unpack<<<1024, 256, 0, s>>>(k1.p, v1.p, total, T.ab.p, T.v.p);
     DNQ_CHECK_LAUNCH();
     // Tied weights in the reference's order; k1/v1 serve as the scratch.

@@ -1,7 +1,6 @@
 // detmap.cu -- construction of the device determinant map.
-#include <cub/cub.cuh>
-
 #include "detmap.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 namespace {
@@ -161,10 +160,7 @@ void build_detmap(DetMap& m, const u64* dets, i64 n, bool strict, cudaStream_t s
             k_map_first<<<blocks, threads, 0, s>>>(dets, n, m.keys.p, m.idx.p, m.mask,
                                                     full_alpha, first.p);
             DNQ_CHECK_LAUNCH();
-            size_t tmp = 0;
-            DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, first.p, rank_out->p, n, s));
-            DBuf<u8> tb(tmp, s);
-            DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, first.p, rank_out->p, n, s));
+            prim::scan<u32, u32, false>(first.p, rank_out->p, n, s);
         }
         return;
     }
@@ -174,10 +170,7 @@ void build_detmap(DetMap& m, const u64* dets, i64 n, bool strict, cudaStream_t s
     k_map_first<<<blocks, threads, 0, s>>>(dets, n, m.keys.p, m.idx.p, m.mask, full_alpha,
                                             first.p);
     DNQ_CHECK_LAUNCH();
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, first.p, rank.p, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, first.p, rank.p, n, s));
+    prim::scan<u32, u32, false>(first.p, rank.p, n, s);
     if (rank_out) {
         rank_out->alloc(n, s);
         k_map_rank<<<blocks, threads, 0, s>>>(dets, n, m.keys.p, m.idx.p, m.mask, full_alpha,

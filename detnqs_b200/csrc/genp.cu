@@ -7,13 +7,11 @@
 // All use count/fill passes of one warp per bra row (exact output sizes),
 // 128-bit radix sort + run-length unique for determinant sets, and hash
 // lookups in the device map of V for exclusion.
-#include <cub/cub.cuh>
-#include <cuda/std/tuple>
-
 #include <memory>
 
 #include "gen.cuh"
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 
@@ -26,13 +24,6 @@ namespace {
 
 constexpr int kW = 8;
 
-struct Key2D {
-    __host__ __device__ ::cuda::std::tuple<unsigned long long&, unsigned long long&>
-    operator()(ulonglong2& k) const {
-        return {k.x, k.y};
-    }
-};
-
 int gsz(i64 n) {
     i64 b = (n + 255) / 256;
     return (int)(b < 1 ? 1 : (b > 65535 ? 65535 : b));
@@ -40,10 +31,7 @@ int gsz(i64 n) {
 
 template <class T>
 void scan_ex(const T* in, i64* out, i64 n, cudaStream_t s) {
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+    prim::scan<T, i64, false>(in, out, n, s);
 }
 
 i64 rd(const i64* d, cudaStream_t s) {
@@ -236,14 +224,12 @@ __global__ void k_compact_keys(const ulonglong2* k, const u32* f, const i64* pos
 
 // Sort keys, keep one of each: the sorted unique set (canonicalize,
 // det_space.cpp:97-101) written to H->dets_p.
-void sort_unique(DBuf<ulonglong2>& keys, i64 n, cudaStream_t s, dnq_ham_s* H) {
+void sort_unique(DBuf<ulonglong2>& keys, i64 n, int n_orb, cudaStream_t s, dnq_ham_s* H) {
     H->n_p = 0;
     if (n == 0) return;
     DBuf<ulonglong2> sorted(n, s);
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, keys.p, sorted.p, n, Key2D{}, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceRadixSort::SortKeys(tb.p, tmp, keys.p, sorted.p, n, Key2D{}, s));
+    const int bits[2] = {n_orb, n_orb};
+    prim::radix_sort<ulonglong2, u32>(keys.p, sorted.p, nullptr, nullptr, n, bits, s);
     keys.release();
     DBuf<u32> f(n, s);
     DBuf<i64> pos(n + 1, s);
@@ -569,7 +555,7 @@ void gen_dets(dnq_ctx_s* ctx, const u64* Vd, i64 n, int n_orb, const double* psi
         DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
         k_comb<true><<<grid, kW * 32, 0, s>>>(P);
         DNQ_CHECK_LAUNCH();
-        sort_unique(keys, tot, s, H);
+        sort_unique(keys, tot, n_orb, s, H);
     } else {
         DIn<double> ps(psi, mode == 2 ? n : 0, s);
         ScrParams P{};
@@ -596,7 +582,7 @@ void gen_dets(dnq_ctx_s* ctx, const u64* Vd, i64 n, int n_orb, const double* psi
         DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
         k_screened<true><<<grid, kW * 32, 0, s>>>(P);
         DNQ_CHECK_LAUNCH();
-        sort_unique(keys, tot, s, H);
+        sort_unique(keys, tot, n_orb, s, H);
     }
     DNQ_CUDA(cudaStreamSynchronize(s));
 }
@@ -710,12 +696,10 @@ void pt2(dnq_ctx_s* ctx, const u64* Vd, i64 n, const double* cd, int n_orb, doub
     out3[1] = 0.0;
     out3[2] = 0.0;
     if (tot == 0) return;
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, ks.p, vals.p, vs.p, tot,
-                                             Key2D{}, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, keys.p, ks.p, vals.p, vs.p, tot,
-                                             Key2D{}, s));
+    {
+        const int bits[2] = {n_orb, n_orb};
+        prim::radix_sort<ulonglong2, double>(keys.p, ks.p, vals.p, vs.p, tot, bits, s);
+    }
     DBuf<unsigned long long> nu(1, s);
     DNQ_CUDA(cudaMemsetAsync(nu.p, 0, 8, s));
     DBuf<double> part2(2 * (i64)nb * 8, s);

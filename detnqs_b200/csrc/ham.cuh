@@ -22,24 +22,6 @@ struct Csr {
     }
 };
 
-// Column-panel layout of a square FP32 operator block (panel.cu).
-struct Panels {
-    i64 nr = 0, nc = 0, nnz = 0, npanels = 0, nslices = 0, nent = 0, nchunks = 0;
-    int grid = 0;              // CTAs the slice split was made for
-    bool ready = false;
-    DBuf<u16> col;             // per slot: column offset in the panel (k-major in a slice)
-    DBuf<float> val;           // per slot: FP32 value (0 in padding slots)
-    DBuf<i64> soff;            // per slice: first slot
-    DBuf<u32> swidth;          // per slice: entries of its longest chunk
-    DBuf<u32> schunk;          // per slice and lane: its chunk's place in row order (~0u: none)
-    DBuf<u32> split;           // per panel: slice range of each CTA (grid + 1 bounds)
-    DBuf<i64> rptr;            // per row: first of its chunks in row order
-    DBuf<float> part;          // per chunk, in row order: Dot2 partial (2 floats)
-    size_t bytes() const {
-        return col.bytes() + val.bytes() + soff.bytes() + swidth.bytes() + schunk.bytes() +
-               split.bytes() + rptr.bytes() + part.bytes();
-    }
-};
 
 }  // namespace dnq
 
@@ -48,8 +30,6 @@ struct dnq_ham_s {
     cudaStream_t stream = nullptr;
     dnq::i64 n_v = 0, n_p = 0;
     int words = 1;                    // uint64 words per spin string of V and P
-    dnq::Panels pan;                  // panel layout of the FP32 V block (repeated H.psi)
-    int f32_uses = 0;                 // FP32 H.psi calls so far
     dnq::Csr vv, vp;
     dnq::Csr pv;                      // transpose of vp, built on first use
     bool pv_ready = false;
@@ -64,7 +44,7 @@ struct dnq_ham_s {
     double t_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     size_t bytes() const {
         return vv.bytes() + vp.bytes() + pv.bytes() + diag.bytes() + diag_op.bytes() + x32.bytes() +
-               dets_p.bytes() + pan.bytes();
+               dets_p.bytes();
     }
 };
 
@@ -85,10 +65,6 @@ struct SpmvDesc {
     double* y;
     i64 nr, nnz;
 };
-// Panel layout of a square block from its FP32 values; y = M x with it.
-void build_panels(const Csr& m, const float* val32, Panels& P, cudaStream_t s);
-void spmv_panels(const Panels& P, const float* x32, const double* diag, const double* x,
-                 double* y, int device, cudaStream_t s);
 // Lanes per row and slots per lane the H.psi kernels use for m.
 void spmv_shape(const Csr& m, int& G, int& U);
 // One launch over nd descriptors (device array) sharing (G, U, precision).

@@ -20,12 +20,12 @@
 //   4. The H_VV row is added, entries with |v| <= 1e-15 dropped
 //      (csr_add, ham_utils.cpp:330-442), and the row is compacted in column
 //      order from the bitmap.
-#include <cub/cub.cuh>
 
 #include <memory>
 #include <vector>
 
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 
@@ -569,10 +569,13 @@ int gs(i64 n) {
 
 template <class T>
 void scan_excl(const T* in, i64* out, i64 n, cudaStream_t s) {
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+    prim::scan<T, i64, false>(in, out, n, s);
+}
+
+inline int bits_for(i64 n) {   // bits of the largest index below n
+    int b = 1;
+    while (b < 63 && ((i64)1 << b) < n) ++b;
+    return b;
 }
 
 // COO (device) -> canonical CSR (sorted, duplicates summed in input order,
@@ -600,16 +603,13 @@ void coo_to_csr_dev(const u32* r, const u32* c, const double* v, i64 n, i64 nr, 
     DNQ_CUDA(cudaMemcpyAsync(&hb, bad.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
     require(hb == 0, DNQ_ERR_RANGE, "coo_to_csr: row index out of bounds");
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, skey.p, idx.p, perm.p, n, 0, 64, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, key.p, skey.p, idx.p, perm.p, n, 0, 64, s));
+    {   // (row << 32 | col): stable, so duplicates keep their input order
+        const int bits[1] = {32 + bits_for(nr)};
+        prim::radix_sort<u64, u32>(key.p, skey.p, idx.p, perm.p, n, bits, s);
+    }
     k_run_flags<<<gs(n), 256, 0, s>>>(skey.p, n, flag.p);
     DNQ_CHECK_LAUNCH();
-    size_t tmp2 = 0;
-    DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp2, flag.p, runid.p, n, s));
-    DBuf<u8> tb2(tmp2, s);
-    DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb2.p, tmp2, flag.p, runid.p, n, s));
+    prim::scan_inclusive<u32, u32>(flag.p, runid.p, n, s);
     u32 nruns = 0;
     DNQ_CUDA(cudaMemcpyAsync(&nruns, runid.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
@@ -620,12 +620,7 @@ void coo_to_csr_dev(const u32* r, const u32* c, const double* v, i64 n, i64 nr, 
     k_nonzero<<<gs(nruns), 256, 0, s>>>(rsum.p, nruns, keep.p);
     DNQ_CHECK_LAUNCH();
     DBuf<u32> pos32(nruns, s);
-    {   // positions fit in u32 (n < 2^32)
-        size_t t3 = 0;
-        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t3, keep.p, pos32.p, (i64)nruns, s));
-        DBuf<u8> tb3(t3, s);
-        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb3.p, t3, keep.p, pos32.p, (i64)nruns, s));
-    }
+    prim::scan<u32, u32, false>(keep.p, pos32.p, (i64)nruns, s);   // n < 2^32
     u32 lastpos = 0, lastkeep = 0;
     DNQ_CUDA(cudaMemcpyAsync(&lastpos, pos32.p + nruns - 1, 4, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaMemcpyAsync(&lastkeep, keep.p + nruns - 1, 4, cudaMemcpyDeviceToHost, s));
@@ -664,12 +659,11 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             k_cap_terms<<<gs(VP.nnz), 256, 0, s>>>(VP.col.p, VP.nnz, PV.rowptr.p, skip.p, len.p);
             DNQ_CHECK_LAUNCH();
         }
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceSegmentedReduce::Sum(nullptr, tmp, len.p, rsum.p, (int)nv,
-                                                 VP.rowptr.p, VP.rowptr.p + 1, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceSegmentedReduce::Sum(tb.p, tmp, len.p, rsum.p, (int)nv, VP.rowptr.p,
-                                                 VP.rowptr.p + 1, s));
+        if (nv) {
+            prim::k_segment_sums<i64, i64><<<gs(nv * 32), 256, 0, s>>>(len.p, VP.rowptr.p, nv,
+                                                                      rsum.p);
+            DNQ_CHECK_LAUNCH();
+        }
         k_cap_finish<<<gs(nv), 256, 0, s>>>(rsum.p, VV.rowptr.p, nv, cap.p);
         DNQ_CHECK_LAUNCH();
     }
@@ -758,16 +752,9 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             DNQ_CHECK_LAUNCH();
             // kept k's whose column holds other rows, in order
             DBuf<u32> idx(m, s), sel(m, s);
-            DBuf<i64> nsel(1, s);
             k_iota_u32<<<gs(m), 256, 0, s>>>(idx.p, m, t0);
             DNQ_CHECK_LAUNCH();
-            size_t tmp = 0;
-            DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, idx.p, multi.p, sel.p, nsel.p, m, s));
-            DBuf<u8> tb(tmp, s);
-            DNQ_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, idx.p, multi.p, sel.p, nsel.p, m, s));
-            i64 ns = 0;
-            DNQ_CUDA(cudaMemcpyAsync(&ns, nsel.p, 8, cudaMemcpyDeviceToHost, s));
-            DNQ_CUDA(cudaStreamSynchronize(s));
+            const i64 ns = prim::select_flagged<u32, u8>(idx.p, multi.p, sel.p, m, s);
             // expand (j, term), stable sort by j, ordered sum per j
             i64 ne = 0;
             DBuf<u32> ecnt(ns + 1, s);
@@ -782,7 +769,7 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             DNQ_CUDA(cudaStreamSynchronize(s));
             require(ne < (i64)0xffffffffll, DNQ_ERR_OVERFLOW, "long-row expansion exceeds 2^32");
             DBuf<u32> ekey(std::max<i64>(1, ne), s), skey(std::max<i64>(1, ne), s);
-            DBuf<u32> eperm(std::max<i64>(1, ne), s), sperm(std::max<i64>(1, ne), s);
+            DBuf<u32> sperm(std::max<i64>(1, ne), s);
             DBuf<double> eterm;
             DBuf<float2> eterm2;
             if (precision == DNQ_F32) eterm2.alloc(std::max<i64>(1, ne), s);
@@ -795,27 +782,17 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
                                                   precision == DNQ_F32, ekey.p, eterm.p,
                                                   eterm2.p);
                 DNQ_CHECK_LAUNCH();
-                k_iota_u32<<<gs(ne), 256, 0, s>>>(eperm.p, ne, 0);
-                DNQ_CHECK_LAUNCH();
-                size_t t2 = 0;
-                DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, ekey.p, skey.p, eperm.p,
-                                                         sperm.p, ne, 0, 32, s));
-                DBuf<u8> tb2(t2, s);
-                DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb2.p, t2, ekey.p, skey.p, eperm.p,
-                                                         sperm.p, ne, 0, 32, s));
+                {   // stable by j: a run keeps its terms in k order
+                    const int bits[1] = {bits_for(nv)};
+                    prim::radix_sort<u32, u32>(ekey.p, skey.p, nullptr, sperm.p, ne, bits, s);
+                }
                 DBuf<u32> head(ne, s), hpos(ne, s);
-                DBuf<i64> nh(1, s);
                 k_run_heads<<<gs(ne), 256, 0, s>>>(skey.p, ne, head.p);
                 DNQ_CHECK_LAUNCH();
                 DBuf<u32> pos(ne, s);
                 k_iota_u32<<<gs(ne), 256, 0, s>>>(pos.p, ne, 0);
                 DNQ_CHECK_LAUNCH();
-                size_t t3 = 0;
-                DNQ_CUDA(cub::DeviceSelect::Flagged(nullptr, t3, pos.p, head.p, hpos.p, nh.p, ne, s));
-                DBuf<u8> tb3(t3, s);
-                DNQ_CUDA(cub::DeviceSelect::Flagged(tb3.p, t3, pos.p, head.p, hpos.p, nh.p, ne, s));
-                DNQ_CUDA(cudaMemcpyAsync(&nruns, nh.p, 8, cudaMemcpyDeviceToHost, s));
-                DNQ_CUDA(cudaStreamSynchronize(s));
+                nruns = prim::select_flagged<u32, u32>(pos.p, head.p, hpos.p, ne, s);
                 DBuf<u32> oj(nruns, s);
                 DBuf<double> ov;
                 DBuf<float2> ov2;

@@ -6,7 +6,6 @@
 // per lane with Dot2 (TwoProduct + TwoSum) and merged across the warp, and
 // the row energies are summed with Dot2 again, so the result carries about
 // twice FP64 precision before the final rounding.
-#include <cub/cub.cuh>
 
 #include "gen.cuh"
 

@@ -20,10 +20,6 @@
 //   * n_V <= kNoAllocMaxDets (larger handles are rejected, nothing is run);
 //   * precision DNQ_F32 needs the handle's FP32 values to exist already
 //     (one earlier dnq_ham_spmv / dnq_ham_local_energy call with DNQ_F32);
-//     this entry point always sums with the CSR kernel, so where the
-//     column-panel option (DNQ_OPT_SPMV_PANELS) makes the allocating FP32
-//     path use panels, the two agree to compensated FP32 precision rather
-//     than bit for bit;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
 //     before any stream capture.  The address is cached per device ordinal

@@ -2,11 +2,11 @@
 //   yv = H_VV xv + H_VP xp
 //   yp = H_PV xv + diag(H_PP) xp
 // H_PV is the transpose of H_VP, built once per handle on first use.
-#include <cub/cub.cuh>
 
 #include <memory>
 
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 
@@ -29,12 +29,6 @@ __global__ void k_rows_of(const i64* rowptr, i64 nr, i64 nnz, u32* rows) {
         }
         rows[k] = (u32)lo;
     }
-}
-
-__global__ void k_iota32(u32* p, i64 n) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
-         t += (i64)gridDim.x * blockDim.x)
-        p[t] = (u32)t;
 }
 
 __global__ void k_gather_t(const u32* perm, const u32* rows, const double* val, i64 n,
@@ -84,17 +78,15 @@ void transpose_csr(const Csr& a, Csr& t, cudaStream_t s) {
         DNQ_CUDA(cudaMemsetAsync(t.rowptr.p, 0, (t.nr + 1) * sizeof(i64), s));
         return;
     }
-    DBuf<u32> rows(a.nnz, s), perm(a.nnz, s), perm2(a.nnz, s), skey(a.nnz, s);
+    DBuf<u32> rows(a.nnz, s), perm2(a.nnz, s), skey(a.nnz, s);
     k_rows_of<<<gsz(a.nnz), 256, 0, s>>>(a.rowptr.p, a.nr, a.nnz, rows.p);
     DNQ_CHECK_LAUNCH();
-    k_iota32<<<gsz(a.nnz), 256, 0, s>>>(perm.p, a.nnz);
-    DNQ_CHECK_LAUNCH();
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, a.col.p, skey.p, perm.p, perm2.p,
-                                             a.nnz, 0, 32, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, a.col.p, skey.p, perm.p, perm2.p,
-                                             a.nnz, 0, 32, s));
+    {   // stable by column: rows stay ascending inside each column
+        int b = 1;
+        while (b < 32 && ((i64)1 << b) < a.nc) ++b;
+        const int bits[1] = {b};
+        prim::radix_sort<u32, u32>(a.col.p, skey.p, nullptr, perm2.p, a.nnz, bits, s);
+    }
     k_gather_t<<<gsz(a.nnz), 256, 0, s>>>(perm2.p, rows.p, a.val.p, a.nnz, t.col.p, t.val.p);
     DNQ_CHECK_LAUNCH();
     k_bounds<<<gsz(t.nr + 1), 256, 0, s>>>(skey.p, a.nnz, t.nr, t.rowptr.p);
@@ -152,10 +144,7 @@ void symmetrize_csr(Csr& a, Csr& out, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     out.nr = out.nc = n;
     out.rowptr.alloc(n + 1, s);
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt.p, out.rowptr.p, n + 1, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, cnt.p, out.rowptr.p, n + 1, s));
+    prim::scan<u32, i64, false>(cnt.p, out.rowptr.p, n + 1, s);
     DNQ_CUDA(cudaMemcpyAsync(&out.nnz, out.rowptr.p + n, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
     out.col.alloc(out.nnz, s);

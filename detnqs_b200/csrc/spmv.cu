@@ -10,7 +10,6 @@
 // and the FP64 diagonal term diag_i * x_i is added in FP64.
 // Reductions x.Hx and x.x use Dot2 in FP64 (Ogita, Rump, Oishi, "Accurate
 // sum and dot product", SIAM J. Sci. Comput. 26 (2005)).
-#include <cub/cub.cuh>
 
 #include "ham.cuh"
 #include "spmv.cuh"
@@ -248,14 +247,6 @@ void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, i
 
 }  // namespace
 
-// When the FP32 V block gets its panel layout: 0 never (default), 1 from
-// its second FP32 H.psi, 2 from the first.  The layout is correct but, on
-// the heat-bath spaces measured, slower than the CSR kernel: rows of very
-// different lengths share each block's barriers (see panel.cu).
-int g_spmv_panels = 0;
-
-void spmv_set_panels(int mode) { g_spmv_panels = mode; }
-
 void spmv_set_option(int lanes, int unroll) {
     if (lanes >= 0) g_spmv_lanes = lanes;
     if (unroll >= 0) g_spmv_unroll = unroll;
@@ -378,24 +369,14 @@ void ensure_f32_all(Csr& m, cudaStream_t s) {
 
 // Prepare the FP32 operator buffers of the V block.
 void ensure_f32(dnq_ham_s* h, cudaStream_t s) {
-    bool fresh = false;
-    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v) {
+    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
         make_f32(h->vv, s, &h->diag_op);
-        h->pan.ready = false;
-        fresh = true;
-    }
     if ((i64)h->x32.n < h->n_v) h->x32.alloc(h->n_v, s);
-    ++h->f32_uses;
-    const bool want = g_spmv_panels == 2 || (g_spmv_panels == 1 && h->f32_uses >= 2);
-    if (want && (!h->pan.ready || fresh) && h->vv.nr == h->vv.nc)
-        build_panels(h->vv, h->vv.val32.p, h->pan, s);
-    if (!want) h->pan.ready = false;
 }
 
-// FP32 V-block operator of a handle: the panel layout when present.
+// FP32 V-block operator of a handle.
 void spmv_vv_f32(dnq_ham_s* h, const double* x, double* y, cudaStream_t s) {
-    if (h->pan.ready) spmv_panels(h->pan, h->x32.p, h->diag_op.p, x, y, h->device, s);
-    else spmv_block(h, h->vv, x, y, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
+    spmv_block(h, h->vv, x, y, nullptr, DNQ_F32, s, h->x32.p, h->diag_op.p);
 }
 
 }  // namespace dnq

@@ -27,8 +27,6 @@
 // k_vv_big / k_vv_eval_long / k_vv_compact_long handle rows longer than a
 // chunk, and k_vv_compact gathers the CSR.  k_vv_twopass is the exact
 // fallback when the arena runs out.
-#include <cub/cub.cuh>
-#include <cuda/std/tuple>
 
 #include <algorithm>
 #include <type_traits>
@@ -37,6 +35,7 @@
 
 #include "gen.cuh"
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 
@@ -86,13 +85,6 @@ struct StrIndex {
     u32 pres_words = 0;
     u32 pres_min = 0xffffffffu;
     StrMapView view() const { return StrMapView{slots.p, mask}; }
-};
-
-struct SwapKey {
-    __host__ __device__ ::cuda::std::tuple<unsigned long long&, unsigned long long&>
-    operator()(ulonglong2& k) const {
-        return {k.x, k.y};
-    }
 };
 
 __global__ void k_keys_by(const u64* V, i64 n, int major, ulonglong2* k, u32* id) {
@@ -204,12 +196,8 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cud
         X.other32.alloc(n, s);
         k_keys_by64<<<gsz(n), 256, 0, s>>>(V, n, major, k64.p, id.p);
         DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k64.p, ks64.p, id.p, X.idx.p, n,
-                                                 0, 32 + n_orb, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k64.p, ks64.p, id.p, X.idx.p, n, 0,
-                                                 32 + n_orb, s));
+        const int bits[1] = {32 + n_orb};
+        prim::radix_sort<u64, u32>(k64.p, ks64.p, id.p, X.idx.p, n, bits, s);
         k_split_sorted64<<<gsz(n), 256, 0, s>>>(ks64.p, n, X.other.p, X.other32.p, head.p);
         DNQ_CHECK_LAUNCH();
     } else {
@@ -217,12 +205,8 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cud
         ks.alloc(n, s);
         k_keys_by<<<gsz(n), 256, 0, s>>>(V, n, major, k.p, id.p);
         DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k.p, ks.p, id.p, X.idx.p, n,
-                                                 SwapKey{}, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k.p, ks.p, id.p, X.idx.p, n,
-                                                 SwapKey{}, s));
+        const int bits[2] = {n_orb, n_orb};
+        prim::radix_sort<ulonglong2, u32>(k.p, ks.p, id.p, X.idx.p, n, bits, s);
         k_split_sorted<<<gsz(n), 256, 0, s>>>(ks.p, n, X.other.p, head.p);
         DNQ_CHECK_LAUNCH();
     }
@@ -230,12 +214,7 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cud
     X.gstart.alloc(n, s);
     DBuf<u32>& gid = X.gid;
     DBuf<u32>& gstart = X.gstart;
-    {
-        size_t t2 = 0;
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t2, head.p, gid.p, n, s));
-        DBuf<u8> tb2(t2, s);
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb2.p, t2, head.p, gid.p, n, s));
-    }
+    prim::scan_inclusive<unsigned, u32>(head.p, gid.p, n, s);
     u32 last_gid = 0;
     DNQ_CUDA(cudaMemcpyAsync(&last_gid, gid.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
@@ -351,10 +330,7 @@ void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
     DBuf<u32> flag(A.ngroups, s), rank(A.ngroups, s);
     k_long_groups<<<gsz(A.ngroups), 256, 0, s>>>(A.gstart.p, A.ngroups, n, thr, flag.p, nullptr);
     DNQ_CHECK_LAUNCH();
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, flag.p, rank.p, A.ngroups, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, flag.p, rank.p, A.ngroups, s));
+    prim::scan<u32, u32, false>(flag.p, rank.p, A.ngroups, s);
     A.prow.alloc(A.ngroups, s);
     k_prow<<<gsz(A.ngroups), 256, 0, s>>>(flag.p, rank.p, A.ngroups, A.prow.p);
     DNQ_CHECK_LAUNCH();
@@ -1475,10 +1451,7 @@ void launch_diag(const dnq_ctx_s* c, const u64* d, i64 n, double* out, cudaStrea
 namespace {
 template <class T>
 void excl_scan(const T* in, i64* out, i64 n, cudaStream_t s) {
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+    prim::scan<T, i64, false>(in, out, n, s);
 }
 }  // namespace
 
@@ -1875,14 +1848,6 @@ __global__ void k_sanitize(i64* rowptr, i64 n, i64 cap, const int* overflow, int
     for (i64 t = threadIdx.x; t <= n; t += blockDim.x) rowptr[t] = 0;
 }
 
-template <class T>
-void scan_plan(const T* in, i64* out, i64 n, cudaStream_t s, DBuf<u8>& tmp) {
-    size_t bytes = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
-    if (tmp.n < bytes) tmp.alloc(bytes, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, bytes, in, out, n, s));
-}
-
 }  // namespace
 }  // namespace dnq
 
@@ -2002,9 +1967,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->x32.alloc(n, s);
     b->e2.alloc(2 * b->n_sys, s);
     {   // scan temporary sized once
-        size_t bytes = 0;
-        DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, b->rlen.p, b->M.rowptr.p, n + 1, s));
-        b->scan_tmp.alloc(bytes, s);
+        b->scan_tmp.alloc(prim::scan_tmp_bytes<i64>(n + 1), s);
     }
     DNQ_CUDA(cudaStreamSynchronize(s));
     b->planned = true;
@@ -2075,9 +2038,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     k_vv_eval_long<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     mark(2);
-    size_t bytes = b->scan_tmp.n;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(b->scan_tmp.p, bytes, b->rlen.p, b->M.rowptr.p,
-                                           n + 1, s));
+    prim::scan<u32, i64, false>(b->rlen.p, b->M.rowptr.p, n + 1, s, b->scan_tmp.p);
     k_sanitize<<<1, 1024, 0, s>>>(b->M.rowptr.p, n, b->M.nnz, b->ovf.p, b->bad.p);
     DNQ_CHECK_LAUNCH();
     // FP32 steps write the FP32 operator copy in the same pass

@@ -17,14 +17,13 @@
 // P keys, run-length unique, column relabelling; per-row sort of H_VP.  The
 // result is an ordinary dnq_ham_t (words = 2), so H.psi, the proxy operator,
 // downfolding and copies work on it unchanged.
-#include <cub/cub.cuh>
-#include <cuda/std/tuple>
 
 #include <memory>
 #include <vector>
 
 #include "context.cuh"
 #include "ham.cuh"
+#include "prim.cuh"
 
 namespace dnq {
 void keep_pool(int device);
@@ -276,12 +275,20 @@ struct alignas(32) Key4 {
     u64 w[4];   // alpha lo, alpha hi, beta lo, beta hi
 };
 
+}  // namespace
+namespace prim {
+namespace {
 // Most significant first: alpha hi, alpha lo, beta hi, beta lo.
-struct Key4Order {
-    __host__ __device__ ::cuda::std::tuple<u64&, u64&, u64&, u64&> operator()(Key4& k) const {
-        return {k.w[1], k.w[0], k.w[3], k.w[2]};
+template <>
+struct RadixKey<Key4> {
+    static constexpr int W = 4;
+    __device__ __forceinline__ static u64 word(const Key4& k, int i) {
+        return k.w[i == 0 ? 1 : i == 1 ? 0 : i == 2 ? 3 : 2];
     }
 };
+}  // namespace
+}  // namespace prim
+namespace {
 
 struct WParams {
     CtxView C;
@@ -519,12 +526,6 @@ __global__ void k_row_starts(const i64* uoff, const u32* first_unit, i64 n, i64*
         rowptr[r] = uoff[first_unit[r]];
 }
 
-__global__ void k_iota4(u32* p, i64 n) {
-    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
-         t += (i64)gridDim.x * blockDim.x)
-        p[t] = (u32)t;
-}
-
 __device__ __forceinline__ bool neq_prev(const Key4* k, i64 t) {
     return t == 0 || k[t].w[0] != k[t - 1].w[0] || k[t].w[1] != k[t - 1].w[1] ||
            k[t].w[2] != k[t - 1].w[2] || k[t].w[3] != k[t - 1].w[3];
@@ -554,10 +555,7 @@ int blocks(i64 n) {
 
 template <class T>
 void exscan(const T* in, i64* out, i64 n, cudaStream_t s) {
-    size_t tmp = 0;
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, s));
-    DBuf<u8> tb(tmp, s);
-    DNQ_CUDA(cub::DeviceScan::ExclusiveSum(tb.p, tmp, in, out, n, s));
+    prim::scan<T, i64, false>(in, out, n, s);
 }
 
 i64 fetch(const i64* d, cudaStream_t s) {
@@ -715,28 +713,19 @@ void wide_build(dnq_ctx_s* ctx, const u64* V_in, i64 n, const double* psi_in, in
 
     // P: 256-bit radix sort with positions, unique, relabel
     DBuf<Key4> ks(nvp, s);
-    DBuf<u32> perm(nvp, s), perm2(nvp, s);
+    DBuf<u32> perm2(nvp, s);
     if (nvp) {
-        k_iota4<<<blocks(nvp), 256, 0, s>>>(perm.p, nvp);
-        DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, ks.p, perm.p, perm2.p,
-                                                 (i64)nvp, Key4Order{}, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, keys.p, ks.p, perm.p, perm2.p,
-                                                 (i64)nvp, Key4Order{}, s));
+        const int hi = n_orb > 64 ? n_orb - 64 : 0, lo = n_orb > 64 ? 64 : n_orb;
+        const int bits[4] = {hi, lo, hi, lo};
+        prim::radix_sort<Key4, u32>(keys.p, ks.p, nullptr, perm2.p, nvp, bits, s);
     }
     keys.release();
-    perm.release();
     i64 np = 0;
     DBuf<u32> flag(nvp, s), runid(nvp, s);
     if (nvp) {
         k_key4_flags<<<blocks(nvp), 256, 0, s>>>(ks.p, nvp, flag.p);
         DNQ_CHECK_LAUNCH();
-        size_t tmp = 0;
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, flag.p, runid.p, nvp, s));
-        DBuf<u8> tb(tmp, s);
-        DNQ_CUDA(cub::DeviceScan::InclusiveSum(tb.p, tmp, flag.p, runid.p, nvp, s));
+        prim::scan_inclusive<u32, u32>(flag.p, runid.p, nvp, s);
         u32 last = 0;
         DNQ_CUDA(cudaMemcpyAsync(&last, runid.p + nvp - 1, 4, cudaMemcpyDeviceToHost, s));
         DNQ_CUDA(cudaStreamSynchronize(s));

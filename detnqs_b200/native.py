@@ -37,7 +37,6 @@ OPT_ARENA_CHUNK = 2
 OPT_ARENA_CAP = 3
 OPT_SPMV_LANES = 4
 OPT_SPMV_UNROLL = 5
-OPT_SPMV_PANELS = 6
 OPT_PARTC_GROUPWALK = 7
 OPT_BUILD_F32 = 8
 NEED_K, NEED_PHASE, NEED_HP, NEED_HP_POS = 1, 2, 4, 8
@@ -60,7 +59,7 @@ EXPORTS = (
     "dnq_ham_local_energy_multi",
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
-    "dnq_batch_apply_multi",
+    "dnq_batch_apply_multi", "dnq_sort_order",
     "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
     "dnq_server_wait", "dnq_server_set_budget", "dnq_server_pause", "dnq_server_stats",
     "dnq_ctx_create_wide", "dnq_wide_diag", "dnq_wide_build", "dnq_ham_symmetrize",
@@ -146,6 +145,7 @@ _sig("dnq_batch_get_config", _P, _P)
 _sig("dnq_batch_step", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
 _sig("dnq_batch_apply", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
 _sig("dnq_batch_apply_multi", _P, _P, _P, _P, _I, _I, _P, C.POINTER(_D))
+_sig("dnq_sort_order", _P, _I64, _I, _P, _P, _I, _P)
 _sig("dnq_batch_timings", _P, _P)
 _sig("dnq_batch_copy_coo", _P, _I, _P, _P, _P, C.POINTER(_I64))
 _sig("dnq_server_create", _I, _I64, _I, _I, C.POINTER(_P))

@@ -65,6 +65,15 @@ int dnq_version(void);
  * reference counterpart (instrumentation). */
 int64_t dnq_launch_count(void);
 
+/* Stable ascending order of n keys by the radix sort the build uses for
+ * determinant sets (no reference counterpart; exposed so that its order can
+ * be checked).  words = 1: uint64 keys; words = 2: (alpha, beta) pairs,
+ * alpha first.  bits[w] = significant low bits of word w (higher bits must
+ * be zero).  order[i] = input position of the i-th key in sorted order.
+ * keys and order may be host or device memory. */
+int dnq_sort_order(const uint64_t* keys, int64_t n, int words, const int* bits,
+                   uint32_t* order, int device, void* stream);
+
 /* ---- integral context ------------------------------------------------------
  * Replaces IntCtx(fcidump_path, num_orb) (bridge.cpp:108-128, :242-248) and
  * IntegralMO (csrc/detnqs/integral/integral_mo.hpp:58-120).  Arrays are in
@@ -160,9 +169,6 @@ int dnq_ham_destroy(dnq_ham_t h);
  *   DNQ_OPT_SPMV_UNROLL n: 4-entry slots each lane keeps in flight, 0/1/2/4
  *                          (0 = by the average row length).  Results do
  *                          not depend on it;
- *   DNQ_OPT_SPMV_PANELS n: column-panel layout of the FP32 V block (x staged
- *                          in shared memory): 0 never (default), 1 from a
- *                          handle's second FP32 H.psi, 2 from the first;
  *   DNQ_OPT_PARTC_GROUPWALK n: 1 walks the short alpha-single groups of
  *                          the string-group matcher's opposite-spin doubles
  *                          one group at a time, 0 packed across the groups of
@@ -175,7 +181,7 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          0 makes them on first FP32 use (default).  The
  *                          copies are the same either way. */
 enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
-       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, DNQ_OPT_SPMV_PANELS = 6,
+       DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, /* 6: unused */
        DNQ_OPT_PARTC_GROUPWALK = 7, DNQ_OPT_BUILD_F32 = 8 };
 int dnq_set_option(int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
@@ -249,9 +255,7 @@ int dnq_ham_local_energy_multi(dnq_ham_t h, const double* X, double* eloc,
  * first receives H x and then y_i / x_i).  out2 may be device memory of that
  * GPU (the call then only enqueues work on the stream) or host memory (the
  * call copies the pair back and waits for the stream).  DNQ_F32 needs the
- * handle's FP32 values to exist (one earlier FP32 call); the sums always use
- * the CSR kernel, so with DNQ_OPT_SPMV_PANELS on they match the allocating
- * FP32 path to compensated precision, not bit for bit.  The first call on a
+ * handle's FP32 values to exist (one earlier FP32 call).  The first call on a
  * device sets up the scratch address with that device current: make it
  * before any stream capture; the address is cached per device ordinal and
  * does not survive cudaDeviceReset.  All calls share the scratch: calls

@@ -533,39 +533,3 @@ def test_spmv_every_lane_and_slot_count(core):
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 0))
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, 0))
     H.close()
-
-
-def test_fp32_panel_layout_matches_csr_and_scipy(core):
-    """The column-panel FP32 operator (x staged in shared memory, rows in
-    slices of 32 by their entry count in a panel) over several panels:
-    same results as the CSR FP32 kernel to compensated precision (panels sum
-    with Dot2, the CSR kernel with Kahan: both within a few 1e-9 of each
-    other), FP64 SciPy to FP32-value precision, and the same bits on every
-    call."""
-    from detnqs_b200 import device as D
-    from detnqs_b200 import native as N
-    sysm = S.make_system(30, 12, 12, 60, 1001)
-    V = S.heat_bath_sample(sysm, 110000, 7)         # 3 panels of 49152 columns
-    ctx = core.IntCtx.from_arrays(30, sysm.h1e, sysm.eri, sysm.e_core)
-    ctx.hb_prepare(1e-15)
-    kw = dict(n_orb=30, policy=1, use_heatbath=True, eps1=1e-6, want_vp=False)
-    x = S.normalized_psi(len(V), 12)
-    try:
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 0))
-        A = D.build(ctx, V, **kw)
-        y_csr = A.spmv(x, precision=N.F32)
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 2))
-        B = D.build(ctx, V, **kw)
-        y_pan = B.spmv(x, precision=N.F32)
-        y_pan2 = B.spmv(x, precision=N.F32)
-        num, den = B.local_energy(x, precision=N.F32)
-    finally:
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_PANELS, 0))
-    ref = A.to_scipy(0).dot(x)
-    scale = np.abs(ref).max()
-    np.testing.assert_array_equal(y_pan, y_pan2)
-    np.testing.assert_allclose(y_pan, y_csr, rtol=0, atol=1e-8 * scale)
-    assert np.abs(y_pan - ref).max() < 1e-5
-    assert abs(num / den - x @ ref / (x @ x)) <= FP32_DE_TOL
-    A.close()
-    B.close()
