@@ -68,6 +68,12 @@ EPS1 = 1e-6
 SMS = 148          # B200 streaming multiprocessors
 INT_SEED, DET_SEED, PSI_SEED = 1001, 2002, 3003
 CACHE = os.path.join(tempfile.gettempdir(), "detnqs_b200_bench")
+_T0 = time.perf_counter()
+
+
+def _log(msg: str) -> None:
+    """Progress on stderr (the JSON line is the only stdout output)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
 
 
 def workload(rank: int, n_dets: int):
@@ -86,7 +92,14 @@ def workload(rank: int, n_dets: int):
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region.
+
+    nvidia-smi's start-up (driver queries) stalls CUDA calls of the same
+    process for up to a few hundred milliseconds, so start() returns only
+    after the first sample has arrived: callers start it before their
+    warm-up steps and bracket the timed steps with begin() / end(); the
+    statistics use the samples taken between the two (all samples when the
+    timed region was shorter than one sampling interval)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -95,7 +108,9 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.t_begin = None
+        self.t_end = None
 
     def start(self):
         try:
@@ -105,12 +120,21 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
 
+    def begin(self):
+        self.t_begin = time.perf_counter()
+
+    def end(self):
+        self.t_end = time.perf_counter()
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -122,7 +146,12 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        lines = [ln for t, ln in self.lines
+                 if (self.t_begin is None or t >= self.t_begin)
+                 and (self.t_end is None or t <= self.t_end + 0.25)]
+        if not lines:
+            lines = [ln for _, ln in self.lines]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -296,7 +325,9 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n_dets = args.n_dets
+    _log("sampling the determinant space")
     sysm, V, psi = workload(rank, n_dets)
+    _log("context")
     ctx = core.IntCtx.from_arrays(N_ORB, sysm.h1e, sysm.eri, sysm.e_core, device=local)
     ctx.hb_prepare(1e-15)
     # the step runs FP32 H.psi on every build: its FP32 copy is written by the build
@@ -323,14 +354,17 @@ def run_ours(args, rank: int, world: int):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
+    _log("warm-up steps")
     for _ in range(args.warmup):
         H, *_ = step()
         H.close()
     barrier()
+    _log("timed steps")
 
     launches0 = native.lib.dnq_launch_count()
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     t_steps, t_build, t_fill, t_count, t_e64, t_e32 = [], [], [], [], [], []
     nnz = cand = 0
     dE = 0.0
@@ -356,11 +390,13 @@ def run_ours(args, rank: int, world: int):
             last = H
         else:
             H.close()
+    clk.end()
     clocks = clk.stop()
     launches = (native.lib.dnq_launch_count() - launches0) // args.steps
     ms_step = max_over_ranks(float(np.mean(t_steps)), world, dev)
 
     # ---- steady state of the inner loop: repeated H.psi on the resident H
+    _log("steady-state H.psi")
     ss = {}
     for prec, key in ((native.F64, "f64"), (native.F32, "f32")):
         for _ in range(2):   # FP32 values prepared outside timing
@@ -403,6 +439,7 @@ def run_ours(args, rank: int, world: int):
         del Xk, Yk
 
     # ---- end to end through the C ABI with host buffers
+    _log("end-to-end steps")
     pin_V = torch.from_numpy(V.view(np.int64)).pin_memory()
     pin_psi = torch.from_numpy(psi).pin_memory()
     pin_eloc = torch.empty(n_dets, dtype=torch.float64).pin_memory()
@@ -505,8 +542,11 @@ def run_ours(args, rank: int, world: int):
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _log("CPU baseline: reference rows")
         rate, rows, cnnz, t, threads, kind = cpu_reference_sample(sysm, V, args.cpu_seconds)
+        _log("CPU baseline: SciPy H.psi")
         er, et = scipy_eloc_rate(last, psi)
+        _log("CPU baseline done")
         result["cpu_baseline"] = {
             "value": rate, "unit": "elements/s", "cores": threads, "kind": kind,
             "sample": f"{rows} random rows of the same 1e6-det space, static heat-bath "
@@ -584,11 +624,12 @@ def run_batched(args, rank: int, world: int):
     launches_per_step = (native.lib.dnq_launch_count() - l0) // 3
     phase = {k: float(np.mean([p[k] for p in phases])) for k in phases[0]}
 
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
     for _ in range(args.warmup):
         bt.step(psi_dev, precision=native.F32, graph=True, stream=sp, eloc=eloc_dev)
     barrier()
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     t_step = []
     for _ in range(args.steps):
         flush.zero_()
@@ -616,6 +657,7 @@ def run_batched(args, rank: int, world: int):
         ts.append(ms)
     t_multi = float(np.mean(ts))
     del Xk
+    clk.end()
     clocks = clk.stop()
     ms_step = max_over_ranks(float(np.mean(t_step)), world, dev)
     e64b, _ = bt.step(psi_dev, precision=native.F64, stream=sp)
@@ -835,6 +877,8 @@ def run_serving(args, rank: int, world: int):
         H = device.build(ctxs[k], d, n_orb=sysm.n_orb, policy=native.POLICY_STATIC,
                          use_heatbath=True, eps1=1e-7, want_vp=False)
         H.close()
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
     small = int(np.argmin([len(d) for _, d in systems]))
     for _ in range(max(1, args.warmup)):
         with V.Server(device=local, budget_bytes=SERVE_BUDGET, build_slots=4) as srv:
@@ -849,8 +893,7 @@ def run_serving(args, rank: int, world: int):
 
     # ---- served: continuous batching, FP32-compensated, HBM admission
     import threading
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     l0 = native.lib.dnq_launch_count()
     srv = V.Server(device=local, budget_bytes=SERVE_BUDGET, build_slots=args.serve_slots,
                    max_group=64)
@@ -874,6 +917,7 @@ def run_serving(args, rank: int, world: int):
     srv.close()
     launches = native.lib.dnq_launch_count() - l0
     barrier()
+    clk.end()
     clocks = clk.stop()
     span_served = t_end - t0
 
@@ -1053,13 +1097,14 @@ def run_downfold(args, rank: int, world: int):
         ev[5].record()
         return H, hpp, e_ref, E64, E32, ev
 
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
     for _ in range(args.warmup):
         H, hpp, e_ref, E64, E32, _ = step()
         for h in (H, E64, E32):
             h.close()
     barrier()
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     l0 = native.lib.dnq_launch_count()
     t_step, t_build, t_diag, t_h64, t_h32 = [], [], [], [], []
     for k in range(args.steps):
@@ -1079,6 +1124,7 @@ def run_downfold(args, rank: int, world: int):
         if k < args.steps - 1:
             for h in (H, E64, E32):
                 h.close()
+    clk.end()
     clocks = clk.stop()
     launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
     ms_step = max_over_ranks(float(np.mean(t_step)), world, dev)
@@ -1220,11 +1266,12 @@ def run_det_batch(args, rank: int, world: int):
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
     for _ in range(args.warmup):
         core.prepare_det_batch(Vd, hf, N_ORB, N_ALPHA, N_BETA, **kw)
     barrier()
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     l0 = native.lib.dnq_launch_count()
     ts = []
     for _ in range(args.steps):
@@ -1237,6 +1284,7 @@ def run_det_batch(args, rank: int, world: int):
         b.record()
         torch.cuda.synchronize()
         ts.append(a.elapsed_time(b))
+    clk.end()
     clocks = clk.stop()
     launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
     ms = max_over_ranks(float(np.mean(ts)), world, dev)
@@ -1335,11 +1383,12 @@ def run_slogdet(args, rank: int, world: int):
         sign, logabs = L.slogdet(x, device=local)
         return sign, logabs, L.slogdet_grad(x, c, device=local)
 
+    clk = ClockSampler(local)   # before the warm-up: see ClockSampler
+    clk.start()
     for _ in range(args.warmup):
         step(ad, cd)
     barrier()
-    clk = ClockSampler(local)
-    clk.start()
+    clk.begin()
     l0 = native.lib.dnq_launch_count()
     ts = []
     for _ in range(args.steps):
@@ -1352,6 +1401,7 @@ def run_slogdet(args, rank: int, world: int):
         e1.record()
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1))
+    clk.end()
     clocks = clk.stop()
     launches = (native.lib.dnq_launch_count() - l0) // max(1, args.steps)
     ms = max_over_ranks(float(np.mean(ts)), world, dev)
@@ -1574,6 +1624,7 @@ def run_extras(args) -> dict:
     for w, reps in EXTRAS:
         runs = []
         for _ in range(reps):
+            _log(f"extra: {w}")
             t0 = time.perf_counter()
             try:
                 p = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", w,
