@@ -48,6 +48,7 @@ int g_build_f32 = 0;   // V->V-only builds write the FP32 copy and the diagonal 
 namespace {
 
 constexpr int kWS = 8;               // warps per block
+constexpr int kBS = 512;   // beta singles of one row kept for the presence rows
 constexpr u32 kBigGroup = 2048;      // part C default: search instead of scan above this
 
 struct StrMapView {
@@ -84,6 +85,10 @@ struct StrIndex {
     DBuf<uint2> pres;            // {bits, set bits in the row's earlier words}
     u32 pres_words = 0;
     u32 pres_min = 0xffffffffu;
+    // Per group: the part C tests of a row whose string is the group's, when
+    // it walks the groups of its singles (scanned members, groups tested by
+    // presence rows, groups binary-searched, singles that are groups).
+    DBuf<uint4> cost;
     StrMapView view() const { return StrMapView{slots.p, mask}; }
 };
 
@@ -308,8 +313,9 @@ __global__ void k_pres_rank(uint2* pres, i64 rows, u32 words) {
     }
 }
 
-// Presence rows of the alpha index A over the beta groups of B.  The
-// threshold starts at kPresMin and doubles until the rows fit kPresBytes.
+// Presence rows of the groups of index A over the groups of index B (alpha
+// over beta, and beta over alpha for the beta-major walk).  The threshold
+// starts at kPresMin and doubles until the rows fit kPresBytes.
 void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
     if (n == 0 || A.ngroups == 0) return;
     const u32 words = (u32)((B.ngroups + 31) / 32);
@@ -352,6 +358,66 @@ __device__ __forceinline__ double eri(const double* E, int p, int q, int r, int 
     return __ldg(&E[tri2(tri2(p, q), tri2(r, s))]);
 }
 
+// Part C costs of every group of index X (one warp per group): the walk of
+// a row whose X string is the group's looks up the group of each single x'
+// of that string and scans it, tests it through presence rows or binary-
+// searches it (the same classification as part_c, with the other string's
+// single count taken from the first determinant: every string of a space
+// has the same electron count).
+__global__ void k_group_cost(const u64* V, const u32* idx, const u32* gstart, i64 ngroups,
+                             int major, int n_orb, StrMapView xmap, int has_pres, u32 pres_min,
+                             u32 big_group, uint4* cost) {
+    __shared__ u8 lists[kWS][128];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    u8* occ = lists[w];
+    u8* vir = lists[w] + 64;
+    const u64 all = low_mask(n_orb);
+    const int ny = __popcll(V[1 - major]);
+    const int nyv = ny * (n_orb - ny);
+    const bool usep = has_pres && nyv <= kBS;
+    for (i64 g = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5; g < ngroups;
+         g += ((i64)gridDim.x * blockDim.x) >> 5) {
+        const u64 x = V[2 * (i64)idx[gstart[g]] + major];
+        for (int o = lane; o < n_orb; o += 32) {
+            const u64 below = (1ull << o) - 1ull;
+            if ((x >> o) & 1ull) occ[__popcll(x & below)] = (u8)o;
+            else vir[o - __popcll(x & below)] = (u8)o;
+        }
+        __syncwarp();
+        const int nx = __popcll(x), nvx = __popcll(~x & all), ns = nx * nvx;
+        u32 scan = 0, pb = 0, bg = 0, ix = 0;
+        for (int i = lane; i < ns; i += 32) {
+            u32 gs = 0, gl = 0;
+            if (!xmap.find(x ^ (1ull << occ[i / nvx]) ^ (1ull << vir[i % nvx]), gs, gl)) continue;
+            ++ix;
+            const bool pbig = usep && gl > pres_min && gl > (u32)nyv;
+            if (pbig) ++pb;
+            else if (gl > big_group) ++bg;
+            else scan += gl;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            scan += __shfl_xor_sync(0xffffffffu, scan, o);
+            pb += __shfl_xor_sync(0xffffffffu, pb, o);
+            bg += __shfl_xor_sync(0xffffffffu, bg, o);
+            ix += __shfl_xor_sync(0xffffffffu, ix, o);
+        }
+        if (lane == 0) cost[g] = make_uint4(scan, pb, bg, ix);
+        __syncwarp();
+    }
+}
+
+void build_group_cost(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cudaStream_t s) {
+    if (n == 0 || X.ngroups == 0) return;
+    X.cost.alloc(X.ngroups, s);
+    const i64 blocks = std::min<i64>((X.ngroups + kWS - 1) / kWS, 65535);
+    k_group_cost<<<(unsigned)blocks, kWS * 32, 0, s>>>(V, X.idx.p, X.gstart.p, X.ngroups, major,
+                                                       n_orb, X.view(), X.pres.p != nullptr,
+                                                       X.pres.p ? X.pres_min : 0xffffffffu,
+                                                       kBigGroup, X.cost.p);
+    DNQ_CHECK_LAUNCH();
+}
+
 struct VVParams {
     CtxView C;
     const double* E;        // packed ERI
@@ -380,6 +446,13 @@ struct VVParams {
     const uint2* pres;
     u32 pres_words;
     u32 pres_min;
+    // the same for beta groups over the alpha groups (beta-major part C)
+    const u32* b_prow;
+    const uint2* pres_b;
+    u32 pres_words_b;
+    u32 pres_min_b;
+    const uint4* a_cost;   // part C costs per alpha / beta group (null: alpha-major)
+    const uint4* b_cost;
 };
 
 // Where rows are written.  Single pass: rows appended to warp-private
@@ -525,7 +598,6 @@ __device__ __forceinline__ bool keep_single(const VVParams& P, double psr, doubl
 }
 
 // Per-warp shared state.
-constexpr int kBS = 512;   // beta singles of one row kept for the presence rows
 
 // Loads of a scan are issued kScanU steps ahead of their tests (every step
 // is a dependent global load); the sink sees the kScanU steps' hits, then
@@ -568,10 +640,14 @@ __device__ __forceinline__ void load_lists(WarpShared& S, u64 a, u64 b, int n_or
 // hold the alpha hole and particle.  The diagonal is a member of its own
 // kind whose position is the row.  Members are found by walk_row and
 // turned into elements by eval_hit, in the order found.
-// kinds: same beta string, same alpha string, opposite-spin double, diagonal,
-// a single evaluated ahead (its position field is its index in the singles
-// list).  kSingleBit marks a single of kind A or B as the walk finds it.
-enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2, kHitD = 3, kHitS = 4 };
+// kinds: same beta string, same alpha string, opposite-spin double found
+// through the alpha groups (position in the alpha-sorted order, tag with the
+// alpha hole and particle), diagonal, a single evaluated ahead (its position
+// field is its index in the singles list), opposite-spin double found
+// through the beta groups (position in the beta-sorted order, tag with the
+// beta hole and particle).  kSingleBit marks a single of kind A or B as the
+// walk finds it.
+enum : u32 { kHitA = 0, kHitB = 1, kHitC = 2, kHitD = 3, kHitS = 4, kHitC2 = 5 };
 constexpr u32 kSingleBit = 0x80;
 
 struct Hit {
@@ -600,6 +676,16 @@ __device__ __forceinline__ Hit eval_hit(const VVParams& P, int r, u64 a, u64 b, 
         e.h = (perm & 1) ? -raw : raw;
         e.keep = keep_double(cut, e.h);
         if (e.keep) e.j = __ldg(&P.a_idx[pos]);
+    } else if (kind == kHitC2) {
+        const u64 y = __ldg(&P.b_other[pos]);   // the member's alpha string
+        const u64 x = a ^ y;
+        const int hb = (tag >> 8) & 0xff, pb = tag >> 16;
+        const int ha = __ffsll(a & x) - 1, pa = __ffsll(y & x) - 1;
+        const double raw = eri(P.E, ha, pa, hb, pb);   // (a i|b j)
+        const int perm = occ_between(a, pa, ha) + occ_between(b, pb, hb);
+        e.h = (perm & 1) ? -raw : raw;
+        e.keep = keep_double(cut, e.h);
+        if (e.keep) e.j = __ldg(&P.b_idx[pos]);
     } else if (kind == kHitD) {
         e.h = P.diag[r];
         e.keep = fabs(e.h) > kElemThresh;
@@ -649,7 +735,7 @@ template <> __device__ __forceinline__ const u32* b_others<u32>(const VVParams& 
 template <class W, class Q>
 __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_other, W b,
                                               unsigned long long& tests, u32 gs, u32 sl, int hh,
-                                              int pp) {
+                                              int pp, u32 kind) {
     const int lane = threadIdx.x & 31;
     u32 incl = sl;   // inclusive prefix over lanes
 #pragma unroll
@@ -664,7 +750,7 @@ __device__ __forceinline__ void part_c_packed(Q& q, WarpShared& S, const W* a_ot
         const int slot = __popc(ne & lanemask_lt());
         const u32 pre = incl - sl;   // first member of this lane's group
         S.off[slot] = gs - pre;
-        S.tg[slot] = kHitC | ((u32)hh << 8) | ((u32)pp << 16);
+        S.tg[slot] = kind | ((u32)hh << 8) | ((u32)pp << 16);
         S.first[slot] = pre;
     }
     const int ns = __popc(ne);
@@ -746,6 +832,174 @@ __device__ __forceinline__ void scan_same(Q& q, const W* other, W x, u32 st, u32
     }
 }
 
+// Part C in one direction.  x is the string whose singles x' give the
+// groups (alpha-major: x = a, the groups of the alpha index, members
+// sorted by their beta strings); y is the other string, and a member is a
+// hit when its string differs from y in one orbital pair.  Its tag holds
+// the kind and x's hole and particle.  bm selects beta-major; the
+// direction's arrays are read from P where they are used (fewer live
+// registers than passing them in).
+template <class W, class Q>
+__device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
+                                       unsigned long long& tests, bool bm, u64 a, u64 b, int na,
+                                       int nva, int nb, int nvb) {
+    const int lane = threadIdx.x & 31;
+    const u64 x = bm ? b : a, y = bm ? a : b;
+    const u8* occx = bm ? S.occb : S.occa;
+    const u8* virx = bm ? S.virb : S.vira;
+    const u8* occy = bm ? S.occa : S.occb;
+    const u8* viry = bm ? S.vira : S.virb;
+    const int nvx = bm ? nvb : nva, ny = bm ? na : nb, nvy = bm ? nva : nvb;
+    const u32 kind = bm ? kHitC2 : kHitC;
+    const W* xo = bm ? b_others<W>(P) : a_others<W>(P);
+    const uint2* pres = bm ? P.pres_b : P.pres;
+    const W yw = (W)y;
+    const int nsx = (bm ? nb : na) * nvx;
+    const int nyv = ny * nvy;
+    const bool usep = pres != nullptr && nyv <= kBS;
+    int nys = -1;   // indexed y singles listed in S (-1: not yet)
+    for (int s0 = 0; s0 < nsx; s0 += 32) {
+        const int sidx = s0 + lane;
+        u32 gs = 0, gl = 0;
+        int hh = 0, pp = 0;
+        if (sidx < nsx) {
+            hh = occx[sidx / nvx];
+            pp = virx[sidx % nvx];
+            if (!(bm ? P.bmap : P.amap).find(x ^ (1ull << hh) ^ (1ull << pp), gs, gl)) gl = 0;
+        }
+        // presence rows for long groups (when the row's y singles fit the
+        // warp's list), binary search above big_group otherwise, else a scan
+        const bool pbig = usep && gl > (bm ? P.pres_min_b : P.pres_min) && gl > (u32)nyv;
+        const bool big = !pbig && gl > P.big_group;
+        const bool small = gl != 0 && !pbig && !big;
+        const u32 prw =
+            pbig ? __ldg(&(bm ? P.b_prow : P.a_prow)[__ldg(&(bm ? P.b_gid : P.a_gid)[gs])]) : 0u;
+        if (!P.c_groupwalk) {
+            part_c_packed(q, S, xo, yw, tests, gs, small ? gl : 0u, hh, pp, kind);
+        } else {
+            // one group at a time: start, length and the x excitation are
+            // warp-uniform, members in order 32 per step
+            unsigned m = __ballot_sync(0xffffffffu, small);
+            while (m) {
+                const int L = __ffs(m) - 1;
+                m &= m - 1;
+                const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
+                const u32 gn = __shfl_sync(0xffffffffu, gl, L);
+                const u32 tag = kind | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                                ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
+                tests += gn;
+                for (u32 t0 = 0; t0 < gn; t0 += 32 * kScanU) {
+                    W w[kScanU];
+#pragma unroll
+                    for (int u = 0; u < kScanU; ++u) {
+                        const u32 t = t0 + 32 * u + lane;
+                        w[u] = t < gn ? __ldg(&xo[g0 + t]) : yw;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kScanU; ++u) {
+                        if (t0 + 32 * u >= gn) break;
+                        q.push(popc_w(yw ^ w[u]) == 2, g0 + t0 + 32 * u + lane, tag);
+                    }
+                    q.sync();
+                }
+            }
+        }
+        unsigned pm = __ballot_sync(0xffffffffu, pbig);
+        if (pm && nys < 0) {   // the row's indexed y singles, once per row, in order
+            nys = 0;
+            for (int q0 = 0; q0 < nyv; q0 += 32) {
+                const int qi = q0 + lane;
+                bool f = false;
+                u32 bid = 0;
+                u16 e = 0;
+                if (qi < nyv) {
+                    const int hb = occy[qi / nvy], pb = viry[qi % nvy];
+                    u32 bst = 0, bln = 0;
+                    if ((bm ? P.amap : P.bmap).find(y ^ (1ull << hb) ^ (1ull << pb), bst, bln)) {
+                        f = true;
+                        bid = __ldg(&(bm ? P.a_gid : P.b_gid)[bst]);
+                        e = (u16)(hb | (pb << 8));
+                    }
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, f);
+                if (f) {
+                    const int at = nys + __popc(fm & lanemask_lt());
+                    S.bs_id[at] = bid;
+                    S.bs_hp[at] = e;
+                }
+                nys += __popc(fm);
+            }
+            __syncwarp();
+        }
+        while (pm) {
+            // members of a long group are sorted by their y group: the member
+            // with y group bid sits at the number of set bits before bid
+            const int L = __ffs(pm) - 1;
+            pm &= pm - 1;
+            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
+            const u32 tag = kind | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
+            const uint2* row =
+                pres + (i64)__shfl_sync(0xffffffffu, prw, L) * (bm ? P.pres_words_b : P.pres_words);
+            tests += nys;
+            for (int q0 = 0; q0 < nys; q0 += 32 * kScanU) {
+                uint2 w[kScanU];
+                u32 sh[kScanU];
+#pragma unroll
+                for (int u = 0; u < kScanU; ++u) {
+                    const int qi = q0 + 32 * u + lane;
+                    w[u] = make_uint2(0u, 0u);
+                    sh[u] = 0;
+                    if (qi < nys) {
+                        const u32 bid = S.bs_id[qi];
+                        sh[u] = ~bid & 31u;   // moves the group's bit to bit 31
+                        w[u] = __ldg(&row[bid >> 5]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kScanU; ++u) {
+                    if (q0 + 32 * u >= nys) break;
+                    const u32 lo = w[u].x << sh[u];   // the group's bit and those below
+                    q.push((int)lo < 0, g0 + w[u].y + __popc(lo) - 1u, tag);
+                }
+                q.sync();
+            }
+        }
+        // other large groups: binary-search every y single
+        unsigned bigm = __ballot_sync(0xffffffffu, big);
+        while (bigm) {
+            const int L = __ffs(bigm) - 1;
+            bigm &= bigm - 1;
+            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
+            const u32 gn = __shfl_sync(0xffffffffu, gl, L);
+            const u32 tag = kind | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
+                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
+            tests += nyv;
+            for (int q0 = 0; q0 < nyv; q0 += 32) {
+                const int qi = q0 + lane;
+                bool hit = false;
+                u32 lo = 0;
+                if (qi < nyv) {
+                    const int hb = occy[qi / nvy];
+                    const int pb = viry[qi % nvy];
+                    const u64 t = y ^ (1ull << hb) ^ (1ull << pb);
+                    lo = g0;
+                    u32 hi = g0 + gn;
+                    while (lo < hi) {
+                        const u32 mid = (lo + hi) >> 1;
+                        if (__ldg(&(bm ? P.b_other : P.a_other)[mid]) < t) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    hit = lo < g0 + gn && __ldg(&(bm ? P.b_other : P.a_other)[lo]) == t;
+                }
+                q.push(hit, lo, tag);
+                q.sync();
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // The members of row r = (a, b) in their fixed order: the diagonal, then
 // parts A, B and C.  q.push(hit, position, tag) is warp-collective, once
 // per step of 32; q.sync() follows every group of at most kScanU steps.
@@ -770,150 +1024,35 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     gln = __shfl_sync(0xffffffffu, ln, 1);
     tests += gln;
     scan_same(q, ao, bw, gst, gln, kHitB);
-    // ---- part C: alpha single x beta single, via the groups of the a'
+    // ---- part C: alpha single x beta single.  Either direction finds the
+    // same members: the groups of the row's alpha singles a' tested for a
+    // beta single of b (alpha-major), or the groups of its beta singles b'
+    // tested for an alpha single of a (beta-major).  The row takes the one
+    // with fewer tests, from the costs precomputed per group of its two
+    // strings (the same rule on every path, so a row's member order does not
+    // depend on the path that builds it).
     const int na = __popcll(a), nva = __popcll(~a & all);
-    const int nsa = na * nva;
     const int nb = __popcll(b), nvb = __popcll(~b & all);
-    const int nbv = nb * nvb;
-    const bool usep = P.pres != nullptr && nbv <= kBS;
-    int nbs = -1;   // indexed beta singles listed in S (-1: not yet)
-    for (int s0 = 0; s0 < nsa; s0 += 32) {
-        const int sidx = s0 + lane;
-        u32 gs = 0, gl = 0;
-        int hh = 0, pp = 0;
-        if (sidx < nsa) {
-            hh = S.occa[sidx / nva];
-            pp = S.vira[sidx % nva];
-            if (!P.amap.find(a ^ (1ull << hh) ^ (1ull << pp), gs, gl)) gl = 0;
-        }
-        // presence rows for long groups (when the row's beta singles fit the
-        // warp's list), binary search above big_group otherwise, else a scan
-        const bool pbig = usep && gl > P.pres_min && gl > (u32)nbv;
-        const bool big = !pbig && gl > P.big_group;
-        const bool small = gl != 0 && !pbig && !big;
-        const u32 prw = pbig ? __ldg(&P.a_prow[__ldg(&P.a_gid[gs])]) : 0u;   // its presence row
-        if (!P.c_groupwalk) {
-            part_c_packed(q, S, ao, bw, tests, gs, small ? gl : 0u, hh, pp);
-        } else {
-            // one group at a time: start, length and the alpha excitation are
-            // warp-uniform, members in order 32 per step
-            unsigned m = __ballot_sync(0xffffffffu, small);
-            while (m) {
-                const int L = __ffs(m) - 1;
-                m &= m - 1;
-                const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
-                const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-                const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
-                                ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
-                tests += gn;
-                for (u32 t0 = 0; t0 < gn; t0 += 32 * kScanU) {
-                    W y[kScanU];
-#pragma unroll
-                    for (int u = 0; u < kScanU; ++u) {
-                        const u32 t = t0 + 32 * u + lane;
-                        y[u] = t < gn ? __ldg(&ao[g0 + t]) : bw;
-                    }
-#pragma unroll
-                    for (int u = 0; u < kScanU; ++u) {
-                        if (t0 + 32 * u >= gn) break;
-                        q.push(popc_w(bw ^ y[u]) == 2, g0 + t0 + 32 * u + lane, tag);
-                    }
-                    q.sync();
-                }
-            }
-        }
-        unsigned pm = __ballot_sync(0xffffffffu, pbig);
-        if (pm && nbs < 0) {   // the row's indexed beta singles, once per row, in order
-            nbs = 0;
-            for (int q0 = 0; q0 < nbv; q0 += 32) {
-                const int qi = q0 + lane;
-                bool f = false;
-                u32 bid = 0;
-                u16 e = 0;
-                if (qi < nbv) {
-                    const int hb = S.occb[qi / nvb], pb = S.virb[qi % nvb];
-                    u32 bst = 0, bln = 0;
-                    if (P.bmap.find(b ^ (1ull << hb) ^ (1ull << pb), bst, bln)) {
-                        f = true;
-                        bid = __ldg(&P.b_gid[bst]);
-                        e = (u16)(hb | (pb << 8));
-                    }
-                }
-                const unsigned fm = __ballot_sync(0xffffffffu, f);
-                if (f) {
-                    const int at = nbs + __popc(fm & lanemask_lt());
-                    S.bs_id[at] = bid;
-                    S.bs_hp[at] = e;
-                }
-                nbs += __popc(fm);
-            }
-            __syncwarp();
-        }
-        while (pm) {
-            // members of a long group are sorted by beta group: the member
-            // with beta group bid sits at the number of set bits before bid
-            const int L = __ffs(pm) - 1;
-            pm &= pm - 1;
-            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
-            const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
-                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
-            const uint2* row = P.pres + (i64)__shfl_sync(0xffffffffu, prw, L) * P.pres_words;
-            tests += nbs;
-            for (int q0 = 0; q0 < nbs; q0 += 32 * kScanU) {
-                uint2 w[kScanU];
-                u32 sh[kScanU];
-#pragma unroll
-                for (int u = 0; u < kScanU; ++u) {
-                    const int qi = q0 + 32 * u + lane;
-                    w[u] = make_uint2(0u, 0u);
-                    sh[u] = 0;
-                    if (qi < nbs) {
-                        const u32 bid = S.bs_id[qi];
-                        sh[u] = ~bid & 31u;   // moves the group's bit to bit 31
-                        w[u] = __ldg(&row[bid >> 5]);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kScanU; ++u) {
-                    if (q0 + 32 * u >= nbs) break;
-                    const u32 lo = w[u].x << sh[u];   // the group's bit and those below
-                    q.push((int)lo < 0, g0 + w[u].y + __popc(lo) - 1u, tag);
-                }
-                q.sync();
-            }
-        }
-        // other large groups: binary-search every beta single of b
-        unsigned bigm = __ballot_sync(0xffffffffu, big);
-        while (bigm) {
-            const int L = __ffs(bigm) - 1;
-            bigm &= bigm - 1;
-            const u32 g0 = __shfl_sync(0xffffffffu, gs, L);
-            const u32 gn = __shfl_sync(0xffffffffu, gl, L);
-            const u32 tag = kHitC | ((u32)__shfl_sync(0xffffffffu, hh, L) << 8) |
-                            ((u32)__shfl_sync(0xffffffffu, pp, L) << 16);
-            tests += nbv;
-            for (int q0 = 0; q0 < nbv; q0 += 32) {
-                const int qi = q0 + lane;
-                bool hit = false;
-                u32 lo = 0;
-                if (qi < nbv) {
-                    const int hb = S.occb[qi / nvb];
-                    const int pb = S.virb[qi % nvb];
-                    const u64 y = b ^ (1ull << hb) ^ (1ull << pb);
-                    lo = g0;
-                    u32 hi = g0 + gn;
-                    while (lo < hi) {
-                        const u32 mid = (lo + hi) >> 1;
-                        if (__ldg(&P.a_other[mid]) < y) lo = mid + 1; else hi = mid;
-                    }
-                    hit = lo < g0 + gn && __ldg(&P.a_other[lo]) == y;
-                }
-                q.push(hit, lo, tag);
-                q.sync();
-            }
-        }
-        __syncwarp();
+    bool bm = false;
+    if (P.a_cost) {   // the costs of the row's two groups (found for parts A and B)
+        uint4 c = make_uint4(0u, 0u, 0u, 0u);
+        if (lane == 0 && ln) c = __ldg(&P.b_cost[__ldg(&P.b_gid[st])]);
+        if (lane == 1 && ln) c = __ldg(&P.a_cost[__ldg(&P.a_gid[st])]);
+        const uint4 cb = make_uint4(__shfl_sync(0xffffffffu, c.x, 0),
+                                    __shfl_sync(0xffffffffu, c.y, 0),
+                                    __shfl_sync(0xffffffffu, c.z, 0),
+                                    __shfl_sync(0xffffffffu, c.w, 0));
+        const uint4 ca = make_uint4(__shfl_sync(0xffffffffu, c.x, 1),
+                                    __shfl_sync(0xffffffffu, c.y, 1),
+                                    __shfl_sync(0xffffffffu, c.z, 1),
+                                    __shfl_sync(0xffffffffu, c.w, 1));
+        const u64 cost_a = ca.x + (u64)ca.y * cb.w + (u64)ca.z * (u32)(nb * nvb);
+        const u64 cost_b = cb.x + (u64)cb.y * ca.w + (u64)cb.z * (u32)(na * nva);
+        bm = cost_b < cost_a;
     }
+    // one call site for both directions: a second inlined copy of the walk
+    // would not fit the instruction cache
+    part_c<W>(P, S, q, tests, bm, a, b, na, nva, nb, nvb);
 }
 
 // A member's tag, given as a value or as a function read only on a hit.
@@ -1662,6 +1801,12 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
     P.pres = A.pres.p;
     P.pres_words = A.pres_words;
     P.pres_min = A.pres.p ? A.pres_min : 0xffffffffu;
+    P.b_prow = B.prow.p;
+    P.pres_b = B.pres.p;
+    P.pres_words_b = B.pres_words;
+    P.pres_min_b = B.pres.p ? B.pres_min : 0xffffffffu;
+    P.a_cost = A.cost.p;
+    P.b_cost = B.cost.p;
     return P;
 }
 
@@ -1681,6 +1826,9 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     build_str_index(A, V, n, 0, n_orb, s);
     build_str_index(B, V, n, 1, n_orb, s);
     build_presence(A, B, n, s);
+    build_presence(B, A, n, s);
+    build_group_cost(A, V, n, 0, n_orb, s);
+    build_group_cost(B, V, n, 1, n_orb, s);
     const bool narrow = n_orb <= 32;
     if (narrow) {
         narrow_index(A, n, s);
@@ -2176,6 +2324,9 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         build_str_index(b->A[k], b->V[k].p, n, 0, n_orb[k], s);
         build_str_index(b->B[k], b->V[k].p, n, 1, n_orb[k], s);
         build_presence(b->A[k], b->B[k], n, s);
+        build_presence(b->B[k], b->A[k], n, s);
+        build_group_cost(b->A[k], b->V[k].p, n, 0, n_orb[k], s);
+        build_group_cost(b->B[k], b->V[k].p, n, 1, n_orb[k], s);
         if (n_orb[k] <= 32) {
             narrow_index(b->A[k], n, s);
             narrow_index(b->B[k], n, s);
