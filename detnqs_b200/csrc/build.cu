@@ -15,6 +15,7 @@
 
 #include <cmath>
 #include <memory>
+#include <mutex>
 
 #include "gen.cuh"
 #include "ham.cuh"
@@ -383,14 +384,17 @@ struct PhaseTimer {
     }
 };
 
-// Testing switch: route V->V-only builds through the candidate walk too
-// (dnq_set_option(DNQ_OPT_FORCE_WALK, 1)); both paths give identical blocks.
-bool g_force_walk = false;
-extern i64 g_arena_chunk;
-extern i64 g_arena_cap;
-extern int g_partc_groupwalk;
-extern int g_build_f32;
-void spmv_set_option(int lanes, int unroll);
+namespace {
+std::mutex g_opt_mu;
+Options g_defaults;   // process-wide defaults of new handles, batches and servers
+}  // namespace
+
+Options default_options() {
+    std::lock_guard<std::mutex> lk(g_opt_mu);
+    return g_defaults;
+}
+
+thread_local const Options* g_build_opt = nullptr;
 
 // Resident-table cut for a policy (see hb_cutoff / full_cutoff).
 static double policy_cut(const dnq_ctx_s* c, int policy, int use_hb, double eps1) {
@@ -425,7 +429,7 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
     H->diag.alloc(nV, s);
     launch_diag(ctx, V.p, nV, H->diag.p, s);
 
-    if (!want_vp && !has_ext && n_orb < 64 && !g_force_walk) {
+    if (!want_vp && !has_ext && n_orb < 64 && !H->opt.force_walk) {
         // V->V block only: match rows against V's string groups.
         T.mark();
         T.fill(H->t_ms);   // [0] maps + diagonal
@@ -763,6 +767,7 @@ int dnq_build(dnq_ctx_t ctx, const uint64_t* dets_V, int64_t n_V, const uint64_t
     std::unique_ptr<dnq_ham_s> H(new dnq_ham_s);
     H->device = ctx->device;
     H->stream = (cudaStream_t)stream;
+    if (g_build_opt) H->opt = *g_build_opt;   // a server's own options
     if (n_V > 0)
         build_ham(ctx, dets_V, n_V, dets_ext, n_ext, psi, n_orb, policy, use_heatbath, eps1,
                   want_vp != 0, (cudaStream_t)stream, H.get());
@@ -780,13 +785,34 @@ int dnq_set_option(int option, int64_t value) {
     if (option == 5)
         require(value == 0 || value == 1 || value == 2 || value == 4, DNQ_ERR_INVALID,
                 "slots per lane must be 0, 1, 2 or 4");
-    if (option == 1) g_force_walk = value != 0;
-    if (option == 2) g_arena_chunk = value;
-    if (option == 3) g_arena_cap = value;
-    if (option == 4) spmv_set_option((int)value, -1);
-    if (option == 5) spmv_set_option(-1, (int)value);
-    if (option == 7) g_partc_groupwalk = value != 0;
-    if (option == 8) g_build_f32 = value != 0;
+    std::lock_guard<std::mutex> lk(g_opt_mu);
+    Options& o = g_defaults;
+    if (option == 1) o.force_walk = value != 0;
+    if (option == 2) o.arena_chunk = value;
+    if (option == 3) o.arena_cap = value;
+    if (option == 4) o.spmv_lanes = (int)value;
+    if (option == 5) o.spmv_unroll = (int)value;
+    if (option == 7) o.partc_groupwalk = value != 0;
+    if (option == 8) o.build_f32 = value != 0;
+    DNQ_API_END
+}
+
+// The H.psi shape of one handle (DNQ_OPT_SPMV_LANES / DNQ_OPT_SPMV_UNROLL),
+// leaving the defaults and other handles as they are.
+int dnq_ham_set_option(dnq_ham_t h, int option, int64_t value) {
+    DNQ_API_BEGIN
+    require(h != nullptr, DNQ_ERR_INVALID, "null handle");
+    require(option == DNQ_OPT_SPMV_LANES || option == DNQ_OPT_SPMV_UNROLL, DNQ_ERR_INVALID,
+            "only the H.psi options (lanes, slots) apply to a built handle");
+    if (option == DNQ_OPT_SPMV_LANES) {
+        require(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
+                DNQ_ERR_INVALID, "lanes per row must be 0, 4, 8, 16 or 32");
+        h->opt.spmv_lanes = (int)value;
+    } else {
+        require(value == 0 || value == 1 || value == 2 || value == 4, DNQ_ERR_INVALID,
+                "slots per lane must be 0, 1, 2 or 4");
+        h->opt.spmv_unroll = (int)value;
+    }
     DNQ_API_END
 }
 

@@ -184,6 +184,26 @@ inline void copy_out(T* dst, const T* dsrc, size_t count, cudaStream_t st) {
     DNQ_CUDA(cudaMemcpyAsync(dst, dsrc, count * sizeof(T), cudaMemcpyDefault, st));
 }
 
+// Library options (dnq_set_option).  The process-wide values are defaults:
+// every handle, batch and server takes a copy when it is created and uses
+// its own copy afterwards, so changing a default never reaches objects that
+// exist already, and a handle's H.psi shape can be set on that handle alone.
+struct Options {
+    int force_walk = 0;        // V->V-only builds through the candidate walk
+    long long arena_chunk = 0; // entries per warp chunk (0: default)
+    long long arena_cap = 0;   // arena capacity (0: automatic)
+    int partc_groupwalk = 0;   // part C short groups one at a time
+    int build_f32 = 0;         // V->V builds write the FP32 copy while compacting
+    int spmv_lanes = 0;        // H.psi lanes per row (0: by row length)
+    int spmv_unroll = 0;       // H.psi slots per lane (0: by row length)
+};
+// A copy of the process-wide defaults (thread-safe).
+Options default_options();
+// Options for the handles the calling thread builds through dnq_build, in
+// place of the defaults (a server's worker threads point it at the
+// server's copy); null outside such threads.
+extern thread_local const Options* g_build_opt;
+
 inline int sm_count(int device) {
     int v = 0;
     DNQ_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));

@@ -38,6 +38,7 @@ struct dnq_ham_s {
     dnq::DBuf<float> x32;             // FP32 scratch for the FP32 operator
     dnq::DBuf<unsigned long long> dets_p;   // (alpha, beta) pairs
     dnq::i64 candidates = 0;
+    dnq::Options opt = dnq::default_options();   // this handle's options
     // device time of the build phases (CUDA events on the build stream), ms:
     // [0] maps + diagonal, [1] count pass, [2] scans + allocation,
     // [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total
@@ -66,7 +67,7 @@ struct SpmvDesc {
     i64 nr, nnz;
 };
 // Lanes per row and slots per lane the H.psi kernels use for m.
-void spmv_shape(const Csr& m, int& G, int& U);
+void spmv_shape(const Options& o, const Csr& m, int& G, int& U);
 // One launch over nd descriptors (device array) sharing (G, U, precision).
 void spmv_grouped(const SpmvDesc* d_dev, int nd, i64 max_rows, int G, int U, int precision,
                   int device, cudaStream_t s);

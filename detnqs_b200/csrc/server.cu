@@ -180,6 +180,7 @@ struct SrvReq {
 
 struct dnq_server_s {
     int device = 0;
+    dnq::Options opt = dnq::default_options();   // options of the blocks it builds
     dnq::i64 budget = 0;
     int slots = 1;
     int max_group = 64;
@@ -352,7 +353,7 @@ void launch_group(dnq_server_s* S) {
         ed[k] = EnergyDesc{S->gx.p + o, S->gy.p + o, S->geloc.p + o, f32 ? S->gx32.p + o : nullptr,
                            h->n_v};
         int G = 4, U = 1;
-        spmv_shape(h->vv, G, U);
+        spmv_shape(h->opt, h->vv, G, U);
         SpmvDesc d{};
         d.rp = h->vv.rowptr.p;
         d.col = h->vv.col.p;
@@ -470,8 +471,10 @@ void worker(dnq_server_s* S, int slot) {
         lk.unlock();
         const auto tb = Clock::now();
         dnq_ham_t H = nullptr;
+        g_build_opt = &S->opt;
         int rc = dnq_build(y.ctx, y.dets.data(), y.n, nullptr, 0, nullptr, y.n_orb, y.policy,
                            y.use_hb, y.eps1, 0, s, &H);
+        g_build_opt = nullptr;
         std::string err = rc == DNQ_OK ? std::string() : std::string(dnq_last_error());
         i64 bytes = 0;
         if (rc == DNQ_OK) {

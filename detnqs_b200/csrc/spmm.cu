@@ -26,7 +26,7 @@
 
 namespace dnq {
 
-void spmv_shape(const Csr& m, int& G, int& U);
+void spmv_shape(const Options& o, const Csr& m, int& G, int& U);
 void ensure_f32(dnq_ham_s* h, cudaStream_t s);
 
 namespace {
@@ -314,12 +314,12 @@ void spmm_csr(const Csr& m, const float* val32, const double* diag32, const doub
               int kx, double* Y, int ldy, int precision, int G, int U, void* scratch,
               int dev, cudaStream_t s) {
     if (m.nr == 0) return;
-    if (G == 0) {
-        int u = 0;
-        spmv_shape(m, G, u);
+    if (G == 0 || U == 0) {
+        int g = 0, u = 0;
+        spmv_shape(Options{}, m, g, u);
+        if (G == 0) G = g;
         if (U == 0) U = u;
     }
-    if (U == 0) U = 1;
     const unsigned gi = (unsigned)std::max<i64>(1, std::min<i64>(4096, (m.nr * 8 + 255) / 256));
     if (precision == DNQ_F32) {
         float* Xg = static_cast<float*>(scratch);
@@ -354,8 +354,8 @@ void spmm_csr(const Csr& m, const float* val32, const double* diag32, const doub
 // The V block of a handle (FP32: its prepared split).
 void spmm_vv(dnq_ham_s* h, const double* X, int ldx, int kx, double* Y, int ldy, int precision,
              void* scratch, cudaStream_t s) {
-    spmm_csr(h->vv, h->vv.val32.p, h->diag_op.p, X, ldx, kx, Y, ldy, precision, 0, 0, scratch,
-             h->device, s);
+    spmm_csr(h->vv, h->vv.val32.p, h->diag_op.p, X, ldx, kx, Y, ldy, precision,
+             h->opt.spmv_lanes, h->opt.spmv_unroll, scratch, h->device, s);
 }
 
 // Bytes of the interleaved scratch for kx columns (n rows and a zero row).

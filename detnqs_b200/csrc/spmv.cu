@@ -226,16 +226,13 @@ void launch_g(int U, const Csr& m, const double* x, double* y, const double* yad
     }
 }
 
-// Lanes per row / slots per lane forced by dnq_set_option (0 = automatic).
-int g_spmv_lanes = 0;
-int g_spmv_unroll = 0;
-
+// G lanes per row and U slots per lane; 0 = by the average row length.
 void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, int precision,
                  const float* x32, const float* val32, const double* diag, int G, int U,
                  int device, cudaStream_t s) {
     if (m.nr == 0) return;
-    if (G == 0) G = g_spmv_lanes ? g_spmv_lanes : group_for(m);
-    if (U == 0) U = g_spmv_unroll ? g_spmv_unroll : unroll_for(m, G);
+    if (G == 0) G = group_for(m);
+    if (U == 0) U = unroll_for(m, G);
     switch (G) {
         case 32: launch_g<32>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
         case 16: launch_g<16>(U, m, x, y, yadd, precision, x32, val32, diag, device, s); break;
@@ -247,11 +244,6 @@ void launch_spmv(const Csr& m, const double* x, double* y, const double* yadd, i
 
 }  // namespace
 
-void spmv_set_option(int lanes, int unroll) {
-    if (lanes >= 0) g_spmv_lanes = lanes;
-    if (unroll >= 0) g_spmv_unroll = unroll;
-}
-
 // Same as spmv_block with lanes per row G and slots per lane U given
 // (0 = automatic).
 void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, int precision,
@@ -261,16 +253,18 @@ void spmv_block_g(const dnq_ham_s* h, const Csr& m, const double* x, double* y, 
     launch_spmv(m, x, y, nullptr, precision, x32, val32, diag, G, U, device, s);
 }
 
-// y (+)= M x for one block; x FP64 device, y FP64 device.
+// y (+)= M x for one block with the handle's H.psi shape; x FP64 device,
+// y FP64 device.
 void spmv_block(const dnq_ham_s* h, const Csr& m, const double* x, double* y,
                 const double* yadd, int precision, cudaStream_t s, float* x32,
                 const double* diag) {
-    launch_spmv(m, x, y, yadd, precision, x32, m.val32.p, diag, 0, 0, h->device, s);
+    launch_spmv(m, x, y, yadd, precision, x32, m.val32.p, diag, h->opt.spmv_lanes,
+                h->opt.spmv_unroll, h->device, s);
 }
 
-void spmv_shape(const Csr& m, int& G, int& U) {
-    G = g_spmv_lanes ? g_spmv_lanes : group_for(m);
-    U = g_spmv_unroll ? g_spmv_unroll : unroll_for(m, G);
+void spmv_shape(const Options& o, const Csr& m, int& G, int& U) {
+    G = o.spmv_lanes ? o.spmv_lanes : group_for(m);
+    U = o.spmv_unroll ? o.spmv_unroll : unroll_for(m, G);
 }
 
 namespace {

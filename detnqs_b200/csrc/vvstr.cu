@@ -42,8 +42,6 @@ namespace dnq {
 // Part C walk over the short groups: 0 = packed across the groups of a
 // round (default), 1 = one group at a time.  Both give the same entries in
 // the same order.
-int g_partc_groupwalk = 0;
-int g_build_f32 = 0;   // V->V-only builds write the FP32 copy and the diagonal as they compact
 
 namespace {
 
@@ -1597,8 +1595,6 @@ void excl_scan(const T* in, i64* out, i64 n, cudaStream_t s) {
 void check_orbitals(const u64* d, i64 n, int n_orb, cudaStream_t s);
 
 // Test options: warp chunk size and arena capacity (0 = automatic).
-i64 g_arena_chunk = 0;
-i64 g_arena_cap = 0;
 
 namespace {
 
@@ -1640,20 +1636,20 @@ void launch_big(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s
 // two-pass fallback leaves both empty.  Returns the number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
-           double* t_gen, double* t_scan, double* t_compact, i64* hits_out = nullptr,
-           int scan = 0, DBuf<double>* dg = nullptr) {
+           const Options& opt, double* t_gen, double* t_scan, double* t_compact,
+           i64* hits_out = nullptr, int scan = 0, DBuf<double>* dg = nullptr) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
     const i64 warps = (i64)grid * kWS;
     size_t freeb = 0, totb = 0;
     DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
-    const i64 chunk = g_arena_chunk > 0 ? g_arena_chunk : kChunk;
+    const i64 chunk = opt.arena_chunk > 0 ? (i64)opt.arena_chunk : kChunk;
     i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 512 * nrows;
     want += warps * chunk;
     const i64 maxfit = (i64)(freeb / 2 / 12);
     i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
-    if (g_arena_cap > 0) cap = g_arena_cap;
+    if (opt.arena_cap > 0) cap = (i64)opt.arena_cap;
     DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
     DBuf<unsigned long long> nt(1, s), cursor(1, s), nh(1, s);
     // singles list: ~5 per row on heat-bath spaces, in one slice per warp;
@@ -1773,7 +1769,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
 
 VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                      double cut, const double* psi, const double* diag, const StrIndex& A,
-                     const StrIndex& B) {
+                     const StrIndex& B, const Options& opt) {
     VVParams P{};
     P.C = ctx->view();
     P.E = ctx->erid.p;
@@ -1794,7 +1790,7 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
     P.cut = cut;
     P.psi = psi;
     P.big_group = kBigGroup;
-    P.c_groupwalk = g_partc_groupwalk;
+    P.c_groupwalk = opt.partc_groupwalk;
     P.a_gid = A.gid.p;
     P.a_prow = A.prow.p;
     P.b_gid = B.gid.p;
@@ -1835,12 +1831,12 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
         narrow_index(B, n, s);
     }
     DNQ_CUDA(cudaEventRecord(e1, s));
-    OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B)};
+    OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B, H->opt)};
     double tg = 0, tsc = 0, tc = 0;
     i64 hits = 0;
     H->candidates =
-        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, &tg, &tsc, &tc, &hits,
-               narrow ? 1 : 0, g_build_f32 ? &H->diag_op : nullptr);
+        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, H->opt, &tg, &tsc, &tc,
+               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);
@@ -2002,6 +1998,7 @@ __global__ void k_sanitize(i64* rowptr, i64 n, i64 cap, const int* overflow, int
 struct dnq_batch_s {
     int device = 0;
     int n_sys = 0;
+    dnq::Options opt = dnq::default_options();   // this batch's options
     dnq::i64 total = 0;
     std::vector<dnq_ctx_s*> ctx;
     std::vector<dnq::DBuf<dnq::u64>> V;
@@ -2082,7 +2079,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     DNQ_CHECK_LAUNCH();
     // the sizing build fills the batch's CSR itself, so the blocks are
     // valid right after creation
-    run_vv(L, n, 0, b->device, s, b->M, nullptr, nullptr, nullptr, &b->hits, b->scan);
+    run_vv(L, n, 0, b->device, s, b->M, b->opt, nullptr, nullptr, nullptr, &b->hits, b->scan);
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
@@ -2291,6 +2288,9 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
     cudaStream_t s = (cudaStream_t)stream;
     std::unique_ptr<dnq_batch_s> b(new dnq_batch_s);
     b->device = device;
+    if (b->opt.arena_chunk > 0) b->chunk = (dnq::i64)b->opt.arena_chunk;
+    b->spmv_group = b->opt.spmv_lanes;
+    b->spmv_unroll = b->opt.spmv_unroll;
     b->n_sys = n_sys;
     b->ctx.assign(ctxs, ctxs + n_sys);
     b->row_off_h.assign(n_sys + 1, 0);
@@ -2334,7 +2334,7 @@ int dnq_batch_create(int n_sys, const dnq_ctx_t* ctxs, const uint64_t* const* de
         const double cut = (policy == DNQ_POLICY_STATIC && use_heatbath)
                                ? hb_cutoff(ctxs[k], eps1) : full_cutoff();
         hp[k] = make_params(ctxs[k], b->V[k].p, n, n_orb[k], policy, eps1, cut, nullptr,
-                            b->diag.p + b->row_off_h[k], b->A[k], b->B[k]);
+                            b->diag.p + b->row_off_h[k], b->A[k], b->B[k], b->opt);
     }
     b->sys.alloc(n_sys, s);
     DNQ_CUDA(cudaMemcpyAsync(b->sys.p, hp.data(), n_sys * sizeof(VVParams),

@@ -79,6 +79,12 @@ class DeviceHamiltonian:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    def set_option(self, option: int, value: int) -> None:
+        """H.psi shape of this handle alone (N.OPT_SPMV_LANES: 0/4/8/16/32
+        lanes per row; N.OPT_SPMV_UNROLL: 0/1/2/4 slots per lane; 0 = by
+        the average row length)."""
+        N.check(N.lib.dnq_ham_set_option(self._h, option, int(value)))
+
     def timings(self) -> dict:
         """Device time (ms) of the build phases, from CUDA events."""
         t = np.zeros(8)

@@ -59,7 +59,7 @@ EXPORTS = (
     "dnq_ham_local_energy_multi",
     "dnq_batch_create", "dnq_batch_destroy", "dnq_batch_info", "dnq_batch_set_config",
     "dnq_batch_get_config", "dnq_batch_step", "dnq_batch_apply", "dnq_batch_timings", "dnq_batch_copy_coo",
-    "dnq_batch_apply_multi", "dnq_sort_order",
+    "dnq_batch_apply_multi", "dnq_sort_order", "dnq_ham_set_option",
     "dnq_server_create", "dnq_server_destroy", "dnq_server_add_system", "dnq_server_submit",
     "dnq_server_wait", "dnq_server_set_budget", "dnq_server_pause", "dnq_server_stats",
     "dnq_ctx_create_wide", "dnq_wide_diag", "dnq_wide_build", "dnq_ham_symmetrize",
@@ -119,6 +119,7 @@ _sig("dnq_prepare_det_batch", _P, _I64, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, 
 _sig("dnq_build", _P, _P, _I64, _P, _I64, _P, _I, _I, _I, _D, _I, _P, C.POINTER(_P))
 _sig("dnq_ham_destroy", _P)
 _sig("dnq_set_option", _I, _I64)
+_sig("dnq_ham_set_option", _P, _I, _I64)
 _sig("dnq_ham_info", _P, _P)
 _sig("dnq_ham_timings", _P, _P)
 _sig("dnq_ham_copy_coo", _P, _I, _P, _P, _P, _P)

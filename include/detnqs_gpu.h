@@ -184,6 +184,12 @@ enum { DNQ_OPT_FORCE_WALK = 1, DNQ_OPT_ARENA_CHUNK = 2, DNQ_OPT_ARENA_CAP = 3,
        DNQ_OPT_SPMV_LANES = 4, DNQ_OPT_SPMV_UNROLL = 5, /* 6: unused */
        DNQ_OPT_PARTC_GROUPWALK = 7, DNQ_OPT_BUILD_F32 = 8 };
 int dnq_set_option(int option, int64_t value);
+/* The values set by dnq_set_option are process-wide defaults: every handle,
+ * batch and server takes a copy when it is created and keeps using its copy,
+ * so a later dnq_set_option does not reach objects that exist already.
+ * dnq_ham_set_option sets the H.psi shape (DNQ_OPT_SPMV_LANES,
+ * DNQ_OPT_SPMV_UNROLL) of one handle. */
+int dnq_ham_set_option(dnq_ham_t h, int option, int64_t value);
 /* sizes: [0] n_V, [1] nnz(H_VV), [2] n_P, [3] nnz(H_VP),
  *        [4] candidates examined, [5] device bytes held */
 int dnq_ham_info(dnq_ham_t h, int64_t* info6);

@@ -515,21 +515,56 @@ def test_spmv_every_lane_and_slot_count(core):
     x = S.normalized_psi(len(V), 5)
     ref = H.to_scipy(0).dot(x)
     scale = np.abs(ref).max()
+    for G in (4, 8, 16, 32):
+        H.set_option(N.OPT_SPMV_LANES, G)
+        first = {}
+        for U in (1, 2, 4):
+            H.set_option(N.OPT_SPMV_UNROLL, U)
+            for prec in (N.F64, N.F32):
+                y = H.spmv(x, precision=prec)
+                if prec in first:
+                    np.testing.assert_array_equal(y, first[prec])
+                else:
+                    first[prec] = y
+                tol = 1e-12 if prec == N.F64 else 1e-6
+                np.testing.assert_allclose(y, ref, rtol=0, atol=tol * scale)
+    H.close()
+
+
+def test_options_are_copied_per_handle(core):
+    """dnq_set_option changes the defaults of handles built afterwards only;
+    dnq_ham_set_option changes one handle's H.psi shape and no other's."""
+    from detnqs_b200 import device as D
+    from detnqs_b200 import native as N
+    sysm = S.make_system(18, 6, 6, 36, 23)
+    V = S.heat_bath_sample(sysm, 12000, 3)
+    ctx = core.IntCtx.from_arrays(18, sysm.h1e, sysm.eri, sysm.e_core)
+    ctx.hb_prepare(1e-15)
+    kw = dict(n_orb=18, policy=1, use_heatbath=True, eps1=1e-7, want_vp=False)
+    x = S.normalized_psi(len(V), 5)
+    A = D.build(ctx, V, **kw)
+    B = D.build(ctx, V, **kw)
+    y_auto = A.spmv(x)
+    B.set_option(N.OPT_SPMV_LANES, 4)
+    B.set_option(N.OPT_SPMV_UNROLL, 1)
+    y4 = B.spmv(x)
+    np.testing.assert_array_equal(A.spmv(x), y_auto)       # A untouched
+    # a default set afterwards reaches neither existing handle
+    N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 32))
     try:
-        for G in (4, 8, 16, 32):
-            N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, G))
-            first = {}
-            for U in (1, 2, 4):
-                N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, U))
-                for prec in (N.F64, N.F32):
-                    y = H.spmv(x, precision=prec)
-                    if prec in first:
-                        np.testing.assert_array_equal(y, first[prec])
-                    else:
-                        first[prec] = y
-                    tol = 1e-12 if prec == N.F64 else 1e-6
-                    np.testing.assert_allclose(y, ref, rtol=0, atol=tol * scale)
+        np.testing.assert_array_equal(A.spmv(x), y_auto)
+        np.testing.assert_array_equal(B.spmv(x), y4)
+        C = D.build(ctx, V, **kw)                           # takes the new default
+        C.set_option(N.OPT_SPMV_UNROLL, 1)
+        y32 = C.spmv(x)
+        A.set_option(N.OPT_SPMV_LANES, 32)
+        A.set_option(N.OPT_SPMV_UNROLL, 1)
+        np.testing.assert_array_equal(A.spmv(x), y32)
     finally:
         N.check(N.lib.dnq_set_option(N.OPT_SPMV_LANES, 0))
-        N.check(N.lib.dnq_set_option(N.OPT_SPMV_UNROLL, 0))
-    H.close()
+    with pytest.raises(ValueError, match="lanes per row"):
+        A.set_option(N.OPT_SPMV_LANES, 3)
+    with pytest.raises(ValueError, match="only the H.psi options"):
+        A.set_option(N.OPT_ARENA_CHUNK, 64)
+    for h in (A, B, C):
+        h.close()

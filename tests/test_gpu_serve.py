@@ -172,3 +172,28 @@ def test_errors_are_per_request(systems):
             srv.submit(V.ELOC, 7, np.ones(3))
         with pytest.raises(ValueError):
             srv.submit(V.ELOC, k, None)
+
+
+def test_wait_times_out_and_request_stays_pending(systems):
+    """dnq_server_wait returns DNQ_ERR_TIMEOUT while a request is held (the
+    server is paused) and the request completes afterwards, unchanged."""
+    from detnqs_b200 import native as N
+    from detnqs_b200 import serve as V
+    from detnqs_b200 import synthetic as S
+    items, ctxs = systems
+    (sysm, dets), ctx = items[0], ctxs[0]
+    psi = S.normalized_psi(len(dets), 77)
+    with V.Server(budget_bytes=8e9, build_slots=1) as srv:
+        k = srv.add_system(ctx, dets, sysm.n_orb, eps1=1e-7)
+        srv.wait(srv.submit(V.BUILD, k))
+        first = srv.wait(srv.submit(V.ELOC, k, psi, want_eloc=True, precision=N.F64))
+        srv.pause(True)
+        t = srv.submit(V.ELOC, k, psi, want_eloc=True, precision=N.F64)
+        with pytest.raises(N.DetnqsError) as e:
+            srv.wait(t, timeout=0.01)
+        assert e.value.code == N.ERR_TIMEOUT
+        srv.pause(False)
+        late = srv.wait(t)
+        st = srv.stats()
+    assert_same([first], [late])
+    assert st["failed"] == 0
