@@ -73,7 +73,7 @@ struct StrIndex {
     DBuf<u32> other32;   // the same in 32 bits (indices of systems with n_orb <= 32)
     DBuf<u32> idx;       // original position in V
     DBuf<u32> gid;       // group number of every sorted position
-    DBuf<u32> gstart;    // first sorted position of every group
+    DBuf<u32> gstart;    // first sorted position of every group, then n
     i64 ngroups = 0;
     DBuf<ulonglong2> slots;
     u64 mask = 0;
@@ -87,6 +87,11 @@ struct StrIndex {
     // it walks the groups of its singles (scanned members, groups tested by
     // presence rows, groups binary-searched, singles that are groups).
     DBuf<uint4> cost;
+    // Per group: the group of each single excitation of its string (~0u:
+    // not a string of the index), in the order of the part C walk (over the
+    // occupied orbitals, then the virtual ones), nbr_stride() entries per
+    // group.  Null when it would pass kNbrBytes.
+    DBuf<u32> nbr;
     StrMapView view() const { return StrMapView{slots.p, mask}; }
 };
 
@@ -107,14 +112,16 @@ __global__ void k_split_sorted(const ulonglong2* k, i64 n, u64* other, unsigned*
     }
 }
 
-// Start position of every group; gid arrives as the inclusive scan of the
-// head flags and leaves as the group number of every position.
+// Start position of every group and n after the last; gid arrives as the
+// inclusive scan of the head flags and leaves as the group number of every
+// position.
 __global__ void k_group_starts(const unsigned* head, u32* gid, i64 n, u32* gstart) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x) {
         const u32 g = gid[t] - 1;
         gid[t] = g;
         if (head[t]) gstart[g] = (u32)t;
+        if (t == n - 1) gstart[g + 1] = (u32)n;
     }
 }
 
@@ -214,7 +221,7 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cud
         DNQ_CHECK_LAUNCH();
     }
     X.gid.alloc(n, s);
-    X.gstart.alloc(n, s);
+    X.gstart.alloc(n + 1, s);
     DBuf<u32>& gid = X.gid;
     DBuf<u32>& gstart = X.gstart;
     prim::scan_inclusive<unsigned, u32>(head.p, gid.p, n, s);
@@ -254,6 +261,12 @@ void narrow_index(StrIndex& X, i64 n, cudaStream_t s) {
 }
 
 constexpr u32 kPresMin = 128;                    // presence rows for alpha groups longer than this
+constexpr i64 kNbrBytes = 1ll << 30;             // cap on the neighbour table of one index
+// Entries per group of a neighbour table: the most single excitations a
+// string of n_orb orbitals has, (n/2) (n - n/2).
+__host__ __device__ __forceinline__ i64 nbr_stride(int n_orb) {
+    return (i64)(n_orb / 2) * (n_orb - n_orb / 2);
+}
 constexpr i64 kPresBytes = 256ll << 20;          // cap on the presence rows of one index
 
 __global__ void k_long_groups(const u32* gstart, i64 ngroups, i64 n, u32 thr, u32* flag,
@@ -361,10 +374,10 @@ __device__ __forceinline__ double eri(const double* E, int p, int q, int r, int 
 // of that string and scans it, tests it through presence rows or binary-
 // searches it (the same classification as part_c, with the other string's
 // single count taken from the first determinant: every string of a space
-// has the same electron count).
-__global__ void k_group_cost(const u64* V, const u32* idx, const u32* gstart, i64 ngroups,
-                             int major, int n_orb, StrMapView xmap, int has_pres, u32 pres_min,
-                             u32 big_group, uint4* cost) {
+// has the same electron count).  Writes the neighbour table when nbr is set.
+__global__ void k_group_cost(const u64* V, const u32* idx, const u32* gstart, const u32* gid,
+                             i64 ngroups, int major, int n_orb, StrMapView xmap, int has_pres,
+                             u32 pres_min, u32 big_group, uint4* cost, u32* nbr) {
     __shared__ u8 lists[kWS][128];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     u8* occ = lists[w];
@@ -386,7 +399,9 @@ __global__ void k_group_cost(const u64* V, const u32* idx, const u32* gstart, i6
         u32 scan = 0, pb = 0, bg = 0, ix = 0;
         for (int i = lane; i < ns; i += 32) {
             u32 gs = 0, gl = 0;
-            if (!xmap.find(x ^ (1ull << occ[i / nvx]) ^ (1ull << vir[i % nvx]), gs, gl)) continue;
+            const bool f = xmap.find(x ^ (1ull << occ[i / nvx]) ^ (1ull << vir[i % nvx]), gs, gl);
+            if (nbr) nbr[g * nbr_stride(n_orb) + i] = f ? __ldg(&gid[gs]) : 0xffffffffu;
+            if (!f) continue;
             ++ix;
             const bool pbig = usep && gl > pres_min && gl > (u32)nyv;
             if (pbig) ++pb;
@@ -405,14 +420,17 @@ __global__ void k_group_cost(const u64* V, const u32* idx, const u32* gstart, i6
     }
 }
 
+// Part C costs of every group, and its neighbour table when that fits
+// kNbrBytes.
 void build_group_cost(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cudaStream_t s) {
     if (n == 0 || X.ngroups == 0) return;
     X.cost.alloc(X.ngroups, s);
+    const i64 st = nbr_stride(n_orb);
+    if (X.ngroups * st * (i64)sizeof(u32) <= kNbrBytes) X.nbr.alloc(X.ngroups * st, s);
     const i64 blocks = std::min<i64>((X.ngroups + kWS - 1) / kWS, 65535);
-    k_group_cost<<<(unsigned)blocks, kWS * 32, 0, s>>>(V, X.idx.p, X.gstart.p, X.ngroups, major,
-                                                       n_orb, X.view(), X.pres.p != nullptr,
-                                                       X.pres.p ? X.pres_min : 0xffffffffu,
-                                                       kBigGroup, X.cost.p);
+    k_group_cost<<<(unsigned)blocks, kWS * 32, 0, s>>>(
+        V, X.idx.p, X.gstart.p, X.gid.p, X.ngroups, major, n_orb, X.view(), X.pres.p != nullptr,
+        X.pres.p ? X.pres_min : 0xffffffffu, kBigGroup, X.cost.p, X.nbr.p);
     DNQ_CHECK_LAUNCH();
 }
 
@@ -451,6 +469,12 @@ struct VVParams {
     u32 pres_min_b;
     const uint4* a_cost;   // part C costs per alpha / beta group (null: alpha-major)
     const uint4* b_cost;
+    // neighbour tables (group of every single of a group's string; null: hash
+    // lookups) and group starts with n after the last group
+    const u32* a_nbr;
+    const u32* b_nbr;
+    const u32* a_gstart;
+    const u32* b_gstart;
 };
 
 // Where rows are written.  Single pass: rows appended to warp-private
@@ -836,11 +860,13 @@ __device__ __forceinline__ void scan_same(Q& q, const W* other, W x, u32 st, u32
 // hit when its string differs from y in one orbital pair.  Its tag holds
 // the kind and x's hole and particle.  bm selects beta-major; the
 // direction's arrays are read from P where they are used (fewer live
-// registers than passing them in).
+// registers than passing them in).  gx and gy are the groups of x and y in
+// their indices (~0u: unknown); with the neighbour tables the groups of
+// their singles are read from the tables, else looked up by string.
 template <class W, class Q>
 __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
                                        unsigned long long& tests, bool bm, u64 a, u64 b, int na,
-                                       int nva, int nb, int nvb) {
+                                       int nva, int nb, int nvb, u32 gx, u32 gy) {
     const int lane = threadIdx.x & 31;
     const u64 x = bm ? b : a, y = bm ? a : b;
     const u8* occx = bm ? S.occb : S.occa;
@@ -858,12 +884,22 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
     int nys = -1;   // indexed y singles listed in S (-1: not yet)
     for (int s0 = 0; s0 < nsx; s0 += 32) {
         const int sidx = s0 + lane;
-        u32 gs = 0, gl = 0;
+        u32 gs = 0, gl = 0, gg = 0xffffffffu;
         int hh = 0, pp = 0;
         if (sidx < nsx) {
             hh = occx[sidx / nvx];
             pp = virx[sidx % nvx];
-            if (!(bm ? P.bmap : P.amap).find(x ^ (1ull << hh) ^ (1ull << pp), gs, gl)) gl = 0;
+            const u32* nbt = bm ? P.b_nbr : P.a_nbr;
+            if (nbt && gx != 0xffffffffu) {
+                gg = __ldg(&nbt[(i64)gx * nbr_stride(P.n_orb) + sidx]);
+                if (gg != 0xffffffffu) {
+                    const u32* gst = bm ? P.b_gstart : P.a_gstart;
+                    gs = __ldg(&gst[gg]);
+                    gl = __ldg(&gst[gg + 1]) - gs;
+                }
+            } else if (!(bm ? P.bmap : P.amap).find(x ^ (1ull << hh) ^ (1ull << pp), gs, gl)) {
+                gl = 0;
+            }
         }
         // presence rows for long groups (when the row's y singles fit the
         // warp's list), binary search above big_group otherwise, else a scan
@@ -871,7 +907,10 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
         const bool big = !pbig && gl > P.big_group;
         const bool small = gl != 0 && !pbig && !big;
         const u32 prw =
-            pbig ? __ldg(&(bm ? P.b_prow : P.a_prow)[__ldg(&(bm ? P.b_gid : P.a_gid)[gs])]) : 0u;
+            pbig ? __ldg(&(bm ? P.b_prow : P.a_prow)[gg != 0xffffffffu
+                                                          ? gg
+                                                          : __ldg(&(bm ? P.b_gid : P.a_gid)[gs])])
+                 : 0u;
         if (!P.c_groupwalk) {
             part_c_packed(q, S, xo, yw, tests, gs, small ? gl : 0u, hh, pp, kind);
         } else {
@@ -912,12 +951,19 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
                 u16 e = 0;
                 if (qi < nyv) {
                     const int hb = occy[qi / nvy], pb = viry[qi % nvy];
-                    u32 bst = 0, bln = 0;
-                    if ((bm ? P.amap : P.bmap).find(y ^ (1ull << hb) ^ (1ull << pb), bst, bln)) {
-                        f = true;
-                        bid = __ldg(&(bm ? P.a_gid : P.b_gid)[bst]);
-                        e = (u16)(hb | (pb << 8));
+                    const u32* nbt = bm ? P.a_nbr : P.b_nbr;
+                    if (nbt && gy != 0xffffffffu) {
+                        bid = __ldg(&nbt[(i64)gy * nbr_stride(P.n_orb) + qi]);
+                        f = bid != 0xffffffffu;
+                    } else {
+                        u32 bst = 0, bln = 0;
+                        if ((bm ? P.amap : P.bmap).find(y ^ (1ull << hb) ^ (1ull << pb), bst,
+                                                        bln)) {
+                            f = true;
+                            bid = __ldg(&(bm ? P.a_gid : P.b_gid)[bst]);
+                        }
                     }
+                    if (f) e = (u16)(hb | (pb << 8));
                 }
                 const unsigned fm = __ballot_sync(0xffffffffu, f);
                 if (f) {
@@ -1013,6 +1059,8 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     u32 st = 0, ln = 0;
     if (lane == 0 && !P.bmap.find(b, st, ln)) ln = 0;
     if (lane == 1 && !P.amap.find(a, st, ln)) ln = 0;
+    u32 grp = 0xffffffffu;   // lane 0: the row's beta group, lane 1: its alpha group
+    if (lane < 2 && ln) grp = __ldg(&(lane == 0 ? P.b_gid : P.a_gid)[st]);
     // ---- part A: same beta string (alpha singles and doubles)
     u32 gst = __shfl_sync(0xffffffffu, st, 0), gln = __shfl_sync(0xffffffffu, ln, 0);
     tests += gln;
@@ -1034,8 +1082,8 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     bool bm = false;
     if (P.a_cost) {   // the costs of the row's two groups (found for parts A and B)
         uint4 c = make_uint4(0u, 0u, 0u, 0u);
-        if (lane == 0 && ln) c = __ldg(&P.b_cost[__ldg(&P.b_gid[st])]);
-        if (lane == 1 && ln) c = __ldg(&P.a_cost[__ldg(&P.a_gid[st])]);
+        if (lane == 0 && ln) c = __ldg(&P.b_cost[grp]);
+        if (lane == 1 && ln) c = __ldg(&P.a_cost[grp]);
         const uint4 cb = make_uint4(__shfl_sync(0xffffffffu, c.x, 0),
                                     __shfl_sync(0xffffffffu, c.y, 0),
                                     __shfl_sync(0xffffffffu, c.z, 0),
@@ -1050,7 +1098,8 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     }
     // one call site for both directions: a second inlined copy of the walk
     // would not fit the instruction cache
-    part_c<W>(P, S, q, tests, bm, a, b, na, nva, nb, nvb);
+    part_c<W>(P, S, q, tests, bm, a, b, na, nva, nb, nvb,
+              __shfl_sync(0xffffffffu, grp, bm ? 0 : 1), __shfl_sync(0xffffffffu, grp, bm ? 1 : 0));
 }
 
 // A member's tag, given as a value or as a function read only on a hit.
@@ -1803,6 +1852,10 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
     P.pres_min_b = B.pres.p ? B.pres_min : 0xffffffffu;
     P.a_cost = A.cost.p;
     P.b_cost = B.cost.p;
+    P.a_nbr = A.nbr.p;
+    P.b_nbr = B.nbr.p;
+    P.a_gstart = A.gstart.p;
+    P.b_gstart = B.gstart.p;
     return P;
 }
 
