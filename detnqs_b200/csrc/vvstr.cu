@@ -500,6 +500,7 @@ struct Arena {
     u32* big_len;                     // their member counts
     int* n_big;
     int* next_row;
+    const u32* order;                 // walk order of the rows (null: 0, 1, ...)
     unsigned long long* n_test;
     unsigned long long* n_hit;        // members recorded by k_vv_arena (optional)
     // single excitations recorded by k_vv_arena in warp-private slices of
@@ -1044,6 +1045,15 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
     }
 }
 
+// Part C direction of a row from the costs of its alpha group (ca) and beta
+// group (cb) and the single counts of its two strings: beta-major when that
+// walk tests fewer members.
+__host__ __device__ __forceinline__ bool row_bm(uint4 ca, uint4 cb, int nsa, int nsb) {
+    const u64 cost_a = ca.x + (u64)ca.y * cb.w + (u64)ca.z * (u32)nsb;
+    const u64 cost_b = cb.x + (u64)cb.y * ca.w + (u64)cb.z * (u32)nsa;
+    return cost_b < cost_a;
+}
+
 // The members of row r = (a, b) in their fixed order: the diagonal, then
 // parts A, B and C.  q.push(hit, position, tag) is warp-collective, once
 // per step of 32; q.sync() follows every group of at most kScanU steps.
@@ -1092,9 +1102,7 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
                                     __shfl_sync(0xffffffffu, c.y, 1),
                                     __shfl_sync(0xffffffffu, c.z, 1),
                                     __shfl_sync(0xffffffffu, c.w, 1));
-        const u64 cost_a = ca.x + (u64)ca.y * cb.w + (u64)ca.z * (u32)(nb * nvb);
-        const u64 cost_b = cb.x + (u64)cb.y * ca.w + (u64)cb.z * (u32)(na * nva);
-        bm = cost_b < cost_a;
+        bm = row_bm(ca, cb, na * nva, nb * nvb);
     }
     // one call site for both directions: a second inlined copy of the walk
     // would not fit the instruction cache
@@ -1240,6 +1248,10 @@ __device__ __forceinline__ int next_row(int* ctr) {
     return __shfl_sync(0xffffffffu, r, 0);
 }
 
+// Rows handed to a walking warp at a time: consecutive rows of the walk
+// order share their string groups, which then stay in the SM's L1.
+constexpr int kRowRun = 4;
+
 // Word type of the scans: u32 / u64 for every row, or PerRowW to pick per
 // row (batches mixing systems of at most and of more than 32 orbitals).
 struct PerRowW {};
@@ -1276,9 +1288,17 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint4* slice = A.sgl ? A.sgl + (i64)wid * A.sgl_slice : nullptr;
     u32 sgn = 0;
+    int t = 0, t_end = 0;   // this warp's run of rows in the walk order
     for (;;) {
-        const int g = next_row(A.next_row);
-        if (g >= nrows) break;
+        if (t == t_end) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(A.next_row, kRowRun);
+            t = __shfl_sync(0xffffffffu, base, 0);
+            if (t >= nrows) break;
+            t_end = (int)std::min<i64>((i64)t + kRowRun, nrows);
+        }
+        const int g = A.order ? (int)__ldg(&A.order[t]) : t;
+        ++t;
         if (*(volatile int*)A.overflow) continue;
         int r;
         u32 cb;
@@ -1661,6 +1681,74 @@ int vv_grid(int device) {
     return std::max(1, per_sm) * sm_count(device);
 }
 
+// Walk order of a single system's rows: rows walking part C alpha-major in
+// the alpha-sorted order, then the beta-major ones in the beta-sorted order,
+// so that a run of rows shares its groups.  Built without a host sync.
+__global__ void k_row_group(const u32* idx, const u32* gid, i64 n, u32* row_gid) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x)
+        row_gid[idx[t]] = gid[t];
+}
+
+__global__ void k_row_dir(const u64* V, i64 n, int n_orb, const u32* rga, const u32* rgb,
+                          const uint4* a_cost, const uint4* b_cost, u32* dir) {
+    const u64 all = low_mask(n_orb);
+    for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < n;
+         g += (i64)gridDim.x * blockDim.x) {
+        const u64 a = V[2 * g], b = V[2 * g + 1];
+        const int nsa = __popcll(a) * __popcll(~a & all), nsb = __popcll(b) * __popcll(~b & all);
+        dir[g] = row_bm(a_cost[rga[g]], b_cost[rgb[g]], nsa, nsb) ? 1u : 0u;
+    }
+}
+
+// flag[t] of sorted position t: its row walks in this direction (want = 0:
+// alpha-major, 1: beta-major); flag[n] = 0 so the scan ends with the count.
+__global__ void k_dir_flags(const u32* idx, const u32* dir, i64 n, u32 want, u32* flag) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t <= n;
+         t += (i64)gridDim.x * blockDim.x)
+        flag[t] = t < n && dir[idx[t]] == want ? 1u : 0u;
+}
+
+__global__ void k_order_scatter(const u32* a_idx, const u32* fa, const u32* pa, const u32* b_idx,
+                                const u32* fb, const u32* pb, i64 n, u32* order) {
+    for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
+         t += (i64)gridDim.x * blockDim.x) {
+        if (fa[t]) order[pa[t]] = a_idx[t];
+        if (fb[t]) order[pa[n] + pb[t]] = b_idx[t];
+    }
+}
+
+void build_row_order(const StrIndex& A, const StrIndex& B, const u64* V, i64 n, int n_orb,
+                     DBuf<u32>& order, cudaStream_t s) {
+    if (n == 0 || !A.cost.p || !B.cost.p) return;
+    DBuf<u32> rga(n, s), rgb(n, s), dir(n, s), fa(n + 1, s), fb(n + 1, s), pa(n + 1, s),
+        pb(n + 1, s);
+    order.alloc(n, s);
+    k_row_group<<<gsz(n), 256, 0, s>>>(A.idx.p, A.gid.p, n, rga.p);
+    DNQ_CHECK_LAUNCH();
+    k_row_group<<<gsz(n), 256, 0, s>>>(B.idx.p, B.gid.p, n, rgb.p);
+    DNQ_CHECK_LAUNCH();
+    k_row_dir<<<gsz(n), 256, 0, s>>>(V, n, n_orb, rga.p, rgb.p, A.cost.p, B.cost.p, dir.p);
+    DNQ_CHECK_LAUNCH();
+    k_dir_flags<<<gsz(n + 1), 256, 0, s>>>(A.idx.p, dir.p, n, 0u, fa.p);
+    DNQ_CHECK_LAUNCH();
+    k_dir_flags<<<gsz(n + 1), 256, 0, s>>>(B.idx.p, dir.p, n, 1u, fb.p);
+    DNQ_CHECK_LAUNCH();
+    prim::scan<u32, u32, false>(fa.p, pa.p, n + 1, s);
+    prim::scan<u32, u32, false>(fb.p, pb.p, n + 1, s);
+    k_order_scatter<<<gsz(n), 256, 0, s>>>(A.idx.p, fa.p, pa.p, B.idx.p, fb.p, pb.p, n, order.p);
+    DNQ_CHECK_LAUNCH();
+}
+
+// Grid of k_vv_eval: as many blocks as fit (it holds fewer registers than
+// the walk, and more warps in flight hide more of its gather latency).
+template <class Loc>
+int eval_grid(int device) {
+    int per_sm = 0;
+    DNQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vv_eval<Loc>, kWS * 32, 0));
+    return std::max(1, per_sm) * sm_count(device);
+}
+
 // scan: 0 = 64-bit strings, 1 = 32-bit, 2 = chosen per row.
 template <class Loc>
 void launch_walk(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s) {
@@ -1686,7 +1774,8 @@ void launch_big(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
            const Options& opt, double* t_gen, double* t_scan, double* t_compact,
-           i64* hits_out = nullptr, int scan = 0, DBuf<double>* dg = nullptr) {
+           i64* hits_out = nullptr, int scan = 0, DBuf<double>* dg = nullptr,
+           const u32* order = nullptr) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
@@ -1726,6 +1815,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.big_len = blen.p;
     A.n_big = nbig.p;
     A.next_row = next.p;
+    A.order = order;
     A.n_test = nt.p;
     A.n_hit = nh.p;
     A.sgl = sgl.p;
@@ -1745,7 +1835,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     launch_walk<Loc>(scan, grid, L, A, s);
     k_vv_singles<Loc><<<grid, 256, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    k_vv_eval<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
+    k_vv_eval<Loc><<<eval_grid<Loc>(device), kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     launch_big<Loc>(scan, grid, L, A, s);
     DNQ_CHECK_LAUNCH();
@@ -1883,13 +1973,15 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
         narrow_index(A, n, s);
         narrow_index(B, n, s);
     }
+    DBuf<u32> order;
+    build_row_order(A, B, V, n, n_orb, order, s);
     DNQ_CUDA(cudaEventRecord(e1, s));
     OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, diag, A, B, H->opt)};
     double tg = 0, tsc = 0, tc = 0;
     i64 hits = 0;
     H->candidates =
         run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, H->opt, &tg, &tsc, &tc,
-               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr);
+               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr, order.p);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);
@@ -2230,7 +2322,7 @@ void enqueue_step(dnq_batch_s* b, int precision, cudaStream_t s, cudaEvent_t* ev
     launch_walk<ManySys>(b->scan, grid, L, A, s);
     k_vv_singles<ManySys><<<grid, 256, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
-    k_vv_eval<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
+    k_vv_eval<ManySys><<<eval_grid<ManySys>(b->device), kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     launch_big<ManySys>(b->scan, grid, L, A, s);
     k_vv_eval_long<ManySys><<<grid, kWS * 32, 0, s>>>(L, A);
