@@ -1071,15 +1071,16 @@ __device__ __forceinline__ void walk_row(const VVParams& P, int r, u64 a, u64 b,
     if (lane == 1 && !P.amap.find(a, st, ln)) ln = 0;
     u32 grp = 0xffffffffu;   // lane 0: the row's beta group, lane 1: its alpha group
     if (lane < 2 && ln) grp = __ldg(&(lane == 0 ? P.b_gid : P.a_gid)[st]);
-    // ---- part A: same beta string (alpha singles and doubles)
-    u32 gst = __shfl_sync(0xffffffffu, st, 0), gln = __shfl_sync(0xffffffffu, ln, 0);
-    tests += gln;
-    scan_same(q, b_others<W>(P), aw, gst, gln, kHitA);
-    // ---- part B: same alpha string (beta singles and doubles)
-    gst = __shfl_sync(0xffffffffu, st, 1);
-    gln = __shfl_sync(0xffffffffu, ln, 1);
-    tests += gln;
-    scan_same(q, ao, bw, gst, gln, kHitB);
+    // ---- part A (same beta string: alpha singles and doubles), then part B
+    // (same alpha string: beta singles and doubles), from one call site: the
+    // walk's speed depends on its code fitting the instruction cache
+#pragma unroll 1
+    for (int part = 0; part < 2; ++part) {
+        const u32 gst = __shfl_sync(0xffffffffu, st, part);
+        const u32 gln = __shfl_sync(0xffffffffu, ln, part);
+        tests += gln;
+        scan_same(q, part ? ao : b_others<W>(P), part ? bw : aw, gst, gln, part ? kHitB : kHitA);
+    }
     // ---- part C: alpha single x beta single.  Either direction finds the
     // same members: the groups of the row's alpha singles a' tested for a
     // beta single of b (alpha-major), or the groups of its beta singles b'
