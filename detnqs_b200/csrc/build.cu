@@ -239,13 +239,13 @@ __global__ void k_val_f32_tail(const double* v, i64 n, float* o) {
 
 // Diagonal entry of each row (column order not assumed): moved out of the
 // FP32 copy into the FP64 vector (0 when the row has none).  Warp per row.
-__global__ void k_split_diag(const i64* rowptr, const u32* col, const double* val, i64 nr,
-                             float* out, double* dout) {
+__global__ void k_split_diag(const i64* rs, const i64* re, const u32* col, const double* val,
+                             i64 nr, float* out, double* dout) {
     const int lane = threadIdx.x & 31;
     const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
     for (i64 r = gw; r < nr; r += nw) {
-        const i64 b = rowptr[r], e = rowptr[r + 1];
+        const i64 b = rs[r], e = re[r];
         double d = 0.0;
         for (i64 k0 = b; k0 < e; k0 += 32) {
             const i64 k = k0 + lane;
@@ -291,6 +291,7 @@ void ensure_sorted(Csr& m, cudaStream_t s) {
 
 
 void sort_rows(Csr& m, cudaStream_t s) {
+    ensure_compact(m, s);
     m.sorted = true;
     m.val32.release();   // an FP32 copy follows the old order: rebuilt on next use
     if (m.nnz == 0 || m.nr == 0) return;
@@ -306,38 +307,25 @@ void launch_f32_split(const Csr& m, float* val32, double* diag_out, cudaStream_t
     int dev = 0;
     DNQ_CUDA(cudaGetDevice(&dev));
     const int sms = sm_count(dev);
-    if (m.nnz) {
-        k_vals_f32<<<sms * 8, 256, 0, s>>>((const double2*)m.val.p, m.nnz / 2, (float2*)val32);
+    const i64 len = m.span();   // every slot of an arena-form block (free ones too)
+    if (len) {
+        k_vals_f32<<<sms * 8, 256, 0, s>>>((const double2*)m.val.p, len / 2, (float2*)val32);
         DNQ_CHECK_LAUNCH();
-        k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, m.nnz, val32);
+        k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, len, val32);
         DNQ_CHECK_LAUNCH();
     }
     if (m.nr) {
-        k_split_diag<<<sms * 8, 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr, val32, diag_out);
+        k_split_diag<<<sms * 8, 256, 0, s>>>(m.row_start(), m.row_end(), m.col.p, m.val.p, m.nr,
+                                             val32, diag_out);
         DNQ_CHECK_LAUNCH();
     }
 }
 
 void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out) {
-    m.val32.alloc(m.nnz, s);
+    m.val32.alloc(m.val.n, s);
     if (diag_out) diag_out->alloc(m.nr, s);
     if (m.nr == 0) return;
-    if (m.nnz) {
-        int dev = 0;
-        DNQ_CUDA(cudaGetDevice(&dev));
-        const int grid = sm_count(dev) * 8;
-        k_vals_f32<<<grid, 256, 0, s>>>((const double2*)m.val.p, m.nnz / 2, (float2*)m.val32.p);
-        DNQ_CHECK_LAUNCH();
-        k_val_f32_tail<<<1, 32, 0, s>>>(m.val.p, m.nnz, m.val32.p);
-        DNQ_CHECK_LAUNCH();
-    }
-    {
-        int dev = 0;
-        DNQ_CUDA(cudaGetDevice(&dev));
-        k_split_diag<<<sm_count(dev) * 8, 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, m.nr,
-                                                       m.val32.p, diag_out ? diag_out->p : nullptr);
-    }
-    DNQ_CHECK_LAUNCH();
+    launch_f32_split(m, m.val32.p, diag_out ? diag_out->p : nullptr, s);
 }
 
 // Validate and stage the determinants; throws on orbitals >= n_orb.

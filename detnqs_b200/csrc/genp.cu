@@ -771,6 +771,7 @@ int dnq_conn_copy(dnq_ham_t h, int32_t* offsets, uint64_t* dets, double* values,
     require(h != nullptr, DNQ_ERR_INVALID, "null argument");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
+    ensure_compact(h->vv, s);
     if (offsets) {
         std::vector<i64> rp(h->n_v + 1, 0);
         if (h->vv.rowptr.p)

@@ -10,17 +10,32 @@
 
 namespace dnq {
 
+// Compressed rows.  Standard form: row r is [rowptr[r], rowptr[r + 1]) of
+// col / val.  Arena form (a V->V build leaves its rows where the build
+// wrote them): row r is [rowptr[r], rowend[r]), and col / val hold free
+// slots between rows; ensure_compact turns it into the standard form.  The
+// H.psi kernels read either through row_start() / row_end(), with span()
+// (the array length) bounding their vector loads.
 struct Csr {
     DBuf<i64> rowptr;
+    DBuf<i64> rowend;    // arena form only
     DBuf<u32> col;
     DBuf<double> val;
-    DBuf<float> val32;   // optional FP32 off-diagonal copy
+    DBuf<float> val32;   // optional FP32 off-diagonal copy (ready when as long as val)
     i64 nr = 0, nc = 0, nnz = 0;
     bool sorted = true;   // columns ascending inside each row
+    bool arena = false;
+    const i64* row_start() const { return rowptr.p; }
+    const i64* row_end() const { return arena ? rowend.p : rowptr.p + 1; }
+    i64 span() const { return (i64)col.n; }
+    bool f32_ready() const { return val32.n == val.n; }
     size_t bytes() const {
-        return rowptr.bytes() + col.bytes() + val.bytes() + val32.bytes();
+        return rowptr.bytes() + rowend.bytes() + col.bytes() + val.bytes() + val32.bytes();
     }
 };
+
+// Standard form of a block in arena form (no-op otherwise); drops nothing.
+void ensure_compact(Csr& m, cudaStream_t s);
 
 
 }  // namespace dnq
@@ -57,14 +72,15 @@ void ensure_sorted(Csr& m, cudaStream_t s);
 // One operator of a grouped H.psi launch: y = M x (+ diag .* x when diag is
 // given).  val / xg are double (FP64) or float (FP32 values and x).
 struct SpmvDesc {
-    const i64* rp;
+    const i64* rp;       // row starts
+    const i64* re;       // row ends
     const u32* col;
     const void* val;
     const void* xg;
     const double* diag;
     const double* x;
     double* y;
-    i64 nr, nnz;
+    i64 nr, nnz;         // rows; length of col / val (bounds the vector loads)
 };
 // Lanes per row and slots per lane the H.psi kernels use for m.
 void spmv_shape(const Options& o, const Csr& m, int& G, int& U);

@@ -912,6 +912,7 @@ int dnq_ham_eff_from(dnq_ham_t proxy, const double* h_pp, double e_ref, int reg_
     require(proxy->n_p == 0 || h_pp, DNQ_ERR_INVALID, "null h_pp_diag");
     DeviceGuard g(proxy->device);
     cudaStream_t s = (cudaStream_t)stream;
+    ensure_compact(proxy->vv, s);
     std::unique_ptr<dnq_ham_s> H(new dnq_ham_s);
     if (proxy->n_p == 0 || proxy->vp.nnz == 0 && proxy->n_p == 0) {
         // empty P: H_eff is H_VV itself

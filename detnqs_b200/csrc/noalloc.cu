@@ -98,7 +98,7 @@ int dnq_ham_local_energy_noalloc(dnq_ham_t h, const double* x, double* eloc, dou
                 "x and eloc must not overlap: eloc receives H x while x is read");
     }
     if (precision == DNQ_F32)
-        require(h->vv.val32.n == (size_t)h->vv.nnz && h->diag_op.n == (size_t)h->n_v,
+        require(h->vv.f32_ready() && h->diag_op.n == (size_t)h->n_v,
                 DNQ_ERR_INVALID,
                 "FP32 values not prepared: run one FP32 dnq_ham_spmv or "
                 "dnq_ham_local_energy on this handle first");

@@ -179,6 +179,7 @@ int dnq_ham_symmetrize(dnq_ham_t h, void* stream, dnq_ham_t* out) {
     H->device = h->device;
     H->stream = s;
     H->n_v = h->n_v;
+    ensure_compact(h->vv, s);
     symmetrize_csr(h->vv, H->vv, s);
     *out = H.release();
     DNQ_API_END
@@ -210,7 +211,7 @@ int dnq_ham_proxy_spmv(dnq_ham_t h, const double* xv, const double* xp, const do
         DBuf<float> xv32(nv, s), xp32(np, s);
         to_f32(xvd.p, nv, xv32.p, s);
         to_f32(xpd.p, np, xp32.p, s);
-        if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
+        if (!h->vv.f32_ready() || h->diag_op.n != (size_t)h->n_v)
             make_f32(h->vv, s, &h->diag_op);
         ensure_f32_all(h->vp, s);
         spmv_block(h, h->vp, xpd.p, tmp.p, nullptr, DNQ_F32, s, xp32.p, nullptr);

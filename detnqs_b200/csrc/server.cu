@@ -355,7 +355,8 @@ void launch_group(dnq_server_s* S) {
         int G = 4, U = 1;
         spmv_shape(h->opt, h->vv, G, U);
         SpmvDesc d{};
-        d.rp = h->vv.rowptr.p;
+        d.rp = h->vv.row_start();
+        d.re = h->vv.row_end();
         d.col = h->vv.col.p;
         d.val = f32 ? (const void*)h->vv.val32.p : (const void*)h->vv.val.p;
         d.xg = f32 ? (const void*)(S->gx32.p + o) : (const void*)(S->gx.p + o);
@@ -363,7 +364,7 @@ void launch_group(dnq_server_s* S) {
         d.x = S->gx.p + o;
         d.y = S->gy.p + o;
         d.nr = h->n_v;
-        d.nnz = h->vv.nnz;
+        d.nnz = h->vv.span();
         cls[{f32 ? DNQ_F32 : DNQ_F64, G, U}].push_back(d);
     }
     size_t bytes = take * sizeof(EnergyDesc);
@@ -479,7 +480,7 @@ void worker(dnq_server_s* S, int slot) {
         i64 bytes = 0;
         if (rc == DNQ_OK) {
             try {
-                if (H->vv.nnz > 0 && (H->vv.val32.n != (size_t)H->vv.nnz ||
+                if (H->vv.nnz > 0 && (!H->vv.f32_ready() ||
                                       H->diag_op.n != (size_t)H->n_v))
                     make_f32(H->vv, s, &H->diag_op);
                 DNQ_CUDA(cudaStreamSynchronize(s));

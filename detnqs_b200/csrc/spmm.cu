@@ -92,7 +92,8 @@ struct Gather<2, double> {
 // columns [j0, j0 + K / min(K, G)).
 template <int G, int U, int K, class T, class Acc>
 __global__ void __launch_bounds__(256)
-k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restrict__ val,
+k_spmm(const i64* __restrict__ rs, const i64* __restrict__ re, const u32* __restrict__ col,
+       const T* __restrict__ val,
        const T* __restrict__ Xg, const double* __restrict__ diag, const double* __restrict__ X,
        int ldx, int kx, i64 nr, i64 nnz, double* __restrict__ Y, int ldy) {
     const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
@@ -104,7 +105,7 @@ k_spmm(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
         const i64 r = gid + it * ngroups;
         Acc acc[K];
         if (r < nr) {
-            const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
+            const i64 b = __ldg(&rs[r]), e = __ldg(&re[r]);
             for (i64 k0 = (b & ~3ll) + 4 * sub; k0 < e; k0 += 4 * G * U) {
                 u32 c[U][4];
                 T v[U][4];
@@ -271,8 +272,8 @@ template <int G, int U, int K, class T, class Acc>
 void launch_spmm(const Csr& m, const T* val, const T* Xg, const double* diag, const double* X,
                  int ldx, int kx, double* Y, int ldy, int device, cudaStream_t s) {
     auto kern = k_spmm<G, U, K, T, Acc>;
-    kern<<<blocks_of(kern, device), 256, 0, s>>>(m.rowptr.p, m.col.p, val, Xg, diag, X, ldx, kx,
-                                                 m.nr, m.nnz, Y, ldy);
+    kern<<<blocks_of(kern, device), 256, 0, s>>>(m.row_start(), m.row_end(), m.col.p, val, Xg,
+                                                 diag, X, ldx, kx, m.nr, m.span(), Y, ldy);
     DNQ_CHECK_LAUNCH();
 }
 

@@ -30,12 +30,13 @@ namespace {
 //   T = float : y_r = Kahan sum of val32 * x32 + diag_r x_r (FP32
 //               off-diagonal values, FP64 diagonal term)
 template <int G, int U, class T, class Acc>
-__device__ __forceinline__ Acc row_acc(const i64* __restrict__ rp, const u32* __restrict__ col,
-                                       const T* __restrict__ val, const T* __restrict__ xg,
-                                       i64 r, bool valid, i64 nnz, int sub) {
+__device__ __forceinline__ Acc row_acc(const i64* __restrict__ rs, const i64* __restrict__ re,
+                                       const u32* __restrict__ col, const T* __restrict__ val,
+                                       const T* __restrict__ xg, i64 r, bool valid, i64 nnz,
+                                       int sub) {
     Acc acc;
     if (valid) {
-        const i64 b = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
+        const i64 b = __ldg(&rs[r]), e = __ldg(&re[r]);
         for (i64 k0 = (b & ~3ll) + 4 * sub; k0 < e; k0 += 4 * G * U) {
             u32 c[U][4];
             T v[U][4];
@@ -79,8 +80,8 @@ __device__ __forceinline__ Acc row_acc(const i64* __restrict__ rp, const u32* __
 
 template <int G, int U, class T, class Acc>
 __global__ void __launch_bounds__(256)
-k_spmv(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restrict__ val,
-       const T* __restrict__ xg, const double* __restrict__ diag,
+k_spmv(const i64* __restrict__ rs, const i64* __restrict__ re, const u32* __restrict__ col,
+       const T* __restrict__ val, const T* __restrict__ xg, const double* __restrict__ diag,
        const double* __restrict__ x, i64 nr, i64 nnz, double* __restrict__ y,
        const double* __restrict__ yadd) {
     const i64 gid = (blockIdx.x * (i64)blockDim.x + threadIdx.x) / G;
@@ -89,7 +90,7 @@ k_spmv(const i64* __restrict__ rp, const u32* __restrict__ col, const T* __restr
     const i64 rounds = (nr + ngroups - 1) / ngroups;
     for (i64 it = 0; it < rounds; ++it) {
         const i64 r = gid + it * ngroups;
-        const Acc acc = row_acc<G, U, T, Acc>(rp, col, val, xg, r, r < nr, nnz, sub);
+        const Acc acc = row_acc<G, U, T, Acc>(rs, re, col, val, xg, r, r < nr, nnz, sub);
         if (sub == 0 && r < nr) {
             double v = acc.value();
             if (diag) v += diag[r] * x[r];
@@ -112,7 +113,8 @@ __global__ void __launch_bounds__(256) k_spmv_grouped(const SpmvDesc* __restrict
     const i64 rounds = (d.nr + ngroups - 1) / ngroups;
     for (i64 it = 0; it < rounds; ++it) {
         const i64 r = gid + it * ngroups;
-        const Acc acc = row_acc<G, U, T, Acc>(d.rp, d.col, val, xg, r, r < d.nr, d.nnz, sub);
+        const Acc acc =
+            row_acc<G, U, T, Acc>(d.rp, d.re, d.col, val, xg, r, r < d.nr, d.nnz, sub);
         if (sub == 0 && r < d.nr) {
             double v = acc.value();
             if (d.diag) v += d.diag[r] * d.x[r];
@@ -206,12 +208,13 @@ void launch_gu(const Csr& m, const double* x, double* y, const double* yadd, int
                cudaStream_t s) {
     if (precision == DNQ_F64 || m.nnz == 0) {
         auto kern = k_spmv<G, U, double, AccF64>;
-        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.rowptr.p, m.col.p, m.val.p, x, nullptr,
-                                                      x, m.nr, m.nnz, y, yadd);
+        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.row_start(), m.row_end(), m.col.p,
+                                                      m.val.p, x, nullptr, x, m.nr, m.span(), y,
+                                                      yadd);
     } else {
         auto kern = k_spmv<G, U, float, AccF32>;
-        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.rowptr.p, m.col.p, val32, x32, diag, x,
-                                                      m.nr, m.nnz, y, yadd);
+        kern<<<blocks_for(kern, device), 256, 0, s>>>(m.row_start(), m.row_end(), m.col.p, val32,
+                                                      x32, diag, x, m.nr, m.span(), y, yadd);
     }
 }
 
@@ -363,7 +366,7 @@ void ensure_f32_all(Csr& m, cudaStream_t s) {
 
 // Prepare the FP32 operator buffers of the V block.
 void ensure_f32(dnq_ham_s* h, cudaStream_t s) {
-    if (h->vv.val32.n != (size_t)h->vv.nnz || h->diag_op.n != (size_t)h->n_v)
+    if (!h->vv.f32_ready() || h->diag_op.n != (size_t)h->n_v)
         make_f32(h->vv, s, &h->diag_op);
     if ((i64)h->x32.n < h->n_v) h->x32.alloc(h->n_v, s);
 }

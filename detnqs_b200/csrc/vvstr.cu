@@ -511,6 +511,11 @@ struct Arena {
     u32* sgl_n;                       // entries used in each warp's slice
     u32 sgl_slice;
     i64 sgl_cap;                      // warps * sgl_slice
+    // arena-form output with the FP32 operator copy: k_vv_eval writes the
+    // FP32 value of every entry (0 for the diagonal entry) and the FP64
+    // diagonal of every row (0 where a row keeps none)
+    float* val32;
+    double* dg;
     u32* cnt;                         // two-pass fallback
     const i64* off;
     u32* col;
@@ -1309,6 +1314,10 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
         const u32 sgn0 = sgn;   // a row that is walked again drops its singles
+        // every row starts on a 4-slot boundary: the H.psi kernels split a row
+        // into slots aligned to its start, so its order of accumulation is
+        // then the same on every build
+        cpos = std::min<i64>((cpos + 3) & ~3ll, cend);
         for (int attempt = 0; attempt < 2; ++attempt) {
             sgn = sgn0;
             HitOut out{reinterpret_cast<u64*>(A.aval) + cpos, (u32)(cend - cpos), slice, &sgn,
@@ -1423,13 +1432,17 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_eval(Loc L, Arena A) {
                 const i64 at = w + __popc(m & lanemask_lt());
                 A.acol[at] = e1.j + cb;
                 A.aval[at] = e1.h;
+                // member 0 is the diagonal (the walk records it first)
+                if (A.val32) A.val32[at] = k1 == 0 ? 0.0f : (float)e1.h;
             }
+            if (A.dg && k1 == 0) A.dg[g] = e1.keep ? e1.h : 0.0;
             w += __popc(m);
             m = __ballot_sync(0xffffffffu, e2.keep);
             if (e2.keep) {
                 const i64 at = w + __popc(m & lanemask_lt());
                 A.acol[at] = e2.j + cb;
                 A.aval[at] = e2.h;
+                if (A.val32) A.val32[at] = (float)e2.h;
             }
             w += __popc(m);
         }
@@ -1454,8 +1467,8 @@ __global__ void __launch_bounds__(kWS * 32) k_vv_big(Loc L, Arena A) {
     for (int i = gw; i < nbig; i += nw) {
         const int g = (int)A.big[i];
         const u32 len = A.row_len[g];
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)len);
+        unsigned long long base = 0;   // 4-slot multiples keep every start aligned
+        if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)((len + 3u) & ~3u));
         base = __shfl_sync(0xffffffffu, base, 0);
         if ((i64)base + len > A.cap) {
             if (lane == 0) atomicExch(A.overflow, 1);
@@ -1619,6 +1632,92 @@ __global__ void k_vv_compact(const i64* row_pos, const i64* rowptr, i64 n, const
     }
 }
 
+// Arena form: the long rows compacted in place (block per row, in order; a
+// tile is read before any of it is written, and writes land below the next
+// tile), with the FP32 copy and the diagonal when val32 is set.
+__global__ void __launch_bounds__(256) k_vv_long_inplace(const u32* big, const u32* big_len,
+                                                         const int* n_big, const i64* row_pos,
+                                                         u32* acol, double* aval, float* val32,
+                                                         double* dg) {
+    __shared__ u32 wsum[8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nbig = *n_big;
+    for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
+        const u32 g = big[i];
+        const i64 base = row_pos[g] & ~kLongRow;
+        const i64 len = big_len[i];
+        if (val32 && threadIdx.x == 0) dg[g] = 0.0;   // set below when the row keeps it
+        __syncthreads();
+        i64 carry = 0;
+        for (i64 t0 = 0; t0 < len; t0 += 256) {
+            const i64 t = t0 + threadIdx.x;
+            const u32 c = t < len ? acol[base + t] : kHole;
+            const double v = t < len ? aval[base + t] : 0.0;
+            const bool keep = c != kHole;
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) wsum[wid] = __popc(m);
+            __syncthreads();   // the tile is read
+            u32 before = 0, total = 0;
+            for (int w = 0; w < 8; ++w) {
+                if (w < wid) before += wsum[w];
+                total += wsum[w];
+            }
+            if (keep) {
+                const i64 o = carry + before + __popc(m & lanemask_lt());
+                acol[base + o] = c;
+                aval[base + o] = v;
+                if (val32) {
+                    const bool diag = o == 0 && c == g;
+                    val32[base + o] = diag ? 0.0f : (float)v;
+                    if (diag) dg[g] = v;
+                }
+            }
+            carry += total;
+            __syncthreads();
+        }
+    }
+}
+
+// Arena form: start and end of every row, and the entry count.
+__global__ void k_arena_rows(const i64* row_pos, const u32* row_len, i64 n, i64* start, i64* end,
+                             unsigned long long* nnz) {
+    unsigned long long c = 0;
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r < n;
+         r += (i64)gridDim.x * blockDim.x) {
+        const i64 b = row_pos[r] & ~kLongRow;
+        start[r] = b;
+        end[r] = b + row_len[r];
+        c += row_len[r];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(nnz, c);
+}
+
+// Standard form from arena form: row r moves from [rs[r], re[r]) to
+// [rp[r], rp[r + 1]), in order (warp per row).
+__global__ void k_row_len(const i64* rs, const i64* re, i64 n, i64* len) {
+    for (i64 r = blockIdx.x * (i64)blockDim.x + threadIdx.x; r <= n;
+         r += (i64)gridDim.x * blockDim.x)
+        len[r] = r < n ? re[r] - rs[r] : 0;
+}
+
+__global__ void k_gather_rows(const i64* rs, const i64* re, const i64* rp, i64 n, const u32* col,
+                              const double* val, const float* val32, u32* col2, double* val2,
+                              float* val32_2) {
+    const int lane = threadIdx.x & 31;
+    const i64 gw = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const i64 nw = (gridDim.x * (i64)blockDim.x) >> 5;
+    for (i64 r = gw; r < n; r += nw) {
+        const i64 src = rs[r], dst = rp[r], len = re[r] - src;
+        for (i64 t = lane; t < len; t += 32) {
+            col2[dst + t] = col[src + t];
+            val2[dst + t] = val[src + t];
+            if (val32_2) val32_2[dst + t] = val32[src + t];
+        }
+    }
+}
+
 // Two-pass fallback (arena too small): count, then exact fill.
 template <class Loc, bool FILL>
 __global__ void __launch_bounds__(kWS * 32) k_vv_twopass(Loc L, Arena A) {
@@ -1670,8 +1769,10 @@ namespace {
 
 // Arena slots that always suffice for rows of `nnz` members in all built by
 // `grid` blocks (see the restart rule of k_vv_arena).
-i64 arena_bound(i64 nnz, int grid, i64 chunk) {
-    return nnz + nnz / 3 + 1 + ((i64)grid * kWS + 1) * chunk;
+i64 arena_bound(i64 nnz, i64 nrows, int grid, i64 chunk) {
+    // members, 1/3 for the ends of retired chunks, up to 3 alignment slots
+    // per row (4 with their share of the ends), the warps' open chunks
+    return nnz + nnz / 3 + 1 + 4 * nrows + ((i64)grid * kWS + 1) * chunk;
 }
 
 template <class Loc>
@@ -1769,24 +1870,29 @@ void launch_big(int scan, int grid, const Loc& L, const Arena& A, cudaStream_t s
 
 // Single-pass build of nrows rows of L into M (allocated here).  cap_hint:
 // expected nnz (0 = unknown).  Falls back to the exact two-pass walk when
-// the arena is too small.  With dg, the compaction also writes M.val32 (the
-// FP32 values, diagonal entries zero) and the FP64 diagonal into *dg; the
-// two-pass fallback leaves both empty.  Returns the number of member tests.
+// the arena is too small.  With arena_out, M keeps the rows where the build
+// wrote them (arena form: the arena becomes M's storage, no compaction);
+// else they are compacted into a standard CSR.  With dg, the build also
+// writes M.val32 (the FP32 values, diagonal entries zero) and the FP64
+// diagonal into *dg; the two-pass fallback leaves both empty.  Returns the
+// number of member tests.
 template <class Loc>
 i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Csr& M,
            const Options& opt, double* t_gen, double* t_scan, double* t_compact,
            i64* hits_out = nullptr, int scan = 0, DBuf<double>* dg = nullptr,
-           const u32* order = nullptr) {
+           const u32* order = nullptr, bool arena_out = false) {
     cudaEvent_t ev[4];
     for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
     const int grid = vv_grid<Loc>(device);
     const i64 warps = (i64)grid * kWS;
     size_t freeb = 0, totb = 0;
     DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
-    const i64 chunk = opt.arena_chunk > 0 ? (i64)opt.arena_chunk : kChunk;
+    // chunks of whole 4-slot groups (row starts stay aligned)
+    const i64 chunk = opt.arena_chunk > 0 ? ((i64)opt.arena_chunk + 3) & ~3ll : kChunk;
     i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 512 * nrows;
     want += warps * chunk;
-    const i64 maxfit = (i64)(freeb / 2 / 12);
+    const bool f32_in_build = arena_out && dg;   // k_vv_eval writes the FP32 copy
+    const i64 maxfit = (i64)(freeb / 2 / (f32_in_build ? 16 : 12));
     i64 cap = std::max<i64>(std::min(want, maxfit), chunk);
     if (opt.arena_cap > 0) cap = (i64)opt.arena_cap;
     DBuf<int> next(1, s), ovf(1, s), nbig(1, s), bad(1, s);
@@ -1801,6 +1907,11 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DBuf<u32> sgn(warps, s);
     DBuf<u32> acol(cap, s), rlen(nrows + 1, s), big(nrows, s), blen(nrows, s);
     DBuf<double> aval(cap, s);
+    DBuf<float> av32;
+    if (f32_in_build) {
+        av32.alloc(cap, s);
+        dg->alloc(nrows, s);
+    }
     DBuf<i64> rpos(nrows, s);
     Arena A{};
     A.acol = acol.p;
@@ -1824,6 +1935,8 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     A.sgl_n = sgn.p;
     A.sgl_slice = slice;
     A.sgl_cap = scap;
+    A.val32 = av32.p;
+    A.dg = f32_in_build ? dg->p : nullptr;
     DNQ_CUDA(cudaMemsetAsync(nt.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(nh.p, 0, 8, s));
     DNQ_CUDA(cudaMemsetAsync(next.p, 0, 4, s));
@@ -1847,8 +1960,27 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_CUDA(cudaEventRecord(ev[1], s));
     M.nr = nrows;
-    M.rowptr.alloc(nrows + 1, s);
-    if (!hov) {
+    unsigned long long nnz_h = 0;   // arena form: read after the final sync
+    DBuf<unsigned long long> nsum;
+    if (!hov && arena_out) {
+        DNQ_CUDA(cudaEventRecord(ev[2], s));
+        k_vv_long_inplace<<<grid, 256, 0, s>>>(big.p, blen.p, nbig.p, rpos.p, acol.p, aval.p,
+                                               A.val32, A.dg);
+        DNQ_CHECK_LAUNCH();
+        M.rowptr.alloc(nrows, s);
+        M.rowend.alloc(nrows, s);
+        nsum.alloc(1, s);
+        DNQ_CUDA(cudaMemsetAsync(nsum.p, 0, 8, s));
+        k_arena_rows<<<gsz(nrows), 256, 0, s>>>(rpos.p, rlen.p, nrows, M.rowptr.p, M.rowend.p,
+                                                nsum.p);
+        DNQ_CHECK_LAUNCH();
+        DNQ_CUDA(cudaMemcpyAsync(&nnz_h, nsum.p, 8, cudaMemcpyDeviceToHost, s));
+        M.col = std::move(acol);
+        M.val = std::move(aval);
+        if (f32_in_build) M.val32 = std::move(av32);
+        M.arena = true;
+    } else if (!hov) {
+        M.rowptr.alloc(nrows + 1, s);
         excl_scan(rlen.p, M.rowptr.p, nrows + 1, s);
         DNQ_CUDA(cudaMemcpyAsync(&M.nnz, M.rowptr.p + nrows, 8, cudaMemcpyDeviceToHost, s));
         DNQ_CUDA(cudaStreamSynchronize(s));
@@ -1870,6 +2002,11 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     } else {
         acol.release();
         aval.release();
+        if (f32_in_build) {   // the two-pass fill leaves the FP32 copy to its first use
+            av32.release();
+            dg->release();
+        }
+        M.rowptr.alloc(nrows + 1, s);
         DBuf<u32> cnt(nrows + 1, s);
         DNQ_CUDA(cudaMemsetAsync(cnt.p + nrows, 0, 4, s));
         A.cnt = cnt.p;
@@ -1894,6 +2031,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     DNQ_CUDA(cudaMemcpyAsync(&tests, nt.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaMemcpyAsync(&hits, nh.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaEventSynchronize(ev[3]));
+    if (M.arena) M.nnz = (i64)nnz_h;
     if (hits_out) *hits_out = hov ? std::max<i64>(M.nnz, 2 * cap) : (i64)hits;
     M.sorted = false;
     float ms;
@@ -1952,6 +2090,38 @@ VVParams make_params(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy,
 
 }  // namespace
 
+// Standard form of an arena-form block: rows gathered in order into fresh
+// arrays of nnz entries (the FP32 copy with them when it is ready).
+void ensure_compact(Csr& m, cudaStream_t s) {
+    if (!m.arena) return;
+    const i64 n = m.nr;
+    DBuf<i64> len(n + 1, s), rp(n + 1, s);
+    k_row_len<<<gsz(n + 1), 256, 0, s>>>(m.row_start(), m.row_end(), n, len.p);
+    DNQ_CHECK_LAUNCH();
+    prim::scan<i64, i64, false>(len.p, rp.p, n + 1, s);
+    const bool f32 = m.val32.n > 0 && m.f32_ready();
+    DBuf<u32> col(m.nnz, s);
+    DBuf<double> val(m.nnz, s);
+    DBuf<float> v32;
+    if (f32) v32.alloc(m.nnz, s);
+    int dev = 0;
+    DNQ_CUDA(cudaGetDevice(&dev));
+    if (n > 0) {
+        k_gather_rows<<<sm_count(dev) * 8, 256, 0, s>>>(m.row_start(), m.row_end(), rp.p, n,
+                                                        m.col.p, m.val.p,
+                                                        f32 ? m.val32.p : nullptr, col.p, val.p,
+                                                        v32.p);
+        DNQ_CHECK_LAUNCH();
+    }
+    m.rowptr = std::move(rp);
+    m.rowend.release();
+    m.col = std::move(col);
+    m.val = std::move(val);
+    if (f32) m.val32 = std::move(v32);
+    else m.val32.release();
+    m.arena = false;
+}
+
 // H_VV only, from string groups.  V on the device, diag already computed.
 // Rows are left in generation order (H->vv.sorted = false); copy-out
 // functions sort them on demand.
@@ -1982,7 +2152,7 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     i64 hits = 0;
     H->candidates =
         run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, H->opt, &tg, &tsc, &tc,
-               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr, order.p);
+               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr, order.p, true);
     H->vv.nc = n;
     // the arena holds members before they become entries: size by the larger
     const long long want = std::max<long long>(H->vv.nnz, hits);
@@ -2229,7 +2399,7 @@ void plan(dnq_batch_s* b, cudaStream_t s) {
     b->M.nc = n;
     const i64 nnz = b->M.nnz;
     const int grid = vv_grid<ManySys>(b->device);
-    b->cap = arena_bound(std::max(nnz, b->hits), grid, b->chunk);
+    b->cap = arena_bound(std::max(nnz, b->hits), n, grid, b->chunk);
     b->acol.alloc(b->cap, s);
     b->aval.alloc(b->cap, s);
     b->rlen.alloc(n + 1, s);
@@ -2530,7 +2700,7 @@ int dnq_batch_set_config(dnq_batch_t b, const int64_t* cfg4) {
     upload_params(b, nullptr);
     if (resize) {   // larger chunks need a larger arena
         const int grid = vv_grid<ManySys>(b->device);
-        b->cap = arena_bound(std::max(b->M.nnz, b->hits), grid, b->chunk);
+        b->cap = arena_bound(std::max(b->M.nnz, b->hits), b->total, grid, b->chunk);
         b->acol.alloc(b->cap, nullptr);
         b->aval.alloc(b->cap, nullptr);
         DNQ_CUDA(cudaStreamSynchronize(nullptr));
