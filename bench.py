@@ -468,7 +468,9 @@ def run_ours(args, rank: int, world: int):
 
     peak, peak_kind = measured_peaks()
     fill_ms = float(np.mean(t_fill))
-    alg_fill = n_dets * 16 + (n_dets + 1) * 8 + nnz * (4 + 8)      # dets in, CSR out
+    # dets in; column, FP64 and FP32 value of every entry and each row's
+    # arena position and length out
+    alg_fill = n_dets * 16 + nnz * (4 + 8 + 4) + n_dets * 12
     spmv_ms = float(np.mean(t_e64))
     alg_spmv = nnz * (4 + 8) + n_dets * (8 + 8 + 8)                 # CSR, rowptr, x, y
     result = {
@@ -501,14 +503,17 @@ def run_ours(args, rank: int, world: int):
         "build_phase_ms": {k: float(v) for k, v in last.timings().items()},
         "ms_steps": [round(x, 3) for x in t_steps],
         "roofline": {"bound": "hbm",
-                     "kernel": "k_vv_arena + k_vv_eval (V->V build: members, then entries)",
+                     "kernel": "V->V fill: k_vv_arena (members) + k_vv_singles + k_vv_eval "
+                               "(entries) + long rows",
                      "achieved": alg_fill / (fill_ms * 1e-3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": alg_fill / (fill_ms * 1e-3) / 1e9 / peak,
                      "traffic": ncu_traffic("vv_fill"),
                      "peak_kind": peak_kind,
                      "note": "the walk is integer-issue bound and the evaluation L2-latency "
-                             "bound; bytes are the CSR written and determinants read; traffic "
-                             "adds the 8-byte member records written and read back"},
+                             "bound; bytes are the determinants read and the block written "
+                             "(column, FP64 and FP32 value per entry, arena position and "
+                             "length per row); traffic (walk + evaluation) adds the 8-byte "
+                             "member records written and read back"},
         "roofline_spmv": {"bound": "hbm", "kernel": "k_spmv_f64 (steady state)", "achieved":
                           alg_spmv / (ss["f64"] * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                           "frac": alg_spmv / (ss["f64"] * 1e-3) / 1e9 / peak,
