@@ -660,9 +660,7 @@ void ham_eff_csr(const Csr& VV, const Csr& VP, i64 nv, i64 np, const double* hpp
             DNQ_CHECK_LAUNCH();
         }
         if (nv) {
-            prim::k_segment_sums<i64, i64><<<gs(nv * 32), 256, 0, s>>>(len.p, VP.rowptr.p, nv,
-                                                                      rsum.p);
-            DNQ_CHECK_LAUNCH();
+            prim::segment_sums<i64, i64>(len.p, VP.rowptr.p, nv, rsum.p, s);
         }
         k_cap_finish<<<gs(nv), 256, 0, s>>>(rsum.p, VV.rowptr.p, nv, cap.p);
         DNQ_CHECK_LAUNCH();

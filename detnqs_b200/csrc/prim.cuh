@@ -359,20 +359,64 @@ i64 select_flagged(const T* in, const F* flag, T* out, i64 n, cudaStream_t s) {
     return (i64)lp + lf;
 }
 
-// out[i] = sum of len[t] over segment i = [rp[i], rp[i+1]); one warp per
-// segment, lanes strided, then a butterfly (integer sums: order-free).
+// out[i] = sum of v[t] over segment i = [rp[i], rp[i+1]) for integer v
+// (order-free sums).  One warp per segment, lanes strided, then a butterfly;
+// a segment longer than kSegWarp is listed instead (its sum set to 0) and
+// summed by the whole grid in k_segment_sums_long.
+constexpr i64 kSegWarp = 1 << 16;
+
 template <class T, class Tout>
-__global__ void k_segment_sums(const T* v, const i64* rp, i64 nseg, Tout* out) {
+__global__ void k_segment_sums(const T* v, const i64* rp, i64 nseg, Tout* out, u32* longs,
+                               u32* nlong) {
     const i64 w = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const i64 nw = ((i64)gridDim.x * blockDim.x) >> 5;
     for (i64 i = w; i < nseg; i += nw) {
+        const i64 b = rp[i], e = rp[i + 1];
+        if (e - b > kSegWarp) {
+            if (lane == 0) {
+                out[i] = 0;
+                longs[atomicAdd(nlong, 1u)] = (u32)i;
+            }
+            continue;
+        }
         Tout a = 0;
-        for (i64 t = rp[i] + lane; t < rp[i + 1]; t += 32) a += (Tout)v[t];
+        for (i64 t = b + lane; t < e; t += 32) a += (Tout)v[t];
 #pragma unroll
         for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
         if (lane == 0) out[i] = a;
     }
+}
+
+template <class T, class Tout>
+__global__ void k_segment_sums_long(const T* v, const i64* rp, const u32* longs,
+                                    const u32* nlong, Tout* out) {
+    static_assert(sizeof(Tout) == 8, "64-bit sums");
+    const u32 n = *nlong;
+    for (u32 q = 0; q < n; ++q) {
+        const u32 i = longs[q];
+        Tout a = 0;
+        for (i64 t = rp[i] + blockIdx.x * (i64)blockDim.x + threadIdx.x; t < rp[i + 1];
+             t += (i64)gridDim.x * blockDim.x)
+            a += (Tout)v[t];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0 && a)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&out[i]), (unsigned long long)a);
+    }
+}
+
+// out[0..nseg) = the integer sums of v over the segments of rp (64-bit out).
+template <class T, class Tout>
+void segment_sums(const T* v, const i64* rp, i64 nseg, Tout* out, cudaStream_t s) {
+    if (nseg <= 0) return;
+    DBuf<u32> longs(nseg, s), nlong(1, s);
+    DNQ_CUDA(cudaMemsetAsync(nlong.p, 0, 4, s));
+    const unsigned g = (unsigned)std::min<i64>((nseg * 32 + 255) / 256, 8192);
+    k_segment_sums<T, Tout><<<g, 256, 0, s>>>(v, rp, nseg, out, longs.p, nlong.p);
+    DNQ_CHECK_LAUNCH();
+    k_segment_sums_long<T, Tout><<<1184, 256, 0, s>>>(v, rp, longs.p, nlong.p, out);
+    DNQ_CHECK_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------
@@ -454,13 +498,16 @@ k_row_sort(const u32* rows, const u32* cnt, const i64* rp, const u32* cin, const
     }
 }
 
-// Long rows: key = (place of the row in the long list) << 32 | column.
+// Long rows: key = (place of the row in the long list) << 32 | column.  The
+// whole grid strides over each long row in turn (a row can hold millions of
+// entries).
 __global__ void k_long_row_keys(const u32* rows, u32 nlong, const i64* rp, const i64* base,
                                 const u32* cin, u64* key, u32* src) {
-    for (u32 q = blockIdx.x; q < nlong; q += gridDim.x) {
+    for (u32 q = 0; q < nlong; ++q) {
         const u32 r = rows[q];
         const i64 lo = rp[r], len = rp[r + 1] - lo, b = base[q];
-        for (i64 t = threadIdx.x; t < len; t += blockDim.x) {
+        for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < len;
+             t += (i64)gridDim.x * blockDim.x) {
             key[b + t] = ((u64)q << 32) | cin[lo + t];
             src[b + t] = (u32)(lo + t);
         }
@@ -470,10 +517,11 @@ __global__ void k_long_row_keys(const u32* rows, u32 nlong, const i64* rp, const
 __global__ void k_long_row_put(const u32* rows, u32 nlong, const i64* rp, const i64* base,
                                const u64* skey, const u32* src, const double* vin, u32* cout,
                                double* vout) {
-    for (u32 q = blockIdx.x; q < nlong; q += gridDim.x) {
+    for (u32 q = 0; q < nlong; ++q) {
         const u32 r = rows[q];
         const i64 lo = rp[r], len = rp[r + 1] - lo, b = base[q];
-        for (i64 t = threadIdx.x; t < len; t += blockDim.x) {
+        for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < len;
+             t += (i64)gridDim.x * blockDim.x) {
             cout[lo + t] = (u32)skey[b + t];
             vout[lo + t] = vin[src[b + t]];
         }
@@ -527,7 +575,7 @@ inline void sort_row_columns(const i64* rp, i64 nr, const u32* cin, const double
         DNQ_CUDA(cudaStreamSynchronize(s));
         DBuf<u64> key(m, s), skey(m, s);
         DBuf<u32> src(m, s), ssrc(m, s);
-        const unsigned gl = std::min<u32>(nl, 65535u);
+        const unsigned gl = (unsigned)std::min<i64>((m + 255) / 256, 4096);
         k_long_row_keys<<<gl, 256, 0, s>>>(rows, nl, rp, base.p, cin, key.p, src.p);
         DNQ_CHECK_LAUNCH();
         int hb = 32;
