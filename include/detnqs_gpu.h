@@ -195,7 +195,8 @@ int dnq_ham_set_option(dnq_ham_t h, int option, int64_t value);
 int dnq_ham_info(dnq_ham_t h, int64_t* info6);
 /* Device time of the build phases, from CUDA events recorded on the build
  * stream (ms): [0] maps + diagonal, [1] count pass, [2] scans/allocation,
- * [3] fill pass, [4] V-row sort, [5] P discovery + P-row sort, [6] total,
+ * [3] fill pass, [4] V-row pass (V->V-only builds: long rows compacted in
+ * place and row bounds; else the row sort), [5] P discovery + P-row sort, [6] total,
  * [7] unused.  No reference counterpart (instrumentation). */
 int dnq_ham_timings(dnq_ham_t h, double* ms8);
 /* block 0 = H_VV, 1 = H_VP; COO sorted by (row, col) as in
