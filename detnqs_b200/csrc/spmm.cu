@@ -246,19 +246,37 @@ k_energy_partials_multi(const double* X, int ldx, const double* Y, int ldy, int 
     }
 }
 
-__global__ void k_energy_final_multi(const double* part, int nb, int kx, double* out) {
+// Thread j < kx merges column j's partials in block order (as the single-
+// vector reduction does); the block stages them in shared memory, 128 per
+// column at a time, so the serial merges wait on no global load.
+constexpr int kFinalChunk = 128;
+__global__ void __launch_bounds__(256) k_energy_final_multi(const double* part, int nb, int kx,
+                                                            double* out) {
+    __shared__ double st[8][4 * kFinalChunk];
     const int j = threadIdx.x;
-    if (blockIdx.x != 0 || j >= kx) return;
     Dot2<double> a, b;
-    const double* p = part + (i64)j * nb * 4;
-    for (int q = 0; q < nb; ++q) {
-        Dot2<double> t1, t2;
-        t1.s = p[4 * q]; t1.c = p[4 * q + 1]; t2.s = p[4 * q + 2]; t2.c = p[4 * q + 3];
-        a.merge(t1);
-        b.merge(t2);
+    for (int q0 = 0; q0 < nb; q0 += kFinalChunk) {
+        const int m = min(kFinalChunk, nb - q0);
+        for (int i = threadIdx.x; i < kx * 4 * m; i += blockDim.x) {
+            const int c = i / (4 * m), e = i % (4 * m);
+            st[c][e] = part[((i64)c * nb + q0) * 4 + e];
+        }
+        __syncthreads();
+        if (j < kx) {
+            for (int q = 0; q < m; ++q) {
+                Dot2<double> t1, t2;
+                t1.s = st[j][4 * q]; t1.c = st[j][4 * q + 1];
+                t2.s = st[j][4 * q + 2]; t2.c = st[j][4 * q + 3];
+                a.merge(t1);
+                b.merge(t2);
+            }
+        }
+        __syncthreads();
     }
-    out[2 * j] = a.value();
-    out[2 * j + 1] = b.value();
+    if (j < kx) {
+        out[2 * j] = a.value();
+        out[2 * j + 1] = b.value();
+    }
 }
 
 template <class Kern>
@@ -377,7 +395,7 @@ void energy_reduce_multi(const double* X, int ldx, const double* Y, int ldy, int
                                                                  lde, part);
     }
     DNQ_CHECK_LAUNCH();
-    k_energy_final_multi<<<1, 32, 0, s>>>(part, kEnergyBlocks, kx, out_dev);
+    k_energy_final_multi<<<1, 256, 0, s>>>(part, kEnergyBlocks, kx, out_dev);
     DNQ_CHECK_LAUNCH();
 }
 

@@ -165,17 +165,31 @@ __global__ void k_energy_partials(const double* x, const double* y, i64 n, doubl
     }
 }
 
-__global__ void k_energy_final(const double* part, int nb, double* out2) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// The partials merged by one thread in block order; the block stages them in
+// shared memory first (1024 at a time), so the serial merge waits on no
+// global load.
+constexpr int kFinalStage = 1024;
+__global__ void __launch_bounds__(256) k_energy_final(const double* part, int nb, double* out2) {
+    __shared__ double st[4 * kFinalStage];
     Dot2<double> a, b;
-    for (int k = 0; k < nb; ++k) {
-        Dot2<double> t1, t2;
-        t1.s = part[4 * k]; t1.c = part[4 * k + 1]; t2.s = part[4 * k + 2]; t2.c = part[4 * k + 3];
-        a.merge(t1);
-        b.merge(t2);
+    for (int k0 = 0; k0 < nb; k0 += kFinalStage) {
+        const int m = min(kFinalStage, nb - k0);
+        for (int i = threadIdx.x; i < 4 * m; i += blockDim.x) st[i] = part[4 * k0 + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < m; ++k) {
+                Dot2<double> t1, t2;
+                t1.s = st[4 * k]; t1.c = st[4 * k + 1]; t2.s = st[4 * k + 2]; t2.c = st[4 * k + 3];
+                a.merge(t1);
+                b.merge(t2);
+            }
+        }
+        __syncthreads();
     }
-    out2[0] = a.value();
-    out2[1] = b.value();
+    if (threadIdx.x == 0) {
+        out2[0] = a.value();
+        out2[1] = b.value();
+    }
 }
 
 int group_for(const Csr& m) {
@@ -319,7 +333,7 @@ void energy_reduce(const double* x, const double* y, i64 n, double* eloc, double
     DBuf<double> part(4 * nb, s);
     k_energy_partials<<<nb, 256, 0, s>>>(x, y, n, eloc, part.p);
     DNQ_CHECK_LAUNCH();
-    k_energy_final<<<1, 32, 0, s>>>(part.p, nb, out2_dev);
+    k_energy_final<<<1, 256, 0, s>>>(part.p, nb, out2_dev);
     DNQ_CHECK_LAUNCH();
 }
 
@@ -329,7 +343,7 @@ void energy_reduce_into(const double* x, const double* y, i64 n, double* eloc, d
                         int nb, double* out2_dev, cudaStream_t s) {
     k_energy_partials<<<nb, 256, 0, s>>>(x, y, n, eloc, part);
     DNQ_CHECK_LAUNCH();
-    k_energy_final<<<1, 32, 0, s>>>(part, nb, out2_dev);
+    k_energy_final<<<1, 256, 0, s>>>(part, nb, out2_dev);
     DNQ_CHECK_LAUNCH();
 }
 
