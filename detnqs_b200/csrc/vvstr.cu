@@ -860,6 +860,16 @@ __device__ __forceinline__ void scan_same(Q& q, const W* other, W x, u32 st, u32
     }
 }
 
+// i / d and i % d for 0 <= i < 2^12 and 1 <= d <= 64 through the correctly
+// rounded reciprocal of d: the product's error (< 2^-11) is far inside the
+// 1/(2d) distance of (i + 0.5) / d from an integer, so truncation gives the
+// quotient exactly, for a few instructions instead of an integer division.
+__device__ __forceinline__ int small_div(int i, float rcp, int d, int& r) {
+    const int q = (int)(((float)i + 0.5f) * rcp);
+    r = i - q * d;
+    return q;
+}
+
 // Part C in one direction.  x is the string whose singles x' give the
 // groups (alpha-major: x = a, the groups of the alpha index, members
 // sorted by their beta strings); y is the other string, and a member is a
@@ -886,6 +896,7 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
     const W yw = (W)y;
     const int nsx = (bm ? nb : na) * nvx;
     const int nyv = ny * nvy;
+    const float rvx = __frcp_rn((float)nvx), rvy = __frcp_rn((float)nvy);
     const bool usep = pres != nullptr && nyv <= kBS;
     int nys = -1;   // indexed y singles listed in S (-1: not yet)
     for (int s0 = 0; s0 < nsx; s0 += 32) {
@@ -893,8 +904,9 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
         u32 gs = 0, gl = 0, gg = 0xffffffffu;
         int hh = 0, pp = 0;
         if (sidx < nsx) {
-            hh = occx[sidx / nvx];
-            pp = virx[sidx % nvx];
+            int pi;
+            hh = occx[small_div(sidx, rvx, nvx, pi)];
+            pp = virx[pi];
             const u32* nbt = bm ? P.b_nbr : P.a_nbr;
             if (nbt && gx != 0xffffffffu) {
                 gg = __ldg(&nbt[(i64)gx * nbr_stride(P.n_orb) + sidx]);
@@ -956,7 +968,8 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
                 u32 bid = 0;
                 u16 e = 0;
                 if (qi < nyv) {
-                    const int hb = occy[qi / nvy], pb = viry[qi % nvy];
+                    int pi;
+                    const int hb = occy[small_div(qi, rvy, nvy, pi)], pb = viry[pi];
                     const u32* nbt = bm ? P.a_nbr : P.b_nbr;
                     if (nbt && gy != 0xffffffffu) {
                         bid = __ldg(&nbt[(i64)gy * nbr_stride(P.n_orb) + qi]);
@@ -1030,8 +1043,9 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
                 bool hit = false;
                 u32 lo = 0;
                 if (qi < nyv) {
-                    const int hb = occy[qi / nvy];
-                    const int pb = viry[qi % nvy];
+                    int pi;
+                    const int hb = occy[small_div(qi, rvy, nvy, pi)];
+                    const int pb = viry[pi];
                     const u64 t = y ^ (1ull << hb) ^ (1ull << pb);
                     lo = g0;
                     u32 hi = g0 + gn;
