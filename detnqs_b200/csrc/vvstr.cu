@@ -1295,15 +1295,7 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
     const int lane = threadIdx.x & 31;
     const i64 nrows = L.rows();
     i64 cpos = 0, cend = 0;
-    {   // first chunk of this warp
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)A.chunk);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if ((i64)base + A.chunk <= A.cap) {
-            cpos = (i64)base;
-            cend = cpos + A.chunk;
-        }
-    }
+    bool chunked = false;   // the first chunk is taken with the first row
     unsigned long long tests = 0, hits = 0;
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint4* slice = A.sgl ? A.sgl + (i64)wid * A.sgl_slice : nullptr;
@@ -1328,6 +1320,16 @@ __global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
         row_setup(P, r, a, b, psr, cut);
         load_lists(S, a, b, P.n_orb);
         const u32 sgn0 = sgn;   // a row that is walked again drops its singles
+        if (!chunked) {   // warps that get no row take no chunk
+            chunked = true;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(A.cursor, (unsigned long long)A.chunk);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if ((i64)base + A.chunk <= A.cap) {
+                cpos = (i64)base;
+                cend = cpos + A.chunk;
+            }
+        }
         // every row starts on a 4-slot boundary: the H.psi kernels split a row
         // into slots aligned to its start, so its order of accumulation is
         // then the same on every build
