@@ -329,6 +329,15 @@ void make_f32(Csr& m, cudaStream_t s, DBuf<double>* diag_out) {
 }
 
 // Validate and stage the determinants; throws on orbitals >= n_orb.
+// Flags in *bad (zeroed by the caller) a determinant with an orbital >= n_orb;
+// no host synchronisation.
+void launch_check_orbitals(const u64* d, i64 n, int n_orb, unsigned long long* bad,
+                           cudaStream_t s) {
+    if (n == 0) return;
+    k_check_orbitals<<<grid_for(n), 256, 0, s>>>(d, n, n_orb, bad);
+    DNQ_CHECK_LAUNCH();
+}
+
 void check_orbitals(const u64* d, i64 n, int n_orb, cudaStream_t s) {
     if (n == 0) return;
     DBuf<unsigned long long> bad(1, s);
@@ -396,6 +405,9 @@ void launch_wide_diag(const dnq_ctx_s* ctx, const u64* d, i64 n, double* out, cu
 void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                       double cut, const double* psi, const double* diag, cudaStream_t s,
                       dnq_ham_s* H, double* t_ms);
+void build_vv_checked(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
+                      double cut, const double* psi, cudaStream_t s, dnq_ham_s* H,
+                      double* t_ms);
 
 void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
                const double* psi_in, int n_orb, int policy, int use_hb, double eps1,
@@ -407,6 +419,20 @@ void build_ham(dnq_ctx_s* ctx, const u64* V_in, i64 nV, const u64* X_in, i64 nX,
     T.mark();
     DIn<u64> V(V_in, 2 * nV, s), X(X_in, 2 * nX, s);
     DIn<double> psi(psi_in, policy == DNQ_POLICY_DYNAMIC ? nV : 0, s);
+    const bool vv_only = !want_vp && !(policy == DNQ_POLICY_KNOWN_SETS && X_in && nX > 0) &&
+                         n_orb < 64 && !H->opt.force_walk;
+    if (vv_only && nV > 0) {
+        // V->V block only, the input checks folded into the string indices'
+        // one host synchronisation (an X set the policy does not use is
+        // still checked, as on every other path)
+        check_orbitals(X.p, nX, n_orb, s);
+        build_vv_checked(ctx, V.p, nV, n_orb, policy, eps1,
+                         policy_cut(ctx, policy, use_hb, eps1), psi.p, s, H, H->t_ms);
+        H->n_p = 0;
+        H->t_ms[6] = H->t_ms[0] + H->t_ms[1] + H->t_ms[2] + H->t_ms[3] + H->t_ms[4];
+        DNQ_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     check_orbitals(V.p, nV, n_orb, s);
     check_orbitals(X.p, nX, n_orb, s);
     DetMap mapV, mapX;

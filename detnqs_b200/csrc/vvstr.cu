@@ -87,6 +87,8 @@ struct StrIndex {
     // it walks the groups of its singles (scanned members, groups tested by
     // presence rows, groups binary-searched, singles that are groups).
     DBuf<uint4> cost;
+    DBuf<u64> ks64;          // sorted keys between the two phases of the build
+    DBuf<ulonglong2> ks;
     // Per group: the group of each single excitation of its string (~0u:
     // not a string of the index), in the order of the part C walk (over the
     // occupied orbitals, then the virtual ones), nbr_stride() entries per
@@ -104,25 +106,47 @@ __global__ void k_keys_by(const u64* V, i64 n, int major, ulonglong2* k, u32* id
     }
 }
 
-__global__ void k_split_sorted(const ulonglong2* k, i64 n, u64* other, unsigned* head) {
+// dup (optional) is set when two sorted keys are equal: a determinant listed
+// twice.
+__global__ void k_split_sorted(const ulonglong2* k, i64 n, u64* other, unsigned* head, u32* dup) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x) {
         other[t] = k[t].y;
         head[t] = (t == 0 || k[t].x != k[t - 1].x) ? 1u : 0u;
+        if (dup && t > 0 && k[t].x == k[t - 1].x && k[t].y == k[t - 1].y) *dup = 1u;
     }
 }
 
 // Start position of every group and n after the last; gid arrives as the
 // inclusive scan of the head flags and leaves as the group number of every
 // position.
-__global__ void k_group_starts(const unsigned* head, u32* gid, i64 n, u32* gstart) {
+__global__ void k_group_starts(const unsigned* head, u32* gid, i64 n, u32* gstart, u32* ngroups) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x) {
         const u32 g = gid[t] - 1;
         gid[t] = g;
         if (head[t]) gstart[g] = (u32)t;
-        if (t == n - 1) gstart[g + 1] = (u32)n;
+        if (t == n - 1) {
+            gstart[g + 1] = (u32)n;
+            if (ngroups) *ngroups = g + 1;
+        }
     }
+}
+
+// Group lengths by floor(log2(len - 1)) (len >= 2): the groups longer than
+// 2^j are the counts of bins j and up.
+__global__ void k_len_hist(const u32* gstart, const u32* ngroups, i64 nmax, u32* hist) {
+    __shared__ u32 h[32];
+    if (threadIdx.x < 32) h[threadIdx.x] = 0;
+    __syncthreads();
+    const i64 G = *ngroups;
+    for (i64 g = blockIdx.x * (i64)blockDim.x + threadIdx.x; g < G && g < nmax;
+         g += (i64)gridDim.x * blockDim.x) {
+        const u32 len = gstart[g + 1] - gstart[g];
+        if (len >= 2) atomicAdd(&h[31 - __clz(len - 1)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32 && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
 // Strings of at most 32 orbitals: one 64-bit key (group string << 32 | companion).
@@ -135,12 +159,14 @@ __global__ void k_keys_by64(const u64* V, i64 n, int major, u64* k, u32* id) {
     }
 }
 
-__global__ void k_split_sorted64(const u64* k, i64 n, u64* other, u32* other32, unsigned* head) {
+__global__ void k_split_sorted64(const u64* k, i64 n, u64* other, u32* other32, unsigned* head,
+                                 u32* dup) {
     for (i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x; t < n;
          t += (i64)gridDim.x * blockDim.x) {
         other[t] = k[t] & 0xffffffffull;
         other32[t] = (u32)k[t];
         head[t] = (t == 0 || (k[t] >> 32) != (k[t - 1] >> 32)) ? 1u : 0u;
+        if (dup && t > 0 && k[t] == k[t - 1]) *dup = 1u;
     }
 }
 
@@ -185,6 +211,79 @@ int gsz(i64 n) {
 // major 0: groups by alpha (companion beta); major 1: groups by beta.  With
 // n_orb <= 32 the sort runs on 64-bit keys over 32 + n_orb bits, and the
 // 32-bit companion strings of the scans come out of the same pass.
+// What the host reads of an index after its first phase: the group count,
+// the group lengths by floor(log2(len - 1)), and whether a determinant is
+// listed twice.
+struct IndexProbe {
+    u32 ngroups;
+    u32 dup;
+    u32 hist[32];
+};
+
+// First phase of a string index (no host synchronisation): sorted keys,
+// companions, group numbers and starts; the probe is filled on the device.
+// The sorted keys stay in X until str_index_finish.
+void str_index_begin(StrIndex& X, const u64* V, i64 n, int major, int n_orb, IndexProbe* probe,
+                     cudaStream_t s) {
+    const bool narrow = n_orb <= 32;
+    DBuf<ulonglong2> k;
+    DBuf<u64> k64;
+    DBuf<u32> id(n, s);
+    X.idx.alloc(n, s);
+    X.other.alloc(n, s);
+    DBuf<unsigned> head(n, s);
+    u32* dup = major == 0 ? &probe->dup : nullptr;
+    if (narrow) {
+        k64.alloc(n, s);
+        X.ks64.alloc(n, s);
+        X.other32.alloc(n, s);
+        k_keys_by64<<<gsz(n), 256, 0, s>>>(V, n, major, k64.p, id.p);
+        DNQ_CHECK_LAUNCH();
+        const int bits[1] = {32 + n_orb};
+        prim::radix_sort<u64, u32>(k64.p, X.ks64.p, id.p, X.idx.p, n, bits, s);
+        k_split_sorted64<<<gsz(n), 256, 0, s>>>(X.ks64.p, n, X.other.p, X.other32.p, head.p, dup);
+        DNQ_CHECK_LAUNCH();
+    } else {
+        k.alloc(n, s);
+        X.ks.alloc(n, s);
+        k_keys_by<<<gsz(n), 256, 0, s>>>(V, n, major, k.p, id.p);
+        DNQ_CHECK_LAUNCH();
+        const int bits[2] = {n_orb, n_orb};
+        prim::radix_sort<ulonglong2, u32>(k.p, X.ks.p, id.p, X.idx.p, n, bits, s);
+        k_split_sorted<<<gsz(n), 256, 0, s>>>(X.ks.p, n, X.other.p, head.p, dup);
+        DNQ_CHECK_LAUNCH();
+    }
+    X.gid.alloc(n, s);
+    X.gstart.alloc(n + 1, s);
+    prim::scan_inclusive<unsigned, u32>(head.p, X.gid.p, n, s);
+    k_group_starts<<<gsz(n), 256, 0, s>>>(head.p, X.gid.p, n, X.gstart.p, &probe->ngroups);
+    DNQ_CHECK_LAUNCH();
+    k_len_hist<<<gsz(n), 256, 0, s>>>(X.gstart.p, &probe->ngroups, n, probe->hist);
+    DNQ_CHECK_LAUNCH();
+}
+
+// Second phase, with the group count read: the string -> group hash.
+void str_index_finish(StrIndex& X, i64 n, i64 ngroups, cudaStream_t s) {
+    X.ngroups = ngroups;
+    u64 cap = 1024;
+    while (cap < (u64)(2 * ngroups)) cap <<= 1;
+    X.mask = cap - 1;
+    X.slots.alloc(cap, s);
+    DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, cap * sizeof(ulonglong2), s));
+    if (X.ks64.p)
+        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key64{X.ks64.p}, X.gstart.p, ngroups, n,
+                                                    X.slots.p, X.mask);
+    else
+        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key128{X.ks.p}, X.gstart.p, ngroups, n,
+                                                    X.slots.p, X.mask);
+    DNQ_CHECK_LAUNCH();
+    X.ks64.release();
+    X.ks.release();
+}
+
+// major 0: groups by alpha (companion beta); major 1: groups by beta.  With
+// n_orb <= 32 the sort runs on 64-bit keys over 32 + n_orb bits, and the
+// 32-bit companion strings of the scans come out of the same pass.
 void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cudaStream_t s) {
     if (n == 0) {   // no groups: an empty table
         X.ngroups = 0;
@@ -193,57 +292,13 @@ void build_str_index(StrIndex& X, const u64* V, i64 n, int major, int n_orb, cud
         DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, 1024 * sizeof(ulonglong2), s));
         return;
     }
-    const bool narrow = n_orb <= 32;
-    DBuf<ulonglong2> k, ks;
-    DBuf<u64> k64, ks64;
-    DBuf<u32> id(n, s);
-    X.idx.alloc(n, s);
-    X.other.alloc(n, s);
-    DBuf<unsigned> head(n, s);
-    if (narrow) {
-        k64.alloc(n, s);
-        ks64.alloc(n, s);
-        X.other32.alloc(n, s);
-        k_keys_by64<<<gsz(n), 256, 0, s>>>(V, n, major, k64.p, id.p);
-        DNQ_CHECK_LAUNCH();
-        const int bits[1] = {32 + n_orb};
-        prim::radix_sort<u64, u32>(k64.p, ks64.p, id.p, X.idx.p, n, bits, s);
-        k_split_sorted64<<<gsz(n), 256, 0, s>>>(ks64.p, n, X.other.p, X.other32.p, head.p);
-        DNQ_CHECK_LAUNCH();
-    } else {
-        k.alloc(n, s);
-        ks.alloc(n, s);
-        k_keys_by<<<gsz(n), 256, 0, s>>>(V, n, major, k.p, id.p);
-        DNQ_CHECK_LAUNCH();
-        const int bits[2] = {n_orb, n_orb};
-        prim::radix_sort<ulonglong2, u32>(k.p, ks.p, id.p, X.idx.p, n, bits, s);
-        k_split_sorted<<<gsz(n), 256, 0, s>>>(ks.p, n, X.other.p, head.p);
-        DNQ_CHECK_LAUNCH();
-    }
-    X.gid.alloc(n, s);
-    X.gstart.alloc(n + 1, s);
-    DBuf<u32>& gid = X.gid;
-    DBuf<u32>& gstart = X.gstart;
-    prim::scan_inclusive<unsigned, u32>(head.p, gid.p, n, s);
-    u32 last_gid = 0;
-    DNQ_CUDA(cudaMemcpyAsync(&last_gid, gid.p + n - 1, 4, cudaMemcpyDeviceToHost, s));
+    DBuf<IndexProbe> probe(1, s);
+    DNQ_CUDA(cudaMemsetAsync(probe.p, 0, sizeof(IndexProbe), s));
+    str_index_begin(X, V, n, major, n_orb, probe.p, s);
+    u32 ng = 0;
+    DNQ_CUDA(cudaMemcpyAsync(&ng, &probe.p->ngroups, 4, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
-    const i64 ngroups = (i64)last_gid;
-    X.ngroups = ngroups;
-    k_group_starts<<<gsz(n), 256, 0, s>>>(head.p, gid.p, n, gstart.p);
-    DNQ_CHECK_LAUNCH();
-    u64 cap = 1024;
-    while (cap < (u64)(2 * ngroups)) cap <<= 1;
-    X.mask = cap - 1;
-    X.slots.alloc(cap, s);
-    DNQ_CUDA(cudaMemsetAsync(X.slots.p, 0xff, cap * sizeof(ulonglong2), s));
-    if (narrow)
-        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key64{ks64.p}, gstart.p, ngroups, n,
-                                                    X.slots.p, X.mask);
-    else
-        k_group_insert<<<gsz(ngroups), 256, 0, s>>>(Key128{ks.p}, gstart.p, ngroups, n,
-                                                    X.slots.p, X.mask);
-    DNQ_CHECK_LAUNCH();
+    str_index_finish(X, n, ng, s);
 }
 
 __global__ void k_narrow(const u64* x, i64 n, u32* y) {
@@ -324,6 +379,9 @@ __global__ void k_pres_rank(uint2* pres, i64 rows, u32 words) {
     }
 }
 
+void presence_rows(StrIndex& A, const StrIndex& B, i64 n, u32 thr, unsigned long long nl,
+                   cudaStream_t s);
+
 // Presence rows of the groups of index A over the groups of index B (alpha
 // over beta, and beta over alpha for the beta-major walk).  The threshold
 // starts at kPresMin and doubles until the rows fit kPresBytes.
@@ -343,6 +401,33 @@ void build_presence(StrIndex& A, const StrIndex& B, i64 n, cudaStream_t s) {
         if ((i64)nl * words * 8 <= kPresBytes || (i64)thr >= n) break;
         thr *= 2;
     }
+    presence_rows(A, B, n, thr, nl, s);
+}
+
+// The same threshold from the group-length histogram of A (str_index_begin):
+// no host synchronisation.
+void build_presence_hist(StrIndex& A, const StrIndex& B, i64 n, const u32* hist,
+                         cudaStream_t s) {
+    if (n == 0 || A.ngroups == 0) return;
+    const u32 words = (u32)((B.ngroups + 31) / 32);
+    auto longer = [&](u32 t) {   // groups longer than t = 2^j: bins j and up
+        unsigned long long c = 0;
+        for (int b = 31 - __builtin_clz(t); b < 32; ++b) c += hist[b];
+        return c;
+    };
+    u32 thr = kPresMin;
+    unsigned long long nl = longer(thr);
+    while (!((i64)nl * words * 8 <= kPresBytes || (i64)thr >= n)) {
+        thr *= 2;
+        nl = longer(thr);
+    }
+    presence_rows(A, B, n, thr, nl, s);
+}
+
+// The presence rows of the nl groups of A longer than thr.
+void presence_rows(StrIndex& A, const StrIndex& B, i64 n, u32 thr, unsigned long long nl,
+                   cudaStream_t s) {
+    const u32 words = (u32)((B.ngroups + 31) / 32);
     if (nl == 0 || (i64)nl * words * 8 > kPresBytes) return;
     DBuf<u32> flag(A.ngroups, s), rank(A.ngroups, s);
     k_long_groups<<<gsz(A.ngroups), 256, 0, s>>>(A.gstart.p, A.ngroups, n, thr, flag.p, nullptr);
@@ -2136,6 +2221,75 @@ void ensure_compact(Csr& m, cudaStream_t s) {
     if (f32) m.val32 = std::move(v32);
     else m.val32.release();
     m.arena = false;
+}
+
+void launch_check_orbitals(const u64* d, i64 n, int n_orb, unsigned long long* bad,
+                           cudaStream_t s);
+
+// H_VV only, from string groups, with dnq_build's input checks folded into
+// the string indices' one host synchronisation: every orbital below n_orb,
+// no determinant listed twice (equal keys side by side in the sorted alpha
+// index), and the group counts and lengths of both indices, read together.
+// Computes the diagonal into H->diag.  n > 0.
+void build_vv_checked(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
+                      double cut, const double* psi, cudaStream_t s, dnq_ham_s* H,
+                      double* t_ms) {
+    cudaEvent_t e0, e1;
+    DNQ_CUDA(cudaEventCreate(&e0));
+    DNQ_CUDA(cudaEventCreate(&e1));
+    DNQ_CUDA(cudaEventRecord(e0, s));
+    DBuf<unsigned long long> bad(1, s);
+    DBuf<IndexProbe> probe(2, s);
+    DNQ_CUDA(cudaMemsetAsync(bad.p, 0, 8, s));
+    DNQ_CUDA(cudaMemsetAsync(probe.p, 0, 2 * sizeof(IndexProbe), s));
+    launch_check_orbitals(V, n, n_orb, bad.p, s);
+    StrIndex A, B;
+    str_index_begin(A, V, n, 0, n_orb, probe.p, s);
+    str_index_begin(B, V, n, 1, n_orb, probe.p + 1, s);
+    unsigned long long hbad = 0;
+    IndexProbe hp[2];
+    DNQ_CUDA(cudaMemcpyAsync(&hbad, bad.p, 8, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaMemcpyAsync(hp, probe.p, 2 * sizeof(IndexProbe), cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaStreamSynchronize(s));
+    require(hbad == 0, DNQ_ERR_INVALID, "determinant occupies an orbital index >= n_orb");
+    require(hp[0].dup == 0, DNQ_ERR_DUPLICATE,
+            "DetMap::from_ordered: duplicate determinant found");
+    H->diag.alloc(n, s);
+    launch_diag(ctx, V, n, H->diag.p, s);
+    str_index_finish(A, n, hp[0].ngroups, s);
+    str_index_finish(B, n, hp[1].ngroups, s);
+    build_presence_hist(A, B, n, hp[0].hist, s);
+    build_presence_hist(B, A, n, hp[1].hist, s);
+    build_group_cost(A, V, n, 0, n_orb, s);
+    build_group_cost(B, V, n, 1, n_orb, s);
+    const bool narrow = n_orb <= 32;
+    if (narrow) {
+        narrow_index(A, n, s);
+        narrow_index(B, n, s);
+    }
+    DBuf<u32> order;
+    build_row_order(A, B, V, n, n_orb, order, s);
+    DNQ_CUDA(cudaEventRecord(e1, s));
+    OneSys L{make_params(ctx, V, n, n_orb, policy, eps1, cut, psi, H->diag.p, A, B, H->opt)};
+    double tg = 0, tsc = 0, tc = 0;
+    i64 hits = 0;
+    H->candidates =
+        run_vv(L, n, ctx->vv_nnz_hint.load(), ctx->device, s, H->vv, H->opt, &tg, &tsc, &tc,
+               &hits, narrow ? 1 : 0, H->opt.build_f32 ? &H->diag_op : nullptr, order.p, true);
+    H->vv.nc = n;
+    const long long want = std::max<long long>(H->vv.nnz, hits);
+    long long prev = ctx->vv_nnz_hint.load();
+    while (prev < want && !ctx->vv_nnz_hint.compare_exchange_weak(prev, want)) {
+    }
+    float ms = 0;
+    DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    t_ms[0] = ms;    // checks, string indices, diagonal
+    t_ms[1] = 0.0;   // no count pass
+    t_ms[3] = tg;    // generation pass(es)
+    t_ms[2] = tsc;   // scan + allocation
+    t_ms[4] = tc;    // arena rows (row sort deferred)
 }
 
 // H_VV only, from string groups.  V on the device, diag already computed.
