@@ -207,7 +207,8 @@ def ncu_traffic(kernel: str):
 # reference CPU path
 # ---------------------------------------------------------------------------
 
-def cpu_reference_sample(sysm, V, target_s: float = 15.0, min_rows: int = 64):
+def cpu_reference_sample(sysm, V, target_s: float = 15.0, min_rows: int = 64,
+                         probe_rows: int = 1024):
     """Time the reference core's static heat-bath H_VV rows on a bounded
     sample of rows of the same workload.  Returns (elements/s, rows, nnz,
     seconds, threads, kind)."""
@@ -228,15 +229,20 @@ def cpu_reference_sample(sysm, V, target_s: float = 15.0, min_rows: int = 64):
             ctx = chk.ctx_from_arrays(N_ORB, sysm.h1e, sysm.eri, sysm.e_core)
         ctx.hb_prepare(1e-15)
         rng = np.random.default_rng(77)
-        rows = np.sort(rng.choice(len(V), min_rows, replace=False))
+        rows = np.sort(rng.choice(len(V), min(probe_rows, len(V)), replace=False))
         t0 = time.perf_counter()
         r = ctx.vv_hb_rows(V, rows, EPS1)
         t_probe = time.perf_counter() - t0
-        # the map of V is built inside each call; time it separately
-        t0 = time.perf_counter()
-        ctx.vv_hb_rows(V, rows[:1], EPS1)
-        t_map = time.perf_counter() - t0
-        per_row = max((t_probe - t_map) / len(rows), 1e-6)
+        # the map of V is built inside each call; time it separately (the
+        # faster of two calls: host noise only adds time)
+        t_map = t_probe
+        for _ in range(2):
+            t0 = time.perf_counter()
+            ctx.vv_hb_rows(V, rows[:1], EPS1)
+            t_map = min(t_map, time.perf_counter() - t0)
+        # a noisy probe must not size the sample past its bound: a row costs
+        # at least a quarter of the probe's time per row
+        per_row = max(t_probe - t_map, 0.25 * t_probe) / len(rows)
         n_rows = int(min(len(V), max(min_rows, (target_s - t_map) / per_row)))
         rows = np.sort(rng.choice(len(V), n_rows, replace=False))
         t0 = time.perf_counter()
@@ -246,7 +252,7 @@ def cpu_reference_sample(sysm, V, target_s: float = 15.0, min_rows: int = 64):
     return nnz / t, n_rows, nnz, t, threads, kind
 
 
-def cpu_reference_rows(systems, target_s: float = 15.0, probe_rows: int = 64, seed: int = 77):
+def cpu_reference_rows(systems, target_s: float = 15.0, probe_rows: int = 1024, seed: int = 77):
     """Reference core's static heat-bath H_VV rows on a sample of rows drawn
     uniformly from the concatenated rows of many systems (sysm, V, eps1).
     Context creation and the per-call map of V stay outside the timing.
@@ -282,6 +288,7 @@ def cpu_reference_rows(systems, target_s: float = 15.0, probe_rows: int = 64, se
             g = np.sort(rng.choice(off[-1], min(n_rows, off[-1]), replace=False))
             which = np.searchsorted(off, g, side="right") - 1
             t_all = 0.0
+            t_calls = 0.0
             nnz = 0
             for k in np.unique(which):
                 _, V, eps = systems[k]
@@ -292,13 +299,17 @@ def cpu_reference_rows(systems, target_s: float = 15.0, probe_rows: int = 64, se
                 t_map = time.perf_counter() - t0
                 t0 = time.perf_counter()
                 r = c.vv_hb_rows(V, rows, eps)
-                t_all += max(time.perf_counter() - t0 - t_map, 0.0)
+                t_call = time.perf_counter() - t0
+                t_calls += t_call
+                t_all += max(t_call - t_map, 0.0)
                 nnz += len(r["val"])
-            return len(g), nnz, t_all
+            return len(g), nnz, t_all, t_calls
 
-        rows, nnz, t = run(probe_rows)
-        per_row = max(t / max(rows, 1), 1e-6)
-        rows, nnz, t = run(int(max(probe_rows, target_s / per_row)))
+        rows, nnz, t, t_calls = run(probe_rows)
+        # a noisy probe must not size the sample past its bound: a row costs
+        # at least a quarter of the probe's whole call time per row
+        per_row = max(t, 0.25 * t_calls) / max(rows, 1)
+        rows, nnz, t, _ = run(int(max(probe_rows, target_s / per_row)))
     return nnz / max(t, 1e-9), rows, nnz, t, threads, kind
 
 

@@ -639,7 +639,10 @@ struct ManySys {
     }
 };
 
-constexpr i64 kChunk = 8192;   // default arena entries per warp chunk
+constexpr i64 kChunk = 8192;          // default arena entries per warp chunk
+constexpr i64 kChunkLarge = 16384;    // the same for single builds of at least 64 rows per
+                                      // walking warp: fewer rows take the long-row kernels,
+                                      // for an open-chunk reserve that is small beside them
 // row_pos of a long row carries this bit: its slots hold entries and holes
 // (column kHole) until k_vv_compact_long gathers them.
 constexpr i64 kLongRow = 1ll << 62;
@@ -984,17 +987,24 @@ __device__ __forceinline__ void part_c(const VVParams& P, WarpShared& S, Q& q,
     const float rvx = __frcp_rn((float)nvx), rvy = __frcp_rn((float)nvy);
     const bool usep = pres != nullptr && nyv <= kBS;
     int nys = -1;   // indexed y singles listed in S (-1: not yet)
+    // neighbour-table row of x (its first entry; ~0: none), read one round ahead
+    const u32 nrow = (bm ? P.b_nbr : P.a_nbr) && gx != 0xffffffffu
+                         ? gx * (u32)nbr_stride(P.n_orb) : 0xffffffffu;
+    u32 gnext = nrow != 0xffffffffu && lane < nsx ? __ldg(&(bm ? P.b_nbr : P.a_nbr)[nrow + lane])
+                                                  : 0xffffffffu;
     for (int s0 = 0; s0 < nsx; s0 += 32) {
         const int sidx = s0 + lane;
+        const u32 gcur = gnext;
+        if (nrow != 0xffffffffu && sidx + 32 < nsx)
+            gnext = __ldg(&(bm ? P.b_nbr : P.a_nbr)[nrow + sidx + 32]);
         u32 gs = 0, gl = 0, gg = 0xffffffffu;
         int hh = 0, pp = 0;
         if (sidx < nsx) {
             int pi;
             hh = occx[small_div(sidx, rvx, nvx, pi)];
             pp = virx[pi];
-            const u32* nbt = bm ? P.b_nbr : P.a_nbr;
-            if (nbt && gx != 0xffffffffu) {
-                gg = __ldg(&nbt[(i64)gx * nbr_stride(P.n_orb) + sidx]);
+            if (nrow != 0xffffffffu) {
+                gg = gcur;
                 if (gg != 0xffffffffu) {
                     const u32* gst = bm ? P.b_gstart : P.a_gstart;
                     gs = __ldg(&gst[gg]);
@@ -1374,7 +1384,7 @@ __device__ __forceinline__ void walk_any(const VVParams& P, int r, u64 a, u64 b,
 // Single pass, first half: each warp appends the members of its rows to
 // private chunks of the arena (k_vv_eval turns them into entries in place).
 template <class Loc, class W>
-__global__ void __launch_bounds__(kWS * 32, 4) k_vv_arena(Loc L, Arena A) {
+__global__ void __launch_bounds__(kWS * 32, 3) k_vv_arena(Loc L, Arena A) {
     __shared__ WarpShared sh[kWS];
     WarpShared& S = sh[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -1989,7 +1999,9 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     size_t freeb = 0, totb = 0;
     DNQ_CUDA(cudaMemGetInfo(&freeb, &totb));
     // chunks of whole 4-slot groups (row starts stay aligned)
-    const i64 chunk = opt.arena_chunk > 0 ? ((i64)opt.arena_chunk + 3) & ~3ll : kChunk;
+    const i64 chunk = opt.arena_chunk > 0 ? ((i64)opt.arena_chunk + 3) & ~3ll
+                      : nrows >= 64 * warps             ? kChunkLarge
+                                                        : kChunk;
     i64 want = cap_hint > 0 ? cap_hint + cap_hint / 8 : 512 * nrows;
     want += warps * chunk;
     const bool f32_in_build = arena_out && dg;   // k_vv_eval writes the FP32 copy

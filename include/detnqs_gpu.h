@@ -160,7 +160,9 @@ int dnq_ham_destroy(dnq_ham_t h);
  *                          candidate walk instead of the string-group
  *                          matcher (both give identical blocks);
  *   DNQ_OPT_ARENA_CHUNK n: entries per warp chunk of the single-pass V->V
- *                          build (0 = default 8192);
+ *                          build (0 = default: 8192, and 16384 for
+ *                          single builds of at least 64 rows per
+ *                          walking warp);
  *   DNQ_OPT_ARENA_CAP   n: arena capacity in entries (0 = automatic); a
  *                          too-small arena falls back to an exact two-pass
  *                          build;

@@ -284,7 +284,7 @@ def test_bench_workload_rows_match_oracle(core, port):
                 want_vp=False)
     rp, cols, vals = H.to_csr_arrays(0)
     lens = np.diff(rp)
-    assert lens.max() > 8192                    # rows over one arena chunk exist
+    assert lens.max() > 16384                   # rows over one arena chunk exist
     rows = np.unique(np.concatenate([np.argsort(-lens, kind="stable")[:16],
                                      np.random.default_rng(1).choice(len(V), 64,
                                                                      replace=False)]))
