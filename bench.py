@@ -294,9 +294,13 @@ def cpu_reference_rows(systems, target_s: float = 15.0, probe_rows: int = 1024, 
                 _, V, eps = systems[k]
                 rows = g[which == k] - off[k]
                 c = ctx_of(k)
-                t0 = time.perf_counter()
-                c.vv_hb_rows(V, rows[:1], eps)
-                t_map = time.perf_counter() - t0
+                # the map of V is built inside each call: the faster of two
+                # one-row calls (host noise only adds time)
+                t_map = float("inf")
+                for _ in range(2):
+                    t0 = time.perf_counter()
+                    c.vv_hb_rows(V, rows[:1], eps)
+                    t_map = min(t_map, time.perf_counter() - t0)
                 t0 = time.perf_counter()
                 r = c.vv_hb_rows(V, rows, eps)
                 t_call = time.perf_counter() - t0
