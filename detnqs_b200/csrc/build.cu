@@ -358,15 +358,10 @@ void launch_diag(const dnq_ctx_s* c, const u64* d, i64 n, double* out, cudaStrea
 
 // CUDA events bracketing the build phases on the build stream.
 struct PhaseTimer {
-    cudaEvent_t ev[8];
+    Events<8> ev;
     int n = 0;
     cudaStream_t s;
-    explicit PhaseTimer(cudaStream_t st) : s(st) {
-        for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
-    }
-    ~PhaseTimer() {
-        for (auto& e : ev) cudaEventDestroy(e);
-    }
+    explicit PhaseTimer(cudaStream_t st) : s(st) {}
     void mark() { DNQ_CUDA(cudaEventRecord(ev[n++], s)); }
     void fill(double* out) {
         DNQ_CUDA(cudaEventSynchronize(ev[n - 1]));

@@ -223,6 +223,33 @@ struct DeviceGuard {
     }
 };
 
+// N timing events, destroyed with the scope on every path (a failed check
+// between their records throws); `make` false leaves them null.
+template <int N>
+struct Events {
+    cudaEvent_t e[N] = {};
+    explicit Events(bool make = true) {
+        if (!make) return;
+        try {
+            for (auto& x : e) DNQ_CUDA(cudaEventCreate(&x));
+        } catch (...) {
+            release();
+            throw;
+        }
+    }
+    ~Events() { release(); }
+    Events(const Events&) = delete;
+    Events& operator=(const Events&) = delete;
+    void release() {
+        for (auto& x : e) {
+            if (x) cudaEventDestroy(x);
+            x = nullptr;
+        }
+    }
+    cudaEvent_t operator[](int i) const { return e[i]; }
+    cudaEvent_t* data() { return e; }
+};
+
 // ---------------------------------------------------------------------------
 // Device bit helpers
 // ---------------------------------------------------------------------------

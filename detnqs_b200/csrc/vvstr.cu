@@ -1992,8 +1992,7 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
            const Options& opt, double* t_gen, double* t_scan, double* t_compact,
            i64* hits_out = nullptr, int scan = 0, DBuf<double>* dg = nullptr,
            const u32* order = nullptr, bool arena_out = false) {
-    cudaEvent_t ev[4];
-    for (auto& e : ev) DNQ_CUDA(cudaEventCreate(&e));
+    Events<4> ev;
     const int grid = vv_grid<Loc>(device);
     const i64 warps = (i64)grid * kWS;
     size_t freeb = 0, totb = 0;
@@ -2154,7 +2153,6 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     if (t_scan) *t_scan = ms;
     DNQ_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
     if (t_compact) *t_compact = ms;
-    for (auto& e : ev) cudaEventDestroy(e);
     return (i64)tests;
 }
 
@@ -2246,9 +2244,8 @@ void launch_check_orbitals(const u64* d, i64 n, int n_orb, unsigned long long* b
 void build_vv_checked(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                       double cut, const double* psi, cudaStream_t s, dnq_ham_s* H,
                       double* t_ms) {
-    cudaEvent_t e0, e1;
-    DNQ_CUDA(cudaEventCreate(&e0));
-    DNQ_CUDA(cudaEventCreate(&e1));
+    Events<2> tev;
+    const cudaEvent_t e0 = tev[0], e1 = tev[1];
     DNQ_CUDA(cudaEventRecord(e0, s));
     DBuf<unsigned long long> bad(1, s);
     DBuf<IndexProbe> probe(2, s);
@@ -2295,8 +2292,6 @@ void build_vv_checked(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     }
     float ms = 0;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     t_ms[0] = ms;    // checks, string indices, diagonal
     t_ms[1] = 0.0;   // no count pass
     t_ms[3] = tg;    // generation pass(es)
@@ -2310,9 +2305,8 @@ void build_vv_checked(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
 void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy, double eps1,
                       double cut, const double* psi, const double* diag, cudaStream_t s,
                       dnq_ham_s* H, double* t_ms) {
-    cudaEvent_t e0, e1;
-    DNQ_CUDA(cudaEventCreate(&e0));
-    DNQ_CUDA(cudaEventCreate(&e1));
+    Events<2> tev;
+    const cudaEvent_t e0 = tev[0], e1 = tev[1];
     DNQ_CUDA(cudaEventRecord(e0, s));
     StrIndex A, B;
     build_str_index(A, V, n, 0, n_orb, s);
@@ -2343,8 +2337,6 @@ void build_vv_strings(dnq_ctx_s* ctx, const u64* V, i64 n, int n_orb, int policy
     }
     float ms = 0;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     t_ms[0] += ms;   // string indices
     t_ms[1] = 0.0;   // no count pass
     t_ms[3] = tg;    // generation pass(es)
@@ -2710,10 +2702,9 @@ void check_step(dnq_batch_s* b, cudaStream_t s) {
 
 // mode 0: full step; mode 1: H.psi only on the resident CSR.
 float run_step(dnq_batch_s* b, int mode, int precision, bool graph, cudaStream_t s) {
-    cudaEvent_t ph[5];
     const bool phases = mode == 0 && !graph;
-    if (phases)
-        for (auto& e : ph) DNQ_CUDA(cudaEventCreate(&e));
+    Events<5> phe(phases);
+    cudaEvent_t* ph = phe.data();
     auto enqueue = [&](cudaStream_t st) {
         if (mode == 0) enqueue_step(b, precision, st, phases ? ph : nullptr);
         else enqueue_apply(b, precision, st);
@@ -2722,9 +2713,8 @@ float run_step(dnq_batch_s* b, int mode, int precision, bool graph, cudaStream_t
         launch_f32_split(b->M, b->val32.p, b->diag_op.p, s);   // once, outside any graph
         b->f32_ready = true;
     }
-    cudaEvent_t e0, e1;
-    DNQ_CUDA(cudaEventCreate(&e0));
-    DNQ_CUDA(cudaEventCreate(&e1));
+    Events<2> tev;
+    const cudaEvent_t e0 = tev[0], e1 = tev[1];
     cudaGraphExec_t& ge = b->gexec[mode];
     if (graph && (ge == nullptr || b->graph_prec[mode] != precision)) {
         if (ge) {
@@ -2749,15 +2739,12 @@ float run_step(dnq_batch_s* b, int mode, int precision, bool graph, cudaStream_t
     DNQ_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (phases) {
         for (int k = 0; k < 4; ++k) {
             float t = 0.f;
             DNQ_CUDA(cudaEventElapsedTime(&t, ph[k], ph[k + 1]));
             b->phase_ms[k] = t;
         }
-        for (auto& e : ph) cudaEventDestroy(e);
     }
     if (mode == 0) {
         b->f32_ready = precision == DNQ_F32;
@@ -2964,9 +2951,8 @@ int dnq_batch_apply_multi(dnq_batch_t b, const double* X, double* eloc, double* 
     }
     const int step = precision == DNQ_F32 ? 8 : 4;
     DBuf<unsigned char> scratch(spmm_scratch_bytes(n, std::min(k, step), precision), s);
-    cudaEvent_t e0, e1;
-    DNQ_CUDA(cudaEventCreate(&e0));
-    DNQ_CUDA(cudaEventCreate(&e1));
+    Events<2> tev;
+    const cudaEvent_t e0 = tev[0], e1 = tev[1];
     DNQ_CUDA(cudaEventRecord(e0, s));
     for (int j0 = 0; j0 < k; j0 += step) {
         const int kx = std::min(step, k - j0);
@@ -2982,8 +2968,6 @@ int dnq_batch_apply_multi(dnq_batch_t b, const double* X, double* eloc, double* 
     DNQ_CUDA(cudaStreamSynchronize(s));
     float ms = 0.f;
     DNQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (step_ms) *step_ms = ms;
     DNQ_API_END
 }
