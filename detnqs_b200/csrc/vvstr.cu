@@ -2068,7 +2068,9 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
     k_vv_eval_long<Loc><<<grid, kWS * 32, 0, s>>>(L, A);
     DNQ_CHECK_LAUNCH();
     int hov = 0;
+    unsigned long long hcur = 0;   // arena slots handed out (chunks and long rows)
     DNQ_CUDA(cudaMemcpyAsync(&hov, ovf.p, 4, cudaMemcpyDeviceToHost, s));
+    DNQ_CUDA(cudaMemcpyAsync(&hcur, cursor.p, 8, cudaMemcpyDeviceToHost, s));
     DNQ_CUDA(cudaStreamSynchronize(s));
     DNQ_CUDA(cudaEventRecord(ev[1], s));
     M.nr = nrows;
@@ -2087,6 +2089,27 @@ i64 run_vv(const Loc& L, i64 nrows, i64 cap_hint, int device, cudaStream_t s, Cs
                                                 nsum.p);
         DNQ_CHECK_LAUNCH();
         DNQ_CUDA(cudaMemcpyAsync(&nnz_h, nsum.p, 8, cudaMemcpyDeviceToHost, s));
+        // Every row lies below the cursor, which stays on a 4-slot boundary.
+        // A block that left at least 3/4 of its arena unused (small systems:
+        // the open-chunk reserve dominates) keeps only the handed-out prefix,
+        // at the same offsets, so its H.psi reads the same slots.
+        const i64 used = std::min<i64>((i64)hcur, cap);
+        const i64 slot_bytes = f32_in_build ? 16 : 12;
+        if (used <= cap / 4 && (cap - used) * slot_bytes >= (64ll << 20)) {
+            DBuf<u32> c2(used, s);
+            DBuf<double> v2(used, s);
+            DNQ_CUDA(cudaMemcpyAsync(c2.p, acol.p, used * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+            DNQ_CUDA(cudaMemcpyAsync(v2.p, aval.p, used * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     s));
+            acol = std::move(c2);
+            aval = std::move(v2);
+            if (f32_in_build) {
+                DBuf<float> f2(used, s);
+                DNQ_CUDA(cudaMemcpyAsync(f2.p, av32.p, used * sizeof(float),
+                                         cudaMemcpyDeviceToDevice, s));
+                av32 = std::move(f2);
+            }
+        }
         M.col = std::move(acol);
         M.val = std::move(aval);
         if (f32_in_build) M.val32 = std::move(av32);
